@@ -1,0 +1,384 @@
+#!/usr/bin/env python
+"""Droplet-step benchmark (one JSON line on stdout, rank 0).
+
+Workload (default): the 16,777,216-droplet precision-study case -- 256^3 grid
+(Lx=Ly=Lz=2 m), seeded divergence-free k^-5/3 velocity of rms 1.0 m/s,
+T = 293 K + N(0, 0.3 K), q = 0.015 + N(0, 2e-4), lognormal radius (median
+2 um, sigma_g 1.6), dt = 5e-4 s -- with 6th-order interpolation, backward
+Euler + Newton radius/temperature solve and two-way coupling.  One "step" is
+particle_update_BE + particle_coupling_update over all droplets.  Inputs are
+generated from fixed seeds (no dataset); the droplet state (~3.5 GB) is far
+larger than L2, so no explicit flush is needed between steps.
+
+  value   mixed-precision droplet-updates/s, device-timed (CUDA events on the
+          library's stream), inputs resident in HBM
+  fp64    the FP64 path on the same inputs
+  e2e     the same metric through the C ABI with host buffers: each step
+          uploads the five halo-padded fields from pinned host memory and
+          downloads the six source arrays
+  roofline  dominant kernel (the droplet update): algorithmic bytes per
+          launch (N*B_d + P_pad*5*s_f) / its event-timed duration, against
+          the measured HBM copy bandwidth
+  cpu_baseline  the CPU restatement of the reference step (oracle/) on the
+          host cores, on a bounded sample of the same workload
+
+--gpus N runs N independent replicas (weak scaling; the step has no data
+exchange on one domain), timed as the max over ranks.
+--impl reference times the reference's CPU implementation of the path (the
+oracle port; the Fortran reference cannot be built here) on the same metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+B_D = {"fp64": 248, "mixed": 224}       # algorithmic bytes per droplet
+METRIC = "droplet-updates/s (mixed precision, 16M droplets, 6th-order BE step + coupling)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=16_777_216)
+    ap.add_argument("--grid", type=int, nargs=3, default=[256, 256, 256])
+    ap.add_argument("--ilin", type=int, default=0)
+    ap.add_argument("--skip-fp64", action="store_true")
+    ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
+                    help="run one precision only (profiling)")
+    return ap.parse_args()
+
+
+def dist_setup(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if ws > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        return rank, ws, dist
+    return rank, ws, None
+
+
+def barrier(dist):
+    if dist is not None:
+        import torch
+        dist.barrier(device_ids=[torch.cuda.current_device()])
+
+
+def max_over_ranks(dist, v: float) -> float:
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def make_workload(args, seed_offset=0):
+    from ntlp_b200 import generator as gen
+    nx, ny, nz = args.grid
+    params = gen.default_params(ilin=args.ilin)
+    return gen.make_case("c1", n=args.n, grid_n=(nx, ny, nz), params=params,
+                         seed=1 + seed_offset)
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    def __init__(self):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            dev = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[0] or "0"
+            self.p = subprocess.Popen(["nvidia-smi", "-i", dev, f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def run_device(case, precision: str, args, dist, rank):
+    """Device-timed steps; returns dict with throughput and per-phase times."""
+    import torch
+    import ntlp_b200
+    from ntlp_b200 import abi
+    p = dict(case.params, precision=abi.NTLP_PREC_MIXED if precision == "mixed" else abi.NTLP_PREC_FP64)
+    n = case.droplets["radius"].shape[0]
+    s = ntlp_b200.DropletStep(case.grid, p, capacity=n)
+    s.set_fields_ext(case.ext_cache)
+    s.set_droplets(case.droplets)
+    stream = torch.cuda.ExternalStream(s.stream_handle)
+    it = 1
+    for _ in range(args.warmup):
+        s.particle_update_BE(case.dt, it, counters=False)
+        s.particle_coupling_update(case.dt, download=False)
+        it += 1
+    s.sync()
+    n0 = s.numpart
+    s.profile(True)
+    s.profile_read()
+    barrier(dist)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    clk = ClockSampler() if rank == 0 else None
+    if clk:
+        clk.start()
+    e0.record(stream)
+    for _ in range(args.steps):
+        s.particle_update_BE(case.dt, it, counters=False)
+        s.particle_coupling_update(case.dt, download=False)
+        it += 1
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    clocks = clk.stop() if clk else None
+    ms = e0.elapsed_time(e1)
+    prof = s.profile_read()
+    n1 = s.numpart
+    ms_max = max_over_ranks(dist, ms)
+    s.close()
+    return dict(ms=ms_max, n0=n0, n1=n1, prof=prof, clocks=clocks)
+
+
+def run_e2e(case, args, dist):
+    """Through the C ABI with host buffers: fields up, step, sources down."""
+    import torch
+    import ntlp_b200
+    from ntlp_b200 import abi
+    p = dict(case.params, precision=abi.NTLP_PREC_MIXED)
+    n = case.droplets["radius"].shape[0]
+    s = ntlp_b200.DropletStep(case.grid, p, capacity=n)
+    pinned = {}
+    for k, v in case.ext_cache.items():
+        t = torch.empty(v.shape, dtype=torch.float64, pin_memory=True)
+        t.numpy()[...] = v
+        pinned[k] = t.numpy()
+    g = case.grid
+    shape = (g["nnx"], g["nny"], g["nnz"] + 2)
+    mom = torch.empty((3,) + shape, dtype=torch.float64, pin_memory=True).numpy()
+    rest = [torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy() for _ in range(3)]
+    s.set_droplets(case.droplets)
+    it = 1
+    for _ in range(max(1, args.warmup)):
+        s.set_fields_ext(pinned)
+        s.particle_update_BE(case.dt, it, counters=False)
+        s.particle_coupling_update(case.dt, out=[mom] + rest)
+        it += 1
+    n0 = s.numpart
+    barrier(dist)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        s.set_fields_ext(pinned)
+        s.particle_update_BE(case.dt, it, counters=False)
+        s.particle_coupling_update(case.dt, out=[mom] + rest)
+        it += 1
+    s.sync()
+    dt = time.perf_counter() - t0
+    dt = max_over_ranks(dist, dt)
+    n1 = s.numpart
+    s.close()
+    npad = (g["nnx"] + 5) * (g["nny"] + 5) * (g["nnz"] + 2)
+    nsrc = g["nnx"] * g["nny"] * (g["nnz"] + 2)
+    return dict(seconds=dt, n0=n0, n1=n1, h2d=5 * npad * 8, d2h=6 * nsrc * 8)
+
+
+def cpu_baseline(case, seconds: float, dist=None):
+    """The oracle's multi-threaded BE step + coupling on a bounded sample of
+    the same workload (same fields, the first n droplets)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from ntlp_b200 import abi
+    L = pyoracle.lib("ntlp")
+    threads = int(L.oracle_max_threads())
+    o = pyoracle.Oracle(case.grid, case.params, case.ext_cache)
+    def sample(n):
+        return {k: (np.ascontiguousarray(v[..., :n]) if isinstance(v, np.ndarray) and v.ndim == 2 else
+                    (np.ascontiguousarray(v[:n]) if isinstance(v, np.ndarray) else v))
+                for k, v in case.droplets.items()}
+    n = min(20000, case.droplets["radius"].shape[0])
+    d = sample(n)
+    t0 = time.perf_counter()
+    o.step_be_omp(d, case.dt, 1, threads)
+    t1 = time.perf_counter() - t0
+    per = t1 / n
+    n = int(min(case.droplets["radius"].shape[0], max(n, seconds / max(per, 1e-9))))
+    d = sample(n)
+    o.step_be_omp(d, case.dt, 1, threads)     # it = 1 (vp = uf), as the GPU's first step
+    t0 = time.perf_counter()
+    o.step_be_omp(d, case.dt, 2, threads)
+    el = time.perf_counter() - t0
+    return dict(value=n / el, unit="droplet-updates/s", cores=threads, kind="port",
+                sample=f"{n} droplets of the same workload, 1 BE step + coupling, {threads} OpenMP threads, "
+                       f"{el:.1f} s")
+
+
+def main():
+    args = parse()
+    rank, ws, dist = dist_setup(args)
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        case = make_workload(args)
+        case.ext_cache = case.ext()
+        steps = []
+        cb = None
+        for _ in range(max(1, args.steps)):
+            cb = cpu_baseline(case, min(args.cpu_seconds, 20.0))
+            steps.append(cb["value"])
+        v = statistics.median(steps)
+        cb["value"] = v
+        line = {"metric": METRIC, "value": v, "unit": "droplet-updates/s", "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic (seeded generator; no dataset)", "impl": "reference",
+                "config": {"workload": f"BE droplet step, {args.n} droplets, {args.grid[0]}x{args.grid[1]}x{args.grid[2]} grid, "
+                                       f"ilin={args.ilin}, dt=5e-4", "parallelism": "host OpenMP"},
+                "cpu_baseline": cb,
+                "e2e": {"value": v, "unit": "droplet-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+
+    import torch
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    if ws == 1:
+        torch.cuda.set_device(0)
+    from ntlp_b200 import build
+    build.build()
+    t_gen = time.perf_counter()
+    case = make_workload(args, seed_offset=rank)
+    case.ext_cache = case.ext()
+    t_gen = time.perf_counter() - t_gen
+    g = case.grid
+    n = case.droplets["radius"].shape[0]
+    npad = (g["nnx"] + 5) * (g["nny"] + 5) * (g["nnz"] + 2)
+    nsrc = g["nnx"] * g["nny"] * (g["nnz"] + 2)
+
+    res = {}
+    for prec in (["mixed", "fp64"] if args.only is None else [args.only]):
+        if prec == "fp64" and args.skip_fp64:
+            continue
+        res[prec] = run_device(case, prec, args, dist, rank)
+    e2e = None if args.skip_e2e else run_e2e(case, args, dist)
+    cb = None
+    if rank == 0 and ws == 1 and not args.skip_cpu:
+        cb = cpu_baseline(case, args.cpu_seconds)
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
+
+    head = "mixed" if "mixed" in res else "fp64"
+    r = res[head]
+    upd = 0.5 * (r["n0"] + r["n1"]) * args.steps
+    value = upd / (r["ms"] * 1e-3) * ws
+    hbm, src = peaks()
+    sf = 4 if head == "mixed" else 8
+    alg_update = n * B_D[head] + npad * 5 * sf
+    upd_ms = r["prof"]["update_ms"] / args.steps
+    achieved = alg_update / (upd_ms * 1e-3) / 1e9
+    step_alg = alg_update + nsrc * 48
+    line = {
+        "metric": METRIC, "value": value, "unit": "droplet-updates/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": r["ms"] / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 interp/drag + f64 state/Newton/sources" if head == "mixed" else "f64",
+        "data": "synthetic (seeded generator; no dataset)",
+        "config": {"workload": f"BE droplet step + coupling, {n} droplets, {g['nnx']}x{g['nny']}x{g['nnz']} grid, "
+                               f"ilin={args.ilin} ({'6th-order' if args.ilin == 0 else 'trilinear'}), dt=5e-4",
+                   "droplets": n, "grid": [g["nnx"], g["nny"], g["nnz"]],
+                   "l2": "state (~3.5 GB) >> L2; no flush needed", "parallelism": f"{ws} replica(s)"},
+        "phases_ms_per_step": {k: v / args.steps for k, v in r["prof"].items() if k.endswith("_ms")},
+        "gpu_launches": int(r["prof"]["launches"]),
+        "roofline": {"bound": "hbm", "kernel": "k_update_be_" + ("mixed" if head == "mixed" else "64"),
+                     "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "peak_source": src, "traffic": None,
+                     "alg_bytes_per_launch": alg_update,
+                     "step_frac": (step_alg / (r["ms"] / args.steps * 1e-3) / 1e9) / hbm},
+        "clocks": r["clocks"],
+        "gen_seconds": t_gen,
+    }
+    if "fp64" in res and head == "mixed":
+        f = res["fp64"]
+        fv = 0.5 * (f["n0"] + f["n1"]) * args.steps / (f["ms"] * 1e-3) * ws
+        f_alg = n * B_D["fp64"] + npad * 5 * 8
+        f_upd_ms = f["prof"]["update_ms"] / args.steps
+        line["fp64"] = {"value": fv, "ms_per_step": f["ms"] / args.steps,
+                        "phases_ms_per_step": {k: v / args.steps for k, v in f["prof"].items() if k.endswith("_ms")},
+                        "update_hbm_frac": f_alg / (f_upd_ms * 1e-3) / 1e9 / hbm}
+        line["mixed_over_fp64"] = value / fv
+    if e2e:
+        ev = 0.5 * (e2e["n0"] + e2e["n1"]) * args.steps / e2e["seconds"] * ws
+        line["e2e"] = {"value": ev, "unit": "droplet-updates/s", "h2d_bytes_per_step": e2e["h2d"],
+                       "d2h_bytes_per_step": e2e["d2h"],
+                       "note": "fields uploaded from pinned host memory and sources downloaded every step"}
+    if cb:
+        line["cpu_baseline"] = cb
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

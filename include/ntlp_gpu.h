@@ -1,0 +1,182 @@
+/*
+ * ntlp_gpu.h -- C ABI of the B200 droplet step (libntlp_gpu.so).
+ *
+ * The reference has no plugin boundary: its droplet step is three
+ * argument-less Fortran module procedures that talk through module globals
+ *   particle_update_BE            particles.f90:3000-3280  (called les.F:422)
+ *   particle_update_rk3(istage)   particles.f90:2845-2998  (called les.F:404)
+ *   particle_coupling_update      particles.f90:1151-1276  (called les.F:431)
+ * plus the single-domain meaning of fill_ext (particles.f90:91-328) and
+ * particle_coupling_exchange (particles.f90:1066-1149).  The entry points
+ * below replace those bodies; the Fortran host keeps its time loop and
+ * passes its arrays by address (ISO_C_BINDING shim: INTEGRATION.md).
+ *
+ * Conventions
+ *   - Every function returns 0 (NTLP_OK) or a negative NTLP_ERR_* code; on
+ *     error ntlp_last_error(ctx) describes it.  Nothing calls exit/abort.
+ *   - The caller owns every host array; the library owns device memory.
+ *   - Arrays are contiguous, column-major (Fortran order), FP64 unless
+ *     stated.  Grid index ranges are the reference's.
+ *   - A context is used by one host thread at a time; many contexts may
+ *     coexist.  All device work of a context runs on its own CUDA stream.
+ */
+#ifndef NTLP_GPU_H
+#define NTLP_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define NTLP_OK             0
+#define NTLP_ERR_ARG       -1   /* invalid argument or size                 */
+#define NTLP_ERR_CUDA      -2   /* CUDA runtime error                       */
+#define NTLP_ERR_CAPACITY  -3   /* droplet count above the context capacity */
+#define NTLP_ERR_STATE     -4   /* call out of order (e.g. no fields yet)   */
+#define NTLP_ERR_NOMEM     -5   /* device allocation refused / over budget  */
+#define NTLP_ERR_DEVICE    -6   /* a kernel reported an error (see message) */
+
+/* ---- enumerations ------------------------------------------------------ */
+#define NTLP_PREC_FP64   0      /* every operation in FP64, reference order  */
+#define NTLP_PREC_MIXED  1      /* FP32 interpolation/drag, FP64 positions,
+                                   Newton solve and source accumulation      */
+
+#define NTLP_LAYOUT_COLUMN 0    /* (0:nnz+1, 1:nny, 1:nnx), z fastest:
+                                   partsrc_t after the periodic fold        */
+#define NTLP_LAYOUT_FLOW   1    /* (1:nnx, 1:nny, 0:nnz+1), x fastest:
+                                   partsrc after ztox_trans, as read by
+                                   apply_particle_coupling                  */
+
+/* ---- grid (les.F:5451-5498 init, les.F:5836-5874 get_dz) --------------- */
+typedef struct ntlp_grid {
+    int32_t nnx, nny, nnz;      /* interior points; dx = xl/nnx, dy = yl/nny */
+    int32_t reserved;
+    double xl, yl, zl;          /* domain lengths (zl used by flux tallies)  */
+    const double *z;            /* z(0:nnz+1)    w levels                    */
+    const double *zz;           /* zz(0:nnz+1)   u levels                    */
+    const double *dzw;          /* dzw(0:nnz+2)                              */
+    const double *dzu;          /* dzu(0:nnz+2)                              */
+} ntlp_grid;
+
+/* ---- flags and constants (namelists &flags, &constants; defs.F) -------- */
+typedef struct ntlp_params {
+    int32_t ilin;               /* 1 trilinear, otherwise 6th-order Lagrange */
+    int32_t ipart_method;       /* 1 RK3, 2 backward Euler (informational)   */
+    int32_t icouple, iTcouple, iHcouple;
+    int32_t ievap, iexner;
+    int32_t icase;              /* 0 reflect at bottom; 4 spray top; else kill */
+    int32_t precision;          /* NTLP_PREC_*                               */
+    int32_t reserved;
+    double nuf, Cpa, Cpp, Pra, Sc, Rd;
+    double rhow, rhos, Mw, Ru, Gam, Lv, Cpv;
+    double grav;                /* gravity used by func_p_base (iexner=1)    */
+    double part_grav[3];
+    double radius_init;         /* namelist radius_init: sets taup0          */
+    double surf_rho, surf_p, tsfcc1;
+    double pi2;                 /* 2*(4*atan(1)) as les.F:5386-5387 computes */
+} ntlp_params;
+
+/* ---- droplet state, structure of arrays (type particle, particles.f90:76-85)
+ * Upload reads every non-NULL pointer of the first n entries; download writes
+ * every non-NULL pointer.  xrhs/vrhs/Tprhs_s/Tprhs_L/radrhs are RK3 state.
+ * lid (download only) is each survivor's position in the uploaded list, so
+ * the caller can compact the record fields the step does not touch
+ * (pidx, procidx, dist, u_sub, sigm_s, ...).                                */
+typedef struct ntlp_droplets {
+    int64_t n;
+    double *xp[3], *vp[3], *uf[3], *xrhs[3], *vrhs[3];
+    double *Tp, *Tprhs_s, *Tprhs_L, *Tf, *radius, *radrhs, *qinf, *qstar;
+    double *res, *m_s, *kappa_s, *rc, *actres, *numact;
+    double *vp_old[3], *Tp_old, *radius_old;
+    int64_t *mult;
+    int32_t *lid;
+} ntlp_droplets;
+
+/* ---- per-step counters (module particles, particles.f90:24-31) --------- */
+typedef struct ntlp_counters {
+    int64_t numpart;            /* droplets alive after the step (tnumpart)  */
+    int64_t num_destroy;        /* killed at the bottom boundary             */
+    int64_t denum, actnum;      /* deactivations / activations (BE)          */
+    int64_t num100, numimpos;   /* Gauss-Newton failures / impossible solves */
+    int64_t neg_qinf;           /* droplets that saw qinf < 0 (warning)      */
+    int64_t bad_index;          /* droplets outside the grid (must be 0)     */
+} ntlp_counters;
+
+typedef struct ntlp_ctx ntlp_ctx;
+
+/* ---- context ----------------------------------------------------------- */
+/* Create a context for one box on the current CUDA device.  capacity is the
+ * largest droplet count that will be uploaded.  Grid arrays are copied.    */
+int  ntlp_ctx_create(const ntlp_grid *grid, const ntlp_params *params,
+                     int64_t capacity, ntlp_ctx **out);
+void ntlp_ctx_destroy(ntlp_ctx *ctx);
+const char *ntlp_last_error(const ntlp_ctx *ctx);
+int64_t ntlp_numpart(const ntlp_ctx *ctx);
+/* Device bytes held by the context (fields, droplets, work arrays). */
+int64_t ntlp_device_bytes(const ntlp_ctx *ctx);
+
+/* ---- fields ------------------------------------------------------------ */
+/* Halo-padded fields in the reference layout uext(0:nnz+1,-1:nny+3,-1:nnx+3)
+ * (particles.f90:5-10, filled by fill_ext): u, v, w, T, q(=t(...,2,...)).  */
+int ntlp_fields_upload_ext(ntlp_ctx *ctx, const double *uext, const double *vext,
+                           const double *wext, const double *Text,
+                           const double *T2ext);
+/* Flow-layout fields u(1:nnx,1:nny,0:nnz+1) (x fastest, les.F arrays u,v,w
+ * and t(:,:,1,:), t(:,:,2,:)); the device transposes to z-fastest columns
+ * and fills the periodic halo (fill_ext on one domain, particles.f90:91-328). */
+int ntlp_fields_upload(ntlp_ctx *ctx, const double *u, const double *v,
+                       const double *w, const double *t, const double *q);
+
+/* ---- droplets ---------------------------------------------------------- */
+int ntlp_droplets_upload(ntlp_ctx *ctx, const ntlp_droplets *d);
+/* Writes the survivors in list order; d->n receives the count.  The arrays
+ * must hold at least ntlp_numpart(ctx) entries.                           */
+int ntlp_droplets_download(ntlp_ctx *ctx, ntlp_droplets *d);
+
+/* ---- the step ---------------------------------------------------------- */
+/* particle_update_BE: interpolation, BE advance, Newton radius/temperature
+ * solve, flux tallies, non-periodic then periodic boundaries, count.
+ * it is the time-step counter (vp = uf when it <= 1).  counters may be NULL;
+ * when given, the call waits for the step to finish.                       */
+int ntlp_step_be(ntlp_ctx *ctx, double dt, int32_t it, ntlp_counters *counters);
+/* particle_update_rk3(istage), istage in 1..3 (coefficients les.F:856-861). */
+int ntlp_step_rk3(ntlp_ctx *ctx, int32_t istage, double dt, int32_t it,
+                  ntlp_counters *counters);
+/* particle_coupling_update + the periodic fold of particle_coupling_exchange.
+ * Deposits momentum (partsrc(...,1:3)), heat (partTsrc), vapour (partHsrc)
+ * and vapour enthalpy (partTEsrc) sources.  Each host pointer may be NULL
+ * (kept on the device).  partsrc holds the three components one after the
+ * other, each an array of the chosen layout.  Summation order per node is
+ * the reference's list order, so FP64 results are bit-reproducible.        */
+int ntlp_coupling(ntlp_ctx *ctx, double dt, int32_t layout, double *partsrc,
+                  double *partTsrc, double *partHsrc, double *partTEsrc);
+/* Vertical droplet flux tallies of the last BE step, pflux(0:nnz),
+ * pmassflux(0:nnz), penegflux(0:nnz) (particles.f90:3209-3238).           */
+int ntlp_flux(ntlp_ctx *ctx, double *pflux, double *pmassflux, double *penegflux);
+/* Wait for the context's stream. */
+int ntlp_sync(ntlp_ctx *ctx);
+/* The context's CUDA stream (a cudaStream_t), for callers that order their
+ * own work or events after the step.                                      */
+void *ntlp_stream(ntlp_ctx *ctx);
+
+/* ---- instrumentation (phase timers; measurement.f90's named phases) ----- */
+/* When enabled, every step records CUDA events around its kernels on the
+ * context's stream; ntlp_profile_read returns the accumulated milliseconds
+ * of the phases {update, sort, deposit, other} and the number of kernel
+ * launches since the last reset, then resets them.                        */
+int ntlp_profile_enable(ntlp_ctx *ctx, int enable);
+int ntlp_profile_read(ntlp_ctx *ctx, double ms[4], int64_t *launches);
+
+/* ---- droplet creation helper ------------------------------------------- */
+/* Koehler critical radius rc of n droplets (crit_radius with the radval
+ * table of setup_radval, particles.f90:5294-5327), computed on the host;
+ * create_particle (particles.f90:2264-2268) sets part%rc with it.          */
+int ntlp_crit_radius(const ntlp_params *params, int64_t n, const double *m_s,
+                     const double *kappa_s, const double *T, double *rc);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NTLP_GPU_H */

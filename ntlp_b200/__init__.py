@@ -1,0 +1,214 @@
+"""B200-native Lagrangian droplet step of the NTLP LES code.
+
+The compute path is libntlp_gpu.so (hand-written sm_100a CUDA behind the C
+ABI of include/ntlp_gpu.h).  This module loads it with ctypes and mirrors
+the reference's Fortran interface for the path:
+
+    particle_update_BE          particles.f90:3000   -> DropletStep.particle_update_BE
+    particle_update_rk3(istage) particles.f90:2845   -> DropletStep.particle_update_rk3
+    particle_coupling_update    particles.f90:1151   -> DropletStep.particle_coupling_update
+    fill_ext (one domain)       particles.f90:91     -> DropletStep.fill_ext / set_fields_ext
+
+There is no CPU fallback: if the library is missing or no CUDA device is
+present, the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libntlp_gpu.so")
+_lib = None
+
+
+class NtlpError(RuntimeError):
+    pass
+
+
+def load_library(path: str = LIB_PATH) -> C.CDLL:
+    """Load libntlp_gpu.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise NtlpError(f"{path} not built; run `python -m ntlp_b200.build`")
+    L = C.CDLL(path)
+    P = C.POINTER
+    dp = P(C.c_double)
+    L.ntlp_ctx_create.argtypes = [P(abi.NtlpGrid), P(abi.NtlpParams), C.c_int64, P(C.c_void_p)]
+    L.ntlp_ctx_destroy.argtypes = [C.c_void_p]
+    L.ntlp_ctx_destroy.restype = None
+    L.ntlp_last_error.argtypes = [C.c_void_p]
+    L.ntlp_last_error.restype = C.c_char_p
+    L.ntlp_numpart.argtypes = [C.c_void_p]
+    L.ntlp_numpart.restype = C.c_int64
+    L.ntlp_device_bytes.argtypes = [C.c_void_p]
+    L.ntlp_device_bytes.restype = C.c_int64
+    L.ntlp_fields_upload_ext.argtypes = [C.c_void_p] + [dp] * 5
+    L.ntlp_fields_upload.argtypes = [C.c_void_p] + [dp] * 5
+    L.ntlp_droplets_upload.argtypes = [C.c_void_p, P(abi.NtlpDroplets)]
+    L.ntlp_droplets_download.argtypes = [C.c_void_p, P(abi.NtlpDroplets)]
+    L.ntlp_step_be.argtypes = [C.c_void_p, C.c_double, C.c_int32, P(abi.NtlpCounters)]
+    L.ntlp_step_rk3.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_int32, P(abi.NtlpCounters)]
+    L.ntlp_coupling.argtypes = [C.c_void_p, C.c_double, C.c_int32, dp, dp, dp, dp]
+    L.ntlp_flux.argtypes = [C.c_void_p, dp, dp, dp]
+    L.ntlp_sync.argtypes = [C.c_void_p]
+    L.ntlp_crit_radius.argtypes = [P(abi.NtlpParams), C.c_int64, dp, dp, dp, dp]
+    L.ntlp_stream.argtypes = [C.c_void_p]
+    L.ntlp_stream.restype = C.c_void_p
+    L.ntlp_profile_enable.argtypes = [C.c_void_p, C.c_int]
+    L.ntlp_profile_read.argtypes = [C.c_void_p, dp, P(C.c_int64)]
+    _lib = L
+    return L
+
+
+def crit_radius(params: dict, m_s, kappa_s, T) -> np.ndarray:
+    """Koehler critical radius per droplet (crit_radius, particles.f90:5307)."""
+    L = load_library()
+    p = abi.make_params_struct(params)
+    m_s, kappa_s, T = (np.ascontiguousarray(a, dtype=np.float64) for a in (m_s, kappa_s, T))
+    out = np.empty_like(m_s)
+    rc = L.ntlp_crit_radius(C.byref(p), len(m_s), abi.as_dptr(m_s), abi.as_dptr(kappa_s), abi.as_dptr(T),
+                            abi.as_dptr(out))
+    if rc != 0:
+        raise NtlpError(f"ntlp_crit_radius failed ({rc})")
+    return out
+
+
+class DropletStep:
+    """One box (periodic domain) with its fields and droplets resident on
+    the current CUDA device."""
+
+    def __init__(self, grid: dict, params: dict, capacity: int):
+        self.L = load_library()
+        self.grid = grid
+        self.params = dict(params)
+        self._g, self._gkeep = abi.make_grid_struct(grid)
+        self._p = abi.make_params_struct(params)
+        h = C.c_void_p()
+        rc = self.L.ntlp_ctx_create(C.byref(self._g), C.byref(self._p), int(capacity), C.byref(h))
+        if rc != 0 or not h.value:
+            raise NtlpError(f"ntlp_ctx_create failed ({rc})")
+        self.h = h
+        self.capacity = int(capacity)
+        self.last_counters: dict = {}
+
+    # -- plumbing --
+    def _check(self, rc: int, what: str):
+        if rc != 0:
+            msg = self.L.ntlp_last_error(self.h).decode(errors="replace")
+            raise NtlpError(f"{what} failed ({rc}): {msg}")
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.L.ntlp_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def numpart(self) -> int:
+        return int(self.L.ntlp_numpart(self.h))
+
+    @property
+    def device_bytes(self) -> int:
+        return int(self.L.ntlp_device_bytes(self.h))
+
+    def sync(self):
+        self._check(self.L.ntlp_sync(self.h), "ntlp_sync")
+
+    @property
+    def stream_handle(self) -> int:
+        """cudaStream_t of the context (for events on the launching stream)."""
+        return int(self.L.ntlp_stream(self.h) or 0)
+
+    def profile(self, enable: bool = True):
+        self._check(self.L.ntlp_profile_enable(self.h, 1 if enable else 0), "ntlp_profile_enable")
+
+    def profile_read(self) -> dict:
+        ms = (C.c_double * 4)()
+        n = C.c_int64()
+        self._check(self.L.ntlp_profile_read(self.h, ms, C.byref(n)), "ntlp_profile_read")
+        return dict(update_ms=ms[0], sort_ms=ms[1], deposit_ms=ms[2], other_ms=ms[3], launches=int(n.value))
+
+    # -- fields (fill_ext) --
+    def set_fields_ext(self, ext: dict):
+        arrs = [np.ascontiguousarray(ext[k], dtype=np.float64) for k in ("u", "v", "w", "T", "q")]
+        self._ext_keep = arrs
+        self._check(self.L.ntlp_fields_upload_ext(self.h, *(abi.as_dptr(a) for a in arrs)),
+                    "ntlp_fields_upload_ext")
+        self.sync()
+
+    def fill_ext(self, flow: dict):
+        """Flow-layout fields u(1:nnx,1:nny,0:nnz+1) -> device halo fill."""
+        arrs = [np.ascontiguousarray(flow[k], dtype=np.float64) for k in ("u", "v", "w", "T", "q")]
+        self._flow_keep = arrs
+        self._check(self.L.ntlp_fields_upload(self.h, *(abi.as_dptr(a) for a in arrs)), "ntlp_fields_upload")
+        self.sync()
+
+    # -- droplets --
+    def set_droplets(self, d: dict):
+        s = abi.make_droplets_struct(d)
+        self._check(self.L.ntlp_droplets_upload(self.h, C.byref(s)), "ntlp_droplets_upload")
+
+    def get_droplets(self, rk3: bool = False) -> dict:
+        n = self.numpart
+        d = abi.empty_droplets(max(n, 1))
+        s = abi.make_droplets_struct(d, n=n)
+        self._check(self.L.ntlp_droplets_download(self.h, C.byref(s)), "ntlp_droplets_download")
+        n = int(s.n)
+        out = {}
+        for k, v in d.items():
+            out[k] = np.ascontiguousarray(v[..., :n] if v.ndim == 2 else v[:n])
+        return out
+
+    # -- the step --
+    def particle_update_BE(self, dt: float, it: int, counters: bool = True) -> dict:
+        c = abi.NtlpCounters()
+        self._check(self.L.ntlp_step_be(self.h, float(dt), int(it), C.byref(c) if counters else None),
+                    "ntlp_step_be")
+        self.last_counters = c.as_dict() if counters else {}
+        return self.last_counters
+
+    def particle_update_rk3(self, istage: int, dt: float, it: int, counters: bool = True) -> dict:
+        c = abi.NtlpCounters()
+        self._check(self.L.ntlp_step_rk3(self.h, int(istage), float(dt), int(it),
+                                         C.byref(c) if counters else None), "ntlp_step_rk3")
+        self.last_counters = c.as_dict() if counters else {}
+        return self.last_counters
+
+    def particle_coupling_update(self, dt: float, layout: int = abi.NTLP_LAYOUT_COLUMN,
+                                 out: list | None = None, download: bool = True):
+        """Returns [partsrc_1, partsrc_2, partsrc_3, partTsrc, partHsrc,
+        partTEsrc]; column layout arrays have shape (nnx, nny, nnz+2) in C
+        order (z fastest), flow layout (nnz+2, nny, nnx) (x fastest)."""
+        g = self.grid
+        nx, ny, nz2 = g["nnx"], g["nny"], g["nnz"] + 2
+        if not download:
+            self._check(self.L.ntlp_coupling(self.h, float(dt), int(layout), None, None, None, None),
+                        "ntlp_coupling")
+            return None
+        shape = (nx, ny, nz2) if layout == abi.NTLP_LAYOUT_COLUMN else (nz2, ny, nx)
+        if out is None:
+            mom = np.empty((3,) + shape)
+            rest = [np.empty(shape) for _ in range(3)]
+        else:
+            mom, rest = out[0], out[1:]
+        self._check(self.L.ntlp_coupling(self.h, float(dt), int(layout), abi.as_dptr(mom.reshape(-1)),
+                                         *(abi.as_dptr(a.reshape(-1)) for a in rest)), "ntlp_coupling")
+        return [mom[0], mom[1], mom[2], rest[0], rest[1], rest[2]]
+
+    def flux(self):
+        nz1 = self.grid["nnz"] + 1
+        out = [np.zeros(nz1) for _ in range(3)]
+        self._check(self.L.ntlp_flux(self.h, *(abi.as_dptr(a) for a in out)), "ntlp_flux")
+        return out

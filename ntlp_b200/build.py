@@ -1,0 +1,91 @@
+"""Build libntlp_gpu.so (sm_100a) in-tree with nvcc.
+
+    python -m ntlp_b200.build [--verbose]
+
+Compilation units:
+  ntlp_fp64.cu   FP64 kernels, --fmad=false (each operation rounds once, in
+                 the reference's order)
+  ntlp_mixed.cu  mixed-precision kernels (contraction allowed)
+  ntlp_sort.cu   counting sort on cell keys, halo fill, bookkeeping
+  ntlp_api.cu    the C ABI of include/ntlp_gpu.h
+Objects go to ntlp_b200/_build/, the library to ntlp_b200/_lib/.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(HERE, "_build")
+LIBDIR = os.path.join(HERE, "_lib")
+LIB = os.path.join(LIBDIR, "libntlp_gpu.so")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+UNITS = {
+    "ntlp_fp64.cu": ["--fmad=false"],
+    "ntlp_mixed.cu": [],
+    "ntlp_sort.cu": [],
+    "ntlp_api.cu": [],
+}
+HEADERS = ["ntlp_math.h", "ntlp_dev.cuh", "ntlp_kernels.h", "ntlp_physics.cuh"]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def host_compiler() -> list[str]:
+    return ["-ccbin", "/usr/bin/g++"] if os.path.exists("/usr/bin/g++") else []
+
+
+def _newer(target: str, deps: list[str]) -> bool:
+    if not os.path.exists(target):
+        return False
+    t = os.path.getmtime(target)
+    return all(os.path.getmtime(d) <= t for d in deps if os.path.exists(d))
+
+
+def build(verbose: bool = False, force: bool = False, ptxas_v: bool = False) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    os.makedirs(LIBDIR, exist_ok=True)
+    inc = ["-I" + CSRC, "-I" + os.path.join(os.path.dirname(HERE), "include")]
+    common = ["-O3", "-std=c++17", "-lineinfo", *ARCH, *host_compiler(),
+              "-Xcompiler", "-fPIC,-O2,-ffp-contract=off", "--expt-relaxed-constexpr"]
+    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(os.path.dirname(HERE), "include", "ntlp_gpu.h")]
+    objs = []
+    for unit, extra in UNITS.items():
+        src = os.path.join(CSRC, unit)
+        obj = os.path.join(BUILD, unit.replace(".cu", ".o"))
+        objs.append(obj)
+        if not force and _newer(obj, [src, *hdrs, __file__]):
+            continue
+        cmd = [nvcc(), *common, *extra, *inc, "-c", src, "-o", obj]
+        if ptxas_v:
+            cmd += ["-Xptxas", "-v"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0 or verbose or ptxas_v:
+            sys.stderr.write(r.stdout + r.stderr)
+        if r.returncode != 0:
+            raise RuntimeError(f"nvcc failed on {unit}")
+    if force or not _newer(LIB, objs):
+        cmd = [nvcc(), *ARCH, *host_compiler(), "-shared", "-cudart", "static", "-o", LIB, *objs]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError("link of libntlp_gpu.so failed")
+    return LIB
+
+
+if __name__ == "__main__":
+    build(verbose="--verbose" in sys.argv, force="--force" in sys.argv, ptxas_v="--ptxas" in sys.argv)
+    print(LIB)

@@ -1,0 +1,148 @@
+// ntlp_dev.cuh -- device-side descriptors and helpers of the droplet step.
+//
+// Layout in HBM (one "box" = one periodic domain with its own grid):
+//   fields  f(0:nnz+1, -1:nny+3, -1:nnx+3), z fastest, FP64 (and an FP32
+//           copy for the mixed path): the reference's uext layout
+//           (particles.f90:5-10).
+//   droplets structure of arrays, two buffers (A/B).  A step reads buffer
+//           `cur` through the permutation `perm` (cell-sorted order) and
+//           writes buffer 1-cur in that order, so the permutation costs no
+//           separate pass.
+//   cells   counting sort on the owning cell key
+//             key = kpt + (nnz+1)*((jpt-1) + (nny+1)*(ipt-1)),
+//           ipt in 1..nnx+1, jpt in 1..nny+1, kpt in 0..nnz (the deposition
+//           cell of particle_coupling_update, particles.f90:1180-1182);
+//           bucket ncells holds droplets whose key is out of range (counted
+//           in bad_index), bucket ncells+1 the killed droplets.
+//   sources (0:nnz+1, 1:nny, 1:nnx) per quantity after the periodic fold.
+#pragma once
+
+#include <cstdint>
+
+#include "ntlp_math.h"
+
+namespace ntlp {
+
+constexpr int kNumCounters = 8;
+enum Counter {
+    C_NUMPART = 0, C_DESTROY = 1, C_DENUM = 2, C_ACTNUM = 3,
+    C_NUM100 = 4, C_NUMIMPOS = 5, C_NEGQ = 6, C_BAD = 7
+};
+
+constexpr int kFluxLimbs = 6;        // fixed-point flux accumulators, 32-bit limbs
+constexpr int kFluxLsbExp = -128;    // value of the lowest limb's bit 0: 2^-128
+
+struct DevGrid {
+    int nnx, nny, nnz;
+    int nz2, ny5, nx5;     // nnz+2, nny+5, nnx+5
+    double dx, dy, xl, yl, zl;
+    const double *z, *zz, *dzw, *dzu;
+    long long ncells;      // (nnx+1)(nny+1)(nnz+1)
+    long long nnodes;      // (nnz+2)*nny*nnx
+};
+
+struct DevParams {
+    int ilin, icouple, iTcouple, iHcouple, ievap, iexner, icase, precision;
+    double nuf, Cpa, Cpp, Pra, Sc, Rd, rhow, rhos, Mw, Ru, Gam, Lv, Cpv, grav;
+    double g[3];
+    double radius_init, surf_rho, surf_p, tsfcc1, pi2;
+    // derived on the host once: Cpa/Cpp (les.F:10759), Sc**(1./3.), Pra**(1./3.)
+    double CpaCpp, Sc13, Pra13;
+};
+
+struct DevState {
+    double *x[3], *v[3], *Tp, *r, *m_s, *kap, *rc, *res, *actres, *numact;
+    long long *mult;
+    int *lid;
+    double *uf[3], *Tf, *qinf, *qstar;
+    double *vold[3], *Tpold, *rold;
+    double *xrhs[3], *vrhs[3], *Tprhs_s, *Tprhs_L, *radrhs;   // RK3 only
+};
+
+// Deposition payload of one droplet (written by the update kernel in the
+// output order, read by the deposition kernel through the cell lists).
+struct DevPayload {
+    double *D[3], *V[3], *T0, *H0, *E1, *E2, *mult;
+};
+
+struct DevBox {
+    DevGrid g;
+    const double *f[5];    // u v w T q, halo-padded FP64
+    const float *f32[5];   // FP32 copies (mixed path)
+    DevState st[2];
+    DevPayload pay;
+    int cur;               // buffer holding the current state
+    int cap;
+    int *n_alive;          // droplets in the current state
+    int *perm;             // [cap] perm[t] = index in st[cur] of the t-th droplet
+    int *key;              // [cap] new cell key of st[1-cur][t]
+    int *cell_cnt;         // [ncells+2]
+    int *cell_start;       // [ncells+3]
+    int *sorted;           // [cap] indices into st[1-cur], by cell then lid
+    long long *counters;   // [kNumCounters]
+    double *pflux;         // [nnz+1]
+    long long *flux_fx;    // [2][nnz+1][kFluxLimbs]
+    double *src[6];        // [nnodes] each, column layout
+    int *err;              // device error word (0 = fine)
+};
+
+// ---- binning ---------------------------------------------------------------
+// Fortran minloc(a, 1, mask=(a .gt. x)) on a strictly increasing a(0:n-1):
+// the 1-based position of the first element above x, 0 if there is none
+// (and for NaN x, where the mask is empty).  The context checks at creation
+// that z and zz increase strictly, which makes the binary search equal to
+// the reference's linear masked scan.
+__device__ __forceinline__ int minloc_gt(const double *a, int n, double x) {
+    if (!(x == x)) return 0;
+    int lo = 0, hi = n;            // first index with a[i] > x, in [0, n]
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (a[mid] > x) hi = mid; else lo = mid + 1;
+    }
+    return lo < n ? lo + 1 : 0;
+}
+
+// floor(x/d)+1 with an IEEE divide (particles.f90:571-572).
+__device__ __forceinline__ int ijpt(double x, double d) {
+    double q = floor(x / d);
+    if (!(q == q) || q < -1e9 || q > 1e9) return -1000000000;
+    return (int)q + 1;
+}
+
+// owning-cell key (ipt, jpt, kpt on the u levels); ncells for out-of-range
+__device__ __forceinline__ int cell_key(const DevGrid &g, double x1, double x2, double x3,
+                                        int *ipt_out = nullptr, int *jpt_out = nullptr,
+                                        int *kpt_out = nullptr) {
+    int ipt = ijpt(x1, g.dx);
+    int jpt = ijpt(x2, g.dy);
+    int kpt = minloc_gt(g.zz, g.nz2, x3) - 2;
+    if (ipt_out) { *ipt_out = ipt; *jpt_out = jpt; *kpt_out = kpt; }
+    if (ipt < 1 || ipt > g.nnx + 1 || jpt < 1 || jpt > g.nny + 1 || kpt < 0 || kpt > g.nnz)
+        return (int)g.ncells;
+    return kpt + (g.nnz + 1) * ((jpt - 1) + (g.nny + 1) * (ipt - 1));
+}
+
+// halo-padded field index f(k, j, i); i = nnx+4 (only named by the 6th-order
+// stencil of a droplet exactly at x == xl) is the periodic image i - nnx;
+// anything else outside the padded array is clamped and flagged.
+__device__ __forceinline__ long long ext_index(const DevGrid &g, int k, int j, int i, int &bad) {
+    if (i > g.nnx + 3) i -= g.nnx;
+    if (j > g.nny + 3) j -= g.nny;
+    if (k < 0 || k > g.nnz + 1 || j < -1 || j > g.nny + 3 || i < -1 || i > g.nnx + 3) {
+        bad = 1;
+        k = k < 0 ? 0 : (k > g.nnz + 1 ? g.nnz + 1 : k);
+        j = j < -1 ? -1 : (j > g.nny + 3 ? g.nny + 3 : j);
+        i = i < -1 ? -1 : (i > g.nnx + 3 ? g.nnx + 3 : i);
+    }
+    return (long long)k + (long long)g.nz2 * ((long long)(j + 1) + (long long)g.ny5 * (long long)(i + 1));
+}
+
+__device__ __forceinline__ double cube(double r) { return (r * r) * r; }
+
+// Tile of work: (box, first element); blocks map to tiles.
+struct Tile {
+    int box;
+    int start;
+};
+
+}  // namespace ntlp

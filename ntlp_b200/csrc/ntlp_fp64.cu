@@ -1,0 +1,462 @@
+// ntlp_fp64.cu -- FP64 droplet-step kernels in the reference's operation order.
+//
+// Compiled with --fmad=false: every add, multiply, divide and square root
+// rounds once, in the order of the Fortran expression it restates, and the
+// elementary functions come from ntlp_math.h, so a droplet advanced here is
+// bit-identical to the CPU restatement.  The restructuring is in what is
+// computed, not how: values the reference recomputes with identical inputs
+// (the Jacobian's base point, r-dependent terms of the T-perturbed residual,
+// per-droplet constants) are computed once, and results the reference
+// discards (v_output of ie_vrt_nd, the backward differences of
+// jacob_approx_2d, corrfac of the BE step) are not formed.
+#include <cuda_runtime.h>
+
+#include "ntlp_dev.cuh"
+#include "ntlp_kernels.h"
+#include "ntlp_physics.cuh"
+
+namespace ntlp {
+
+// ---------------------------------------------------------------------------
+// interpolation (particles.f90:554-847)
+// ---------------------------------------------------------------------------
+// uf_interp_lin, particles.f90:767-847
+__device__ void interp_lin64(const DevBox &B, double x1, double x2, double x3, Interp &o, int &bad) {
+    const DevGrid &g = B.g;
+    const double dx = g.dx, dy = g.dy;
+    int ipt = ijpt(x1, dx);
+    int jpt = ijpt(x2, dy);
+    int kpt = minloc_gt(g.zz, g.nz2, x3) - 2;
+    int kwpt = minloc_gt(g.z, g.nz2, x3) - 2;
+    if (kpt + 1 < 0 || kpt + 1 > g.nnz + 2 || kwpt + 1 < 0 || kwpt + 1 > g.nnz + 2) {
+        bad = 1;
+        kpt = kpt < -1 ? -1 : (kpt > g.nnz + 1 ? g.nnz + 1 : kpt);
+        kwpt = kwpt < -1 ? -1 : (kwpt > g.nnz + 1 ? g.nnz + 1 : kwpt);
+    }
+    // weights depend on one index each; the reference recomputes them in the
+    // innermost loop with the same operands
+    double wx[2], wy[2], wz[2], wzw[2];
+    for (int i = 0; i < 2; ++i) {
+        double xv = dx * (double)(i + ipt - 1);
+        wx[i] = (1.0 - fabs(x1 - xv) / dx);
+        double yv = dy * (double)(i + jpt - 1);
+        wy[i] = (1.0 - fabs(x2 - yv) / dy);
+        int kz = i + kpt, kzw = i + kwpt;
+        double zv = g.zz[kz < 0 ? 0 : (kz > g.nnz + 1 ? g.nnz + 1 : kz)];
+        double zwv = g.z[kzw < 0 ? 0 : (kzw > g.nnz + 1 ? g.nnz + 1 : kzw)];
+        wz[i] = (1.0 - fabs(x3 - zv) / g.dzu[kpt + 1]);
+        wzw[i] = (1.0 - fabs(x3 - zwv) / g.dzw[kwpt + 1]);
+    }
+    const double *fu = B.f[0], *fv = B.f[1], *fw = B.f[2], *fT = B.f[3], *fq = B.f[4];
+    double u1 = 0.0, u2 = 0.0, u3 = 0.0, T = 0.0, q = 0.0;
+    int ix = 0, iy = 0;
+    for (int i = 0; i <= 1; ++i) {
+        for (int j = 0; j <= 1; ++j) {
+            for (int k = 0; k <= 1; ++k) {
+                ix = ipt + i;
+                iy = jpt + j;
+                long long a = ext_index(g, kpt + k, iy, ix, bad);
+                long long aw = ext_index(g, kwpt + k, iy, ix, bad);
+                u1 = u1 + __ldg(fu + a) * wx[i] * wy[j] * wz[k];
+                u2 = u2 + __ldg(fv + a) * wx[i] * wy[j] * wz[k];
+                u3 = u3 + __ldg(fw + aw) * wx[i] * wy[j] * wzw[k];
+                T = T + __ldg(fT + a) * wx[i] * wy[j] * wz[k];
+                q = q + __ldg(fq + a) * wx[i] * wy[j] * wz[k];
+            }
+            if (kpt == g.nnz) {
+                long long a = ext_index(g, kpt, iy, ix, bad);
+                u1 = __ldg(fu + a); u2 = __ldg(fv + a); T = __ldg(fT + a); q = __ldg(fq + a);
+            }
+            if (kpt == 0) {
+                long long a = ext_index(g, 1, iy, ix, bad);
+                u1 = __ldg(fu + a); u2 = __ldg(fv + a); T = __ldg(fT + a); q = __ldg(fq + a);
+            }
+        }
+    }
+    o.uf[0] = u1; o.uf[1] = u2; o.uf[2] = u3; o.Tf = T; o.qinf = q;
+}
+
+// Lagrange weights over 6 nodes (particles.f90:612-624 and 682-689):
+// w_j = prod_{k != j} (x - x_k)/(x_j - x_k), evaluated left to right.
+__device__ __forceinline__ void lagrange6(double x, const double xn[6], int first, int last, double w[6]) {
+    for (int j = 0; j < 6; ++j) w[j] = 0.0;
+    for (int j = first; j <= last && first > 0; ++j) {
+        double xj = xn[j - 1];
+        double pj = 1.0;
+        for (int k = first; k <= last; ++k)
+            if (j != k) pj = pj * (x - xn[k - 1]) / (xj - xn[k - 1]);
+        w[j - 1] = pj;
+    }
+}
+
+// uf_interp, particles.f90:554-765
+__device__ void interp6_64(const DevBox &B, double x1, double x2, double x3, Interp &o, int &bad) {
+    const DevGrid &g = B.g;
+    const int nnz = g.nnz;
+    int ip3 = ijpt(x1, g.dx), jp3 = ijpt(x2, g.dy);
+    int ku[6], kw[6];
+    ku[2] = minloc_gt(g.zz, g.nz2, x3) - 2;
+    kw[2] = minloc_gt(g.z, g.nz2, x3) - 2;
+    for (int a = 0; a < 6; ++a) { ku[a] = ku[2] + (a - 2); kw[a] = kw[2] + (a - 2); }
+    double wx[6], wy[6], wz[6], wzw[6];
+    {
+        double xn[6], yn[6];
+        for (int a = 0; a < 6; ++a) {
+            xn[a] = g.dx * (double)(ip3 + (a - 2) - 1);
+            yn[a] = g.dy * (double)(jp3 + (a - 2) - 1);
+        }
+        lagrange6(x1, xn, 1, 6, wx);
+        lagrange6(x2, yn, 1, 6, wy);
+    }
+    int first, last;
+    // u levels (particles.f90:635-676)
+    if (ku[2] == 1) { first = 3; last = 4; ku[0] = 1; ku[1] = 1; }
+    else if (ku[2] == 0) { first = 4; last = 5; ku[0] = 1; ku[1] = 1; ku[2] = 1; }
+    else if (ku[2] < 0) { first = 0; last = 0; }
+    else if (ku[2] == 2) { first = 2; last = 5; }
+    else if (ku[2] == nnz) { first = 2; last = 3; ku[3] = nnz; ku[4] = nnz; ku[5] = nnz; }
+    else if (ku[2] > nnz) { first = 0; last = 0; }
+    else if (ku[2] == nnz - 1) { first = 3; last = 4; ku[4] = nnz; ku[5] = nnz; }
+    else if (ku[2] == nnz - 2) { first = 2; last = 5; }
+    else { first = 1; last = 6; }
+    {
+        double zn[6];
+        for (int a = 0; a < 6; ++a) {
+            int kk = ku[a] < 0 ? 0 : (ku[a] > nnz + 1 ? nnz + 1 : ku[a]);
+            zn[a] = g.zz[kk];
+        }
+        lagrange6(x3, zn, first, last, wz);
+    }
+    // w levels (particles.f90:694-728)
+    if (kw[2] == 0) { first = 3; last = 4; kw[0] = 1; kw[1] = 1; }
+    else if (kw[2] < 0) { first = 0; last = 0; kw[0] = 1; kw[1] = 1; kw[2] = 1; }
+    else if (kw[2] == 1) { first = 2; last = 5; kw[0] = 1; }
+    else if (kw[2] == nnz - 1) { first = 3; last = 4; kw[4] = nnz; kw[5] = nnz; }
+    else if (kw[2] >= nnz) { first = 0; last = 0; kw[2] = nnz; kw[3] = nnz; kw[4] = nnz; kw[5] = nnz; }
+    else if (kw[2] == nnz - 2) { first = 2; last = 5; kw[5] = nnz; }
+    else { first = 1; last = 6; }
+    {
+        double zn[6];
+        for (int a = 0; a < 6; ++a) {
+            int kk = kw[a] < 0 ? 0 : (kw[a] > nnz + 1 ? nnz + 1 : kw[a]);
+            zn[a] = g.z[kk];
+        }
+        lagrange6(x3, zn, first, last, wzw);
+    }
+    const double *fu = B.f[0], *fv = B.f[1], *fw = B.f[2], *fT = B.f[3], *fq = B.f[4];
+    double u1 = 0.0, u2 = 0.0, u3 = 0.0, T = 0.0, q = 0.0;
+    for (int k = 0; k < 6; ++k) {
+        const int izuv = ku[k], izw = kw[k];
+        const double wk = wz[k], wkw = wzw[k];
+        for (int j = 0; j < 6; ++j) {
+            const int iy = jp3 + (j - 2);
+            const double wj = wy[j];
+            for (int i = 0; i < 6; ++i) {
+                const int ix = ip3 + (i - 2);
+                const double wi = wx[i];
+                long long a = ext_index(g, izuv, iy, ix, bad);
+                long long aw = ext_index(g, izw, iy, ix, bad);
+                u1 = u1 + __ldg(fu + a) * wi * wj * wk;
+                u2 = u2 + __ldg(fv + a) * wi * wj * wk;
+                u3 = u3 + __ldg(fw + aw) * wi * wj * wkw;
+                T = T + __ldg(fT + a) * wi * wj * wk;
+                q = q + __ldg(fq + a) * wi * wj * wk;
+            }
+        }
+    }
+    o.uf[0] = u1; o.uf[1] = u2; o.uf[2] = u3; o.Tf = T; o.qinf = q;
+}
+
+// ---------------------------------------------------------------------------
+// backward-Euler droplet update (particles.f90:3043-3242, 3248-3260)
+// ---------------------------------------------------------------------------
+template <int ILIN>
+__global__ void __launch_bounds__(kUpdateThreads)
+k_update_be64(DevBox *boxes, const Tile *tiles, const DevParams *pp, StepIn in) {
+    const Tile tl = tiles[blockIdx.x];
+    const DevBox &B = boxes[tl.box];
+    const DevParams &p = pp[0];
+    Counts cnt;
+    for (int k = 0; k < kNumCounters; ++k) cnt.v[k] = 0;
+    const int t = tl.start + threadIdx.x;
+    if (t < *B.n_alive) {
+        const DevState &S = B.st[B.cur];
+        const int s = B.perm[t];
+        double x[3] = {S.x[0][s], S.x[1][s], S.x[2][s]};
+        Interp I;
+        int bad = 0;
+        if (ILIN == 1) interp_lin64(B, x[0], x[1], x[2], I, bad);
+        else interp6_64(B, x[0], x[1], x[2], I, bad);
+        be_body<false>(B, p, in, t, s, x, I, bad, cnt);
+    }
+    block_add_counters(B, cnt);
+}
+
+// ---------------------------------------------------------------------------
+// RK3 stage (particles.f90:2845-2998), coefficients les.F:856-861
+// ---------------------------------------------------------------------------
+template <int ILIN>
+__global__ void __launch_bounds__(kUpdateThreads)
+k_update_rk3_64(DevBox *boxes, const Tile *tiles, const DevParams *pp, StepIn in) {
+    const Tile tl = tiles[blockIdx.x];
+    const DevBox &B = boxes[tl.box];
+    const DevParams &p = pp[0];
+    Counts cnt;
+    for (int k = 0; k < kNumCounters; ++k) cnt.v[k] = 0;
+    const int t = tl.start + threadIdx.x;
+    const int n = *B.n_alive;
+    if (t < n) {
+        const double zetas[3] = {0.0, -17.0 / 60.0, -5.0 / 12.0};
+        const double gama[3] = {8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0};
+        const double zs = zetas[in.istage - 1], ga = gama[in.istage - 1];
+        const DevState &S = B.st[B.cur];
+        const DevState &O = B.st[1 - B.cur];
+        const int s = B.perm[t];
+        const double dt = in.dt;
+        double x[3], v[3], vold[3], xrhs[3], vrhs[3];
+        for (int a = 0; a < 3; ++a) {
+            x[a] = S.x[a][s]; v[a] = S.v[a][s];
+            xrhs[a] = S.xrhs[a][s]; vrhs[a] = S.vrhs[a][s];
+        }
+        double Tp = S.Tp[s], radius = S.r[s];
+        double Tpold, rold;
+        if (in.istage == 1) {
+            for (int a = 0; a < 3; ++a) vold[a] = v[a];
+            Tpold = Tp;
+            rold = radius;
+        } else {
+            for (int a = 0; a < 3; ++a) vold[a] = S.vold[a][s];
+            Tpold = S.Tpold[s];
+            rold = S.rold[s];
+        }
+        const double m_s = S.m_s[s], kap = S.kap[s];
+        double res = S.res[s];
+        double Tprhs_s = S.Tprhs_s[s], Tprhs_L = S.Tprhs_L[s], radrhs = S.radrhs[s];
+        const long long multi = S.mult[s];
+
+        Interp I;
+        int bad = 0;
+        if (ILIN == 1) interp_lin64(B, x[0], x[1], x[2], I, bad);
+        else interp6_64(B, x[0], x[1], x[2], I, bad);
+        double Tf = I.Tf, qinf = I.qinf, rhoa;
+        if (p.iexner == 1) {
+            Tf = Tf * exner64(p, p.surf_p, func_p_base64(p, p.surf_p, p.tsfcc1, x[2]));
+            rhoa = func_p_base64(p, p.surf_p, p.tsfcc1, x[2]) / p.Rd / Tf;
+        } else {
+            rhoa = p.surf_rho;
+        }
+        if (qinf < 0.0) cnt.v[C_NEGQ]++;
+        if (in.it <= 1) {
+            for (int a = 0; a < 3; ++a) v[a] = I.uf[a];
+            Tp = Tf;
+        }
+        double d0 = v[0] - I.uf[0], d1 = v[1] - I.uf[1], d2 = v[2] - I.uf[2];
+        double diffnorm = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+        double Rep = 2.0 * radius * diffnorm / p.nuf;
+        double Volp = p.pi2 * 2.0 / 3.0 * cube(radius);
+        double rhop = (m_s + Volp * p.rhow) / Volp;
+        double taup_i = 18.0 * rhoa * p.nuf / rhop / ((2.0 * radius) * (2.0 * radius));
+        double corrfac = (1.0 + 0.15 * ntlp_pow(Rep, 0.687));
+        double Nup = 2.0 + 0.6 * sqrt(Rep) * p.Pra13;
+        double Shp = 2.0 + 0.6 * sqrt(Rep) * p.Sc13;
+        double einf = mod_magnus64(Tf);
+        double Eff_C = 2.0 * p.Mw * p.Gam / (p.Ru * p.rhow * radius * Tp);
+        double Eff_S = kap * m_s * p.rhow / p.rhos / (Volp * rhop - m_s);
+        double estar = einf * ntlp_exp(p.Mw * p.Lv / p.Ru * (1.0 / Tf - 1.0 / Tp) + Eff_C - Eff_S);
+        double qstar = p.Mw / p.Ru * estar / Tp / rhoa;
+        double xtmp[3], vtmp[3];
+        for (int a = 0; a < 3; ++a) xtmp[a] = x[a] + dt * zs * xrhs[a];
+        for (int a = 0; a < 3; ++a) vtmp[a] = v[a] + dt * zs * vrhs[a];
+        double Tptmp = Tp + dt * zs * Tprhs_s;
+        Tptmp = Tptmp + dt * zs * Tprhs_L;
+        double radiustmp = radius + dt * zs * radrhs;
+        for (int a = 0; a < 3; ++a) xrhs[a] = v[a];
+        for (int a = 0; a < 3; ++a) vrhs[a] = corrfac * taup_i * (I.uf[a] - v[a]) + p.g[a];
+        if (p.ievap == 1)
+            radrhs = Shp / 9.0 / p.Sc * rhop / p.rhow * radius * taup_i * (qinf - qstar);
+        else
+            radrhs = 0.0;
+        Tprhs_s = -Nup / 3.0 / p.Pra * p.CpaCpp * rhop / p.rhow * taup_i * (Tp - Tf);
+        Tprhs_L = 3.0 * p.Lv / p.Cpp / radius * radrhs;
+        for (int a = 0; a < 3; ++a) x[a] = xtmp[a] + dt * ga * xrhs[a];
+        for (int a = 0; a < 3; ++a) v[a] = vtmp[a] + dt * ga * vrhs[a];
+        Tp = Tptmp + dt * ga * Tprhs_s;
+        Tp = Tp + dt * ga * Tprhs_L;
+        radius = radiustmp + dt * ga * radrhs;
+        if (in.istage == 3) res = res + dt;
+
+        const int alive = apply_bcs(B, p, x, v, radius);
+        if (bad) cnt.v[C_BAD]++;
+        for (int a = 0; a < 3; ++a) {
+            O.x[a][t] = x[a]; O.v[a][t] = v[a]; O.uf[a][t] = I.uf[a]; O.vold[a][t] = vold[a];
+            O.xrhs[a][t] = xrhs[a]; O.vrhs[a][t] = vrhs[a];
+        }
+        O.Tp[t] = Tp; O.r[t] = radius; O.m_s[t] = m_s; O.kap[t] = kap; O.rc[t] = S.rc[s];
+        O.res[t] = res; O.actres[t] = S.actres[s]; O.numact[t] = S.numact[s]; O.mult[t] = multi;
+        O.lid[t] = S.lid[s];
+        O.Tf[t] = Tf; O.qinf[t] = qinf; O.qstar[t] = qstar; O.Tpold[t] = Tpold; O.rold[t] = rold;
+        O.Tprhs_s[t] = Tprhs_s; O.Tprhs_L[t] = Tprhs_L; O.radrhs[t] = radrhs;
+        int key;
+        if (!alive) {
+            key = (int)B.g.ncells + 1;
+            cnt.v[C_DESTROY]++;
+        } else {
+            key = cell_key(B.g, x[0], x[1], x[2]);
+            if (in.write_payload)
+                write_payload(B, p, t, x, v, vold, radius, rold, Tp, Tpold, Tf, m_s, multi, dt);
+        }
+        B.key[t] = key;
+    }
+    block_add_counters(B, cnt);
+}
+
+// Payload from the stored state, for a coupling call whose dt differs from
+// the step's.  Runs after the finish kernel: st[cur] is the new state and
+// the payload is indexed like it.
+__global__ void k_payload64(DevBox *boxes, const Tile *tiles, const DevParams *pp, double dt) {
+    const Tile tl = tiles[blockIdx.x];
+    const DevBox &B = boxes[tl.box];
+    const DevParams &p = pp[0];
+    const int t = tl.start + threadIdx.x;
+    if (t >= *B.n_alive) return;
+    const DevState &S = B.st[B.cur];
+    const int s = B.perm[t];
+    double x[3], v[3], vold[3];
+    for (int a = 0; a < 3; ++a) { x[a] = S.x[a][s]; v[a] = S.v[a][s]; vold[a] = S.vold[a][s]; }
+    write_payload(B, p, s, x, v, vold, S.r[s], S.rold[s], S.Tp[s], S.Tpold[s], S.Tf[s], S.m_s[s], S.mult[s], dt);
+}
+
+// ---------------------------------------------------------------------------
+// deterministic deposition (particles.f90:1151-1276 + fold :1078-1113)
+// ---------------------------------------------------------------------------
+// One thread per output node.  The node's value is the reference's: the
+// sum, in list order (ascending lid), of the contributions of the droplets
+// in its (up to) 8 neighbouring cells at each of its pre-fold images
+// (ix, iy), (ix+nnx, iy), (ix, iy+nny), (ix+nnx, iy+nny), combined in the
+// order of the periodic fold.  Cell lists are lid-sorted, so each image is
+// an 8-way merge.
+struct Acc {
+    double s[6];
+};
+
+__device__ __forceinline__ void deposit_image(const DevBox &B, const DevParams &p, int px, int py, int pz,
+                                              Acc &acc) {
+    const DevGrid &g = B.g;
+    for (int q = 0; q < 6; ++q) acc.s[q] = 0.0;
+    int pos[8], end[8], head[8], ck[8];
+    int ncur = 0;
+    for (int i = 0; i <= 1; ++i)
+        for (int j = 0; j <= 1; ++j)
+            for (int k = 0; k <= 1; ++k) {
+                int ci = px - i, cj = py - j, ckk = pz - k;
+                if (ci < 1 || ci > g.nnx + 1 || cj < 1 || cj > g.nny + 1 || ckk < 0 || ckk > g.nnz) continue;
+                int key = ckk + (g.nnz + 1) * ((cj - 1) + (g.nny + 1) * (ci - 1));
+                int a = B.cell_start[key], b = B.cell_start[key + 1];
+                if (a < b) {
+                    pos[ncur] = a;
+                    end[ncur] = b;
+                    ck[ncur] = ckk;
+                    ncur++;
+                }
+            }
+    if (ncur == 0) return;
+    const DevState &O = B.st[B.cur];   // after the finish kernel: the new state, cell lists in perm
+    for (int c = 0; c < ncur; ++c) head[c] = O.lid[B.perm[pos[c]]];
+    const double dx = g.dx, dy = g.dy;
+    const double xv = dx * (double)(px - 1);
+    const double yv = dy * (double)(py - 1);
+    const double zv = g.zz[pz];
+    const DevPayload &P = B.pay;
+    while (true) {
+        int best = -1, bl = 0x7fffffff;
+        for (int c = 0; c < ncur; ++c)
+            if (pos[c] < end[c] && head[c] < bl) { bl = head[c]; best = c; }
+        if (best < 0) break;
+        const int t = B.perm[pos[best]];
+        const int kpt = ck[best];
+        pos[best]++;
+        if (pos[best] < end[best]) head[best] = O.lid[B.perm[pos[best]]];
+        const double x1 = O.x[0][t], x2 = O.x[1][t], x3 = O.x[2][t];
+        const double wtx = (1.0 - fabs(x1 - xv) / dx);
+        const double wty = (1.0 - fabs(x2 - yv) / dy);
+        const double wtz = (1.0 - fabs(x3 - zv) / g.dzu[kpt + 1]);
+        const double wtt = wtx * wty * wtz;
+        const double dV = dx * dy * g.dzu[kpt + 1];
+        const double mult = P.mult[t];
+        if (p.icouple == 1) {
+            for (int a = 0; a < 3; ++a) {
+                acc.s[a] = acc.s[a] - P.D[a][t] * wtt / dV * mult;
+                acc.s[a] = acc.s[a] - P.V[a][t] * wtt / dV * mult;
+            }
+        }
+        if (p.iTcouple == 1) acc.s[3] = acc.s[3] - P.T0[t] * wtt / dV * mult;
+        if (p.iHcouple == 1) {
+            acc.s[4] = acc.s[4] - P.H0[t] * wtt / dV * mult;
+            acc.s[5] = acc.s[5] - P.E1[t] * wtt / dV * mult + P.E2[t] * wtt / dV * mult;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kDepositThreads)
+k_deposit64(DevBox *boxes, const Tile *tiles, const DevParams *pp) {
+    const Tile tl = tiles[blockIdx.x];
+    const DevBox &B = boxes[tl.box];
+    const DevParams &p = pp[0];
+    const long long node = (long long)tl.start + threadIdx.x;
+    const DevGrid &g = B.g;
+    if (node >= g.nnodes) return;
+    const int iz = (int)(node % g.nz2);
+    const long long rest = node / g.nz2;
+    const int iy = (int)(rest % g.nny) + 1;
+    const int ix = (int)(rest / g.nny) + 1;
+    Acc a0, a1;
+    deposit_image(B, p, ix, iy, iz, a0);
+    if (ix <= 2) {
+        deposit_image(B, p, ix + g.nnx, iy, iz, a1);
+        for (int q = 0; q < 6; ++q) a0.s[q] = a0.s[q] + a1.s[q];
+    }
+    if (iy <= 2) {
+        Acc b0;
+        deposit_image(B, p, ix, iy + g.nny, iz, b0);
+        if (ix <= 2) {
+            deposit_image(B, p, ix + g.nnx, iy + g.nny, iz, a1);
+            for (int q = 0; q < 6; ++q) b0.s[q] = b0.s[q] + a1.s[q];
+        }
+        for (int q = 0; q < 6; ++q) a0.s[q] = a0.s[q] + b0.s[q];
+    }
+    for (int q = 0; q < 6; ++q) B.src[q][node] = a0.s[q];
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+void launch_update_be64(int ilin, DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp,
+                        StepIn in, cudaStream_t st) {
+    if (ntiles <= 0) return;
+    if (ilin == 1)
+        k_update_be64<1><<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles, pp, in);
+    else
+        k_update_be64<0><<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles, pp, in);
+}
+
+void launch_update_rk3_64(int ilin, DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp,
+                          StepIn in, cudaStream_t st) {
+    if (ntiles <= 0) return;
+    if (ilin == 1)
+        k_update_rk3_64<1><<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles, pp, in);
+    else
+        k_update_rk3_64<0><<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles, pp, in);
+}
+
+void launch_payload64(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp, double dt,
+                      cudaStream_t st) {
+    if (ntiles <= 0) return;
+    k_payload64<<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles, pp, dt);
+}
+
+void launch_deposit64(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp, cudaStream_t st) {
+    if (ntiles <= 0) return;
+    k_deposit64<<<ntiles, kDepositThreads, 0, st>>>(boxes, tiles, pp);
+}
+
+}  // namespace ntlp

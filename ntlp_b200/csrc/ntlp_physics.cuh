@@ -1,0 +1,519 @@
+// ntlp_physics.cuh -- per-droplet physics of the droplet step, shared by the
+// FP64 kernels (compiled with --fmad=false: reference rounding) and the
+// mixed-precision kernels (contraction allowed).
+//
+// Residual and solvers: ie_vrt_nd, jacob_approx_2d, gauss_newton_2d,
+// LV_solver, rad_solver2 (particles.f90:4071-4371); thermodynamic helpers
+// mod_magnus, exner, func_p_base (les.F:10764-10795); boundaries
+// (particles.f90:2683-2843); the deposition payload (particles.f90:1186-1264)
+// and the backward-Euler droplet body (particles.f90:3043-3242).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "ntlp_dev.cuh"
+#include "ntlp_kernels.h"
+
+namespace ntlp {
+namespace {
+
+struct Interp {
+    double uf[3], Tf, qinf;
+};
+
+// ---------------------------------------------------------------------------
+// thermodynamics (les.F:10764-10795)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double mod_magnus64(double T) {
+    return 610.94 * ntlp_exp((17.6257 * (T - 273.15)) / (243.04 + (T - 273.15)));
+}
+__device__ __forceinline__ double func_p_base64(const DevParams &p, double p_surf, double T_surf, double z) {
+    return p_surf * ntlp_pow(1.0 - ((z * p.grav) / p.Cpa) / T_surf, p.Cpa / p.Rd);
+}
+__device__ __forceinline__ double exner64(const DevParams &p, double p0, double pz) {
+    return ntlp_pow(p0 / pz, -p.Rd / p.Cpa);
+}
+
+// ---------------------------------------------------------------------------
+// radius/temperature residual and solvers (particles.f90:4071-4371)
+// ---------------------------------------------------------------------------
+struct Drop {
+    double Tf, qinf, m_s, radius, Tp, rhoa, h;
+    double diffnorm;             // |uf - vnext|
+    double esa;                  // mod_magnus(Tf)
+    double taup0;
+    double inv_Tf;               // 1./Tf
+    double c_taup;               // 18.0*rhoa*nuf
+    double c_sol;                // kappa_s*m_s*rhow/rhos
+    double t0r, rt0, t0T;        // taup0/radius, radius/taup0, taup0/Tp
+};
+
+// ie_vrt_nd split in its r-dependent and T-dependent parts; the evaluation
+// order of every expression is the reference's.
+struct RPart {
+    double rnext, rhop, taup, rpre, tpre, clat, rdr, ruwr, solterm;
+};
+
+__device__ __forceinline__ void rpart(const DevParams &p, const Drop &d, double tempr, RPart &r) {
+    double rnext = tempr * d.radius;
+    double dnext = rnext * 2.0;
+    double VolP = (2.0 / 3.0) * p.pi2 * cube(rnext);
+    double rhop = (d.m_s + VolP * p.rhow) / VolP;
+    double Rep = dnext * d.diffnorm / p.nuf;
+    double taup = (rhop * (dnext * dnext)) / d.c_taup;
+    double sRep = sqrt(Rep);
+    double Shp = 2.0 + 0.6 * sRep * p.Sc13;
+    double Nup = 2.0 + 0.6 * sRep * p.Pra13;
+    r.rnext = rnext;
+    r.rhop = rhop;
+    r.taup = taup;
+    r.rpre = (1.0 / 9.0) * (Shp / p.Sc) * (rhop / p.rhow) * (rnext / taup);
+    r.tpre = -(1.0 / 3.0) * (Nup / p.Pra) * p.CpaCpp * (rhop / p.rhow) * (1.0 / taup);
+    r.clat = 3.0 * p.Lv * (1.0 / (rnext * p.Cpp));
+    r.rdr = rnext / d.radius - 1.0;
+    r.ruwr = p.Ru * p.rhow * rnext;
+    r.solterm = (d.c_sol / (VolP * rhop - d.m_s));
+}
+
+__device__ __forceinline__ void tpart(const DevParams &p, const Drop &d, const RPart &r, double tempt,
+                                      double out[2]) {
+    double Tnext = tempt * d.Tp;
+    double qstr = (p.Mw / (p.Ru * Tnext * d.rhoa)) * d.esa *
+                  ntlp_exp(((p.Lv * p.Mw / p.Ru) * (d.inv_Tf - (1.0 / Tnext))) +
+                           ((2.0 * p.Mw * p.Gam) / (r.ruwr * Tnext)) - r.solterm);
+    double rprime = r.rpre * (d.qinf - qstr);
+    rprime = rprime * d.t0r;
+    double Tprime = r.tpre * (Tnext - d.Tf) + r.clat * rprime * d.rt0;
+    Tprime = Tprime * d.t0T;
+    out[0] = r.rdr - d.h * rprime;
+    out[1] = Tnext / d.Tp - 1.0 - d.h * Tprime;
+}
+
+// residual at (a, b) and the one-sided Jacobian (jacob_approx_2d)
+__device__ __forceinline__ void resid_jac(const DevParams &p, const Drop &d, double a, double b,
+                                          double f0[2], double J[4]) {
+    const double diff = 1e-12;
+    RPart r0, r1;
+    double fr[2], ft[2];
+    rpart(p, d, a, r0);
+    tpart(p, d, r0, b, f0);
+    rpart(p, d, a + diff, r1);
+    tpart(p, d, r1, b, fr);
+    tpart(p, d, r0, b + diff, ft);
+    J[0] = (fr[0] - f0[0]) / diff;   // J(1,1)
+    J[1] = (fr[1] - f0[1]) / diff;   // J(2,1)
+    J[2] = (ft[0] - f0[0]) / diff;   // J(1,2)
+    J[3] = (ft[1] - f0[1]) / diff;   // J(2,2)
+}
+
+__device__ __forceinline__ void resid(const DevParams &p, const Drop &d, double a, double b, double f[2]) {
+    RPart r0;
+    rpart(p, d, a, r0);
+    tpart(p, d, r0, b, f);
+}
+
+// gauss_newton_2d, particles.f90:4071-4142
+__device__ int gauss_newton64(const DevParams &p, const Drop &d, const double vec1[2], double vec2[2]) {
+    int iterations = 0, flag = 0;
+    double v1a = vec1[0], v1b = vec1[1];
+    vec2[0] = 0.0;
+    vec2[1] = 0.0;
+    while (iterations < 50) {
+        iterations++;
+        double fv1[2], J[4];
+        resid_jac(p, d, v1a, v1b, fv1, J);
+        // fancy = transpose(J) J  (column-major J: J(1,1)=J[0] J(2,1)=J[1] J(1,2)=J[2] J(2,2)=J[3])
+        double f11 = J[0] * J[0] + J[1] * J[1];
+        double f21 = J[2] * J[0] + J[3] * J[1];
+        double f12 = J[0] * J[2] + J[1] * J[3];
+        double f22 = J[2] * J[2] + J[3] * J[3];
+        double det = f11 * f22 - f12 * f21;
+        if (fabs(det) < 1.0e-10) { flag = 1; break; }
+        double rd = 1.0 / det;
+        double i11 = rd * f22, i21 = rd * (-f21), i12 = rd * (-f12), i22 = rd * f11;
+        // finalJ = inv transpose(J)
+        double g11 = i11 * J[0] + i12 * J[2];
+        double g12 = i11 * J[1] + i12 * J[3];
+        double g21 = i21 * J[0] + i22 * J[2];
+        double g22 = i21 * J[1] + i22 * J[3];
+        double c1 = g11 * fv1[0] + g12 * fv1[1];
+        double c2 = g21 * fv1[0] + g22 * fv1[1];
+        vec2[0] = v1a - c1;
+        vec2[1] = v1b - c2;
+        int counts = 0;
+        double relax = 1.0;
+        while ((vec2[0] < 0) || (vec2[1] < 0) || ntlp_isnan(vec2[0])) {
+            counts++;
+            relax = relax * 0.5;
+            vec2[0] = v1a - c1 * relax;
+            vec2[1] = v1b - c2 * relax;
+            if (counts > 10) break;
+        }
+        if (vec2[0] < 0.01 || vec2[1] < 0.01 || ntlp_isnan(vec2[0]) || ntlp_isnan(vec2[1])) { flag = 1; break; }
+        if (sqrt(c1 * c1 + c2 * c2) < 1.0e-8) break;
+        v1a = vec2[0];
+        v1b = vec2[1];
+    }
+    if (iterations == 50) flag = 1;
+    if (ntlp_isnan(vec2[0]) || vec2[0] < 0 || ntlp_isnan(vec2[1]) || vec2[1] < 0) flag = 1;
+    return flag;
+}
+
+// LV_solver, particles.f90:4143-4223
+__device__ int lv_solver64(const DevParams &p, const Drop &d, const double vec1[2], double vec2[2]) {
+    int iterations = 0, flag = 0;
+    double v1a = vec1[0], v1b = vec1[1];
+    double lambda = 0.001;
+    while (iterations < 1000) {
+        iterations++;
+        double fv1[2], J[4], fv2[2];
+        resid_jac(p, d, v1a, v1b, fv1, J);
+        double g11 = (J[0] * J[0] + J[1] * J[1]) + lambda * 1.0;
+        double g21 = (J[2] * J[0] + J[3] * J[1]) + lambda * 0.0;
+        double g12 = (J[0] * J[2] + J[1] * J[3]) + lambda * 0.0;
+        double g22 = (J[2] * J[2] + J[3] * J[3]) + lambda * 1.0;
+        double gc1 = J[0] * fv1[0] + J[1] * fv1[1];
+        double gc2 = J[2] * fv1[0] + J[3] * fv1[1];
+        double C1 = 0.5 * fv1[0] * fv1[0];
+        double C2 = 0.5 * fv1[1] * fv1[1];
+        double det = g11 * g22 - g12 * g21;
+        if (fabs(det) < 1.0e-10) { flag = 1; break; }
+        double rd = 1.0 / det;
+        double i11 = rd * g22, i21 = rd * (-g21), i12 = rd * (-g12), i22 = rd * g11;
+        double c1 = i11 * gc1 + i12 * gc2;
+        double c2 = i21 * gc1 + i22 * gc2;
+        vec2[0] = v1a - c1;
+        vec2[1] = v1b - c2;
+        if (sqrt(c1 * c1 + c2 * c2) < 1.0e-8) break;
+        if (vec2[0] < 0.0 || vec2[1] < 0.0 || ntlp_isnan(vec2[0]) || ntlp_isnan(vec2[1])) { flag = 1; break; }
+        resid(p, d, vec2[0], vec2[1], fv2);
+        double n1 = 0.5 * fv2[0] * fv2[0];
+        double n2 = 0.5 * fv2[1] * fv2[1];
+        if (sqrt(n1 * n1 + n2 * n2) < sqrt(C1 * C1 + C2 * C2)) {
+            v1a = vec2[0];
+            v1b = vec2[1];
+            lambda = lambda / 2.0;
+        } else {
+            lambda = lambda * 2.0;
+        }
+    }
+    if (iterations == 1000) flag = 1;
+    if (vec2[0] < 0 || vec2[1] < 0) flag = 1;
+    return flag;
+}
+
+// rad_solver2, particles.f90:4328-4371
+__device__ double rad_solver2_64(const DevParams &p, double Tf, double qinf, double rhoa, double m_s,
+                                 double kap, double radius, double esa, int &mflag) {
+    mflag = 0;
+    double lg = ntlp_log((p.Ru * Tf * rhoa * qinf) / (p.Mw * esa));
+    double a = -(2.0 * p.Mw * p.Gam) / (p.Ru * p.rhow * Tf) / lg;
+    double c = (kap * m_s) / ((2.0 / 3.0) * p.pi2 * p.rhos) / lg;
+    double Q = (a * a) / 9.0;
+    double R = (2.0 * cube(a) + 27.0 * c) / 54.0;
+    double M = R * R - cube(Q);
+    double guess;
+    if (M < 0) {
+        double theta = ntlp_acos(R / sqrt(cube(Q)));
+        guess = -(2.0 * sqrt(Q) * ntlp_cos((theta - p.pi2) / 3.0)) - a / 3.0;
+        if (guess < 0) guess = -(2.0 * sqrt(Q) * ntlp_cos((theta + p.pi2) / 3.0)) - a / 3.0;
+    } else {
+        double S = -(R / fabs(R)) * ntlp_pow(fabs(R) + sqrt(M), 1.0 / 3.0);
+        double T = Q / S;
+        guess = S + T - a / 3.0;
+        if (guess < 0) {
+            guess = radius;
+            mflag = 1;
+        }
+    }
+    return guess;
+}
+
+__device__ __forceinline__ double taup0_64(const DevParams &p, double m_s, double rhoa) {
+    double ri = p.radius_init;
+    double num = ((m_s) / ((2.0 / 3.0) * p.pi2 * cube(ri)) + p.rhow) * ((ri * 2.0) * (ri * 2.0));
+    return num / (18.0 * rhoa * p.nuf);
+}
+
+// ---------------------------------------------------------------------------
+// shared pieces of the update kernels
+// ---------------------------------------------------------------------------
+struct Counts {
+    int v[kNumCounters];
+};
+
+__device__ __forceinline__ void block_add_counters(const DevBox &B, const Counts &c) {
+    __shared__ int sh[kNumCounters];
+    if (threadIdx.x < kNumCounters) sh[threadIdx.x] = 0;
+    __syncthreads();
+    for (int k = 0; k < kNumCounters; ++k) {
+        int v = c.v[k];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0 && v) atomicAdd(&sh[k], v);
+    }
+    __syncthreads();
+    if (threadIdx.x < kNumCounters && sh[threadIdx.x])
+        atomicAdd((unsigned long long *)&B.counters[threadIdx.x], (unsigned long long)(long long)sh[threadIdx.x]);
+}
+
+// Exact fixed-point accumulation of a double into 32-bit limbs held in
+// 64-bit integers (bit 0 of limb 0 is worth 2^-128).  Integer addition is
+// associative, so the tally does not depend on the order droplets arrive in.
+__device__ __forceinline__ void fx_add(long long *limbs, double v) {
+    if (v == 0.0 || !(v == v)) return;
+    uint64_t u = ntlp_bits(v);
+    int neg = (int)(u >> 63);
+    int e = (int)((u >> 52) & 0x7ff);
+    uint64_t m = u & 0x000fffffffffffffULL;
+    if (e == 0) e = 1; else m |= 0x0010000000000000ULL;
+    int shift = e - 1075 - kFluxLsbExp;            // bit position of m's LSB
+    if (shift < 0) {
+        if (shift <= -64) return;
+        m >>= -shift;
+        shift = 0;
+    }
+    int L = shift >> 5, o = shift & 31;
+    // m < 2^53, shifted by o < 32: spans at most three 32-bit limbs
+    unsigned long long lo = (unsigned long long)(m << o);          // low 64 bits
+    unsigned long long hi = o ? (unsigned long long)(m >> (64 - o)) : 0ULL;
+    unsigned long long parts[3] = {lo & 0xffffffffULL, lo >> 32, hi};
+    for (int k = 0; k < 3; ++k) {
+        if (L + k >= kFluxLimbs) break;
+        if (parts[k] == 0) continue;
+        long long add = neg ? -(long long)parts[k] : (long long)parts[k];
+        atomicAdd((unsigned long long *)&limbs[L + k], (unsigned long long)add);
+    }
+}
+
+// particle_bcs_nonperiodic (reflect/kill) + particle_bcs_periodic for one
+// droplet (particles.f90:2683-2843); returns 0 if the droplet is killed.
+__device__ __forceinline__ int apply_bcs(const DevBox &B, const DevParams &p, double x[3], double v[3], double r) {
+    const DevGrid &g = B.g;
+    double top = (p.icase == 4) ? g.z[g.nnz - 1] - r : g.z[g.nnz] - r;
+    double bot = 0.0 + r;
+    if (x[2] > top) {
+        x[2] = top - (x[2] - top);
+        v[2] = -v[2];
+    } else if (x[2] < bot) {
+        if (p.icase == 0) {
+            x[2] = bot + (bot - x[2]);
+            v[2] = -v[2];
+        } else {
+            return 0;
+        }
+    }
+    if (x[0] > g.xl) x[0] = x[0] - g.xl;
+    else if (x[0] < 0) x[0] = g.xl + x[0];
+    if (x[1] > g.yl) x[1] = x[1] - g.yl;
+    else if (x[1] < 0) x[1] = g.yl + x[1];
+    return 1;
+}
+
+// Deposition payload (the droplet factors of particle_coupling_update,
+// particles.f90:1186-1264, that do not depend on the node).
+__device__ __forceinline__ void write_payload(const DevBox &B, const DevParams &p, int t, const double x[3],
+                                              const double v[3], const double vold[3], double r, double rold,
+                                              double Tp, double Tpold, double Tf, double m_s, long long mult,
+                                              double dt) {
+    const double pi2 = p.pi2;
+    double vrhs[3];
+    for (int a = 0; a < 3; ++a) vrhs[a] = (v[a] - vold[a]) / dt;
+    double radrhs = (r - rold) / dt;
+    double Tprhs_L = 3.0 * p.Lv / p.Cpp / r * radrhs;
+    double Tprhs_s = (Tp - Tpold) / dt - Tprhs_L;
+    double rhoa;
+    if (p.iexner == 1)
+        rhoa = func_p_base64(p, p.surf_p, p.tsfcc1, x[2]) / p.Rd / Tf;
+    else
+        rhoa = p.surf_rho;
+    double rhop = (m_s + pi2 * 2.0 / 3.0 * cube(r) * p.rhow) / (pi2 * 2.0 / 3.0 * cube(r));
+    double partmass = rhop * 2.0 / 3.0 * pi2 * cube(r);
+    double taup_i = 18.0 * rhoa * p.nuf / rhop / ((2.0 * r) * (2.0 * r));
+    double H0 = p.rhow / rhoa * pi2 * 2.0 * (r * r) * radrhs;
+    const DevPayload &P = B.pay;
+    for (int a = 0; a < 3; ++a) {
+        P.D[a][t] = partmass / rhoa * (vrhs[a] - p.g[a]);
+        P.V[a][t] = H0 * v[a];
+    }
+    P.T0[t] = (Tprhs_s * 6.0 * p.rhow / rhop / p.CpaCpp / taup_i * (pi2 / 2.0) * r * p.nuf);
+    P.H0[t] = H0;
+    P.E1[t] = H0 * p.Cpv / p.Cpa * Tp;
+    P.E2[t] = H0 * p.Cpv / p.Cpa * Tf;
+    P.mult[t] = (double)mult;
+}
+
+
+// ---------------------------------------------------------------------------
+// backward-Euler droplet body (particles.f90:3043-3242 + 3248-3260): all of
+// the per-droplet work after the interpolation.  MIXED computes the drag
+// (taup_i and the implicit velocity update) in FP32; positions, the Newton
+// radius/temperature solve and everything else stay FP64.
+// ---------------------------------------------------------------------------
+template <bool MIXED>
+__device__ __forceinline__ void be_body(const DevBox &B, const DevParams &p, const StepIn &in, int t, int s,
+                                        const double xin[3], const Interp &I, int bad, Counts &cnt) {
+    const DevState &S = B.st[B.cur];
+    const DevState &O = B.st[1 - B.cur];
+    double x[3] = {xin[0], xin[1], xin[2]};
+    double v[3], vold[3];
+    for (int a = 0; a < 3; ++a) v[a] = S.v[a][s];
+    double Tp = S.Tp[s], radius = S.r[s];
+    const double m_s = S.m_s[s], kap = S.kap[s], rc = S.rc[s];
+    double res = S.res[s], actres = S.actres[s], numact = S.numact[s];
+    const long long multi = S.mult[s];
+    const int lid = S.lid[s];
+    const double mult = (double)multi;
+    const double dt = in.dt;
+    for (int a = 0; a < 3; ++a) vold[a] = v[a];
+    const double Tpold = Tp, rold = radius;
+
+    double Tf = I.Tf, qinf = I.qinf;
+    if (in.it <= 1) { v[0] = I.uf[0]; v[1] = I.uf[1]; v[2] = I.uf[2]; }
+    double rhoa;
+    if (p.iexner == 1) {
+        Tf = Tf * exner64(p, p.surf_p, func_p_base64(p, p.surf_p, p.tsfcc1, x[2]));
+        rhoa = func_p_base64(p, p.surf_p, p.tsfcc1, x[2]) / p.Rd / Tf;
+    } else {
+        rhoa = p.surf_rho;
+    }
+    if (qinf < 0.0) cnt.v[C_NEGQ]++;
+
+    double Volp = p.pi2 * 2.0 / 3.0 * cube(radius);
+    double rhop = (m_s + Volp * p.rhow) / Volp;
+    double Rep = 0.0;
+    const double xp3i = x[2];
+    for (int a = 0; a < 3; ++a) x[a] = x[a] + dt * v[a];
+    if (MIXED) {
+        const float rr = (float)radius;
+        const float taup_if = 18.0f * (float)rhoa * (float)p.nuf / (float)rhop / ((2.0f * rr) * (2.0f * rr));
+        const float dtf = (float)dt;
+        const float den = 1.0f + dtf * taup_if;
+        float d0 = (float)(v[0] - I.uf[0]), d1 = (float)(v[1] - I.uf[1]), d2 = (float)(v[2] - I.uf[2]);
+        Rep = (double)(2.0f * rr * sqrtf(d0 * d0 + d1 * d1 + d2 * d2) / (float)p.nuf);
+        for (int a = 0; a < 3; ++a)
+            v[a] = (double)(((float)v[a] + taup_if * dtf * (float)I.uf[a] + dtf * (float)p.g[a]) / den);
+    } else {
+        double d0 = v[0] - I.uf[0], d1 = v[1] - I.uf[1], d2 = v[2] - I.uf[2];
+        double diffnorm = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+        double taup_i = 18.0 * rhoa * p.nuf / rhop / ((2.0 * radius) * (2.0 * radius));
+        Rep = 2.0 * radius * diffnorm / p.nuf;
+        const double corrfac = 1.0;
+        for (int a = 0; a < 3; ++a)
+            v[a] = (v[a] + taup_i * dt * corrfac * I.uf[a] + dt * p.g[a]) / (1.0 + dt * corrfac * taup_i);
+    }
+    const double taup0 = taup0_64(p, m_s, rhoa);
+    const double dt_taup0 = dt / taup0;
+
+    if (p.ievap == 1 && qinf > 0.0) {
+        const double esa = mod_magnus64(Tf);
+        int mflag;
+        double guess = rad_solver2_64(p, Tf, qinf, rhoa, m_s, kap, radius, esa, mflag);
+        double rt_start[2], rtz[2];
+        if (mflag == 0) { rt_start[0] = guess / radius; rt_start[1] = Tf / Tp; }
+        else { rt_start[0] = 1.0; rt_start[1] = 1.0; }
+        Drop D;
+        D.Tf = Tf; D.qinf = qinf; D.m_s = m_s; D.radius = radius; D.Tp = Tp; D.rhoa = rhoa;
+        D.h = dt_taup0;
+        {
+            double e0 = I.uf[0] - v[0], e1 = I.uf[1] - v[1], e2 = I.uf[2] - v[2];
+            D.diffnorm = sqrt(e0 * e0 + e1 * e1 + e2 * e2);
+        }
+        D.esa = esa;
+        D.taup0 = taup0;
+        D.inv_Tf = 1.0 / Tf;
+        D.c_taup = 18.0 * rhoa * p.nuf;
+        D.c_sol = kap * m_s * p.rhow / p.rhos;
+        D.t0r = taup0 / radius;
+        D.rt0 = radius / taup0;
+        D.t0T = taup0 / Tp;
+        int flag = gauss_newton64(p, D, rt_start, rtz);
+        if (flag == 1) {
+            cnt.v[C_NUM100]++;
+            flag = lv_solver64(p, D, rt_start, rtz);
+        }
+        if ((flag == 1) || ntlp_isnan(rtz[0]) || (rtz[0] * radius < 0) || ntlp_isnan(rtz[1]) ||
+            (rtz[1] < 0) || (rtz[0] * radius > 1.0e-2)) {
+            cnt.v[C_NUMIMPOS]++;
+            rtz[0] = 1.0;
+            rtz[1] = Tf / Tp;
+        }
+        if (radius > rc && radius * rtz[0] < rc) {
+            cnt.v[C_DENUM]++;
+        } else if (radius < rc && radius * rtz[0] > rc) {
+            cnt.v[C_ACTNUM]++;
+            numact = numact + 1.0;
+            actres = 0.0;
+        }
+        radius = rtz[0] * radius;
+        Tp = rtz[1] * Tp;
+    } else {
+        double taup_i = 18.0 * rhoa * p.nuf / rhop / ((2.0 * radius) * (2.0 * radius));
+        double Nup = 2.0 + 0.6 * sqrt(Rep) * p.Pra13;
+        double tmp_coeff = Nup / 3.0 / p.Pra * p.CpaCpp * rhop / p.rhow * taup_i;
+        Tp = (Tp + tmp_coeff * dt * Tf) / (1.0 + dt * tmp_coeff);
+    }
+    Volp = p.pi2 * 2.0 / 3.0 * cube(radius);
+    rhop = (m_s + Volp * p.rhow) / Volp;
+    double einf = mod_magnus64(Tf);
+    double qstar = (p.Mw / (p.Ru * Tp * rhoa)) * einf *
+                   ntlp_exp(((p.Lv * p.Mw / p.Ru) * ((1.0 / Tf) - (1.0 / Tp))) +
+                            ((2.0 * p.Mw * p.Gam) / (p.Ru * p.rhow * radius * Tp)) -
+                            ((kap * m_s * p.rhow / p.rhos) / (Volp * rhop - m_s)));
+    res = res + dt;
+    actres = actres + dt;
+
+    // vertical flux tallies (particles.f90:3209-3238), before the boundaries
+    {
+        const DevGrid &g = B.g;
+        int fluxloc, fluxloci;
+        if (x[2] > g.zl) {
+            fluxloc = g.nnz + 1;
+            fluxloci = minloc_gt(g.z, g.nz2, xp3i) - 1;
+        } else if (x[2] < 0.0) {
+            fluxloci = minloc_gt(g.z, g.nz2, xp3i) - 1;
+            fluxloc = 0;
+        } else {
+            fluxloc = minloc_gt(g.z, g.nz2, x[2]) - 1;
+            fluxloci = minloc_gt(g.z, g.nz2, xp3i) - 1;
+        }
+        int lo = 0, hi = -1;
+        double sgn = 0.0;
+        if (xp3i < x[2]) { lo = fluxloci; hi = fluxloc - 1; sgn = 1.0; }
+        else if (xp3i > x[2]) { lo = fluxloc; hi = fluxloci - 1; sgn = -1.0; }
+        if (hi >= lo) {
+            double mterm = rhop * Volp * mult;
+            double eterm = rhop * Volp * p.Cpp * Tp * mult;
+            const int nz1 = g.nnz + 1;
+            for (int iz = lo; iz <= hi; ++iz) {
+                if (iz < 0 || iz > g.nnz) continue;
+                atomicAdd(&B.pflux[iz], sgn * mult);
+                fx_add(B.flux_fx + (long long)iz * kFluxLimbs, sgn * mterm);
+                fx_add(B.flux_fx + (long long)(nz1 + iz) * kFluxLimbs, sgn * eterm);
+            }
+        }
+    }
+
+    const int alive = apply_bcs(B, p, x, v, radius);
+    if (bad) cnt.v[C_BAD]++;
+    for (int a = 0; a < 3; ++a) {
+        O.x[a][t] = x[a];
+        O.v[a][t] = v[a];
+        O.uf[a][t] = I.uf[a];
+        O.vold[a][t] = vold[a];
+    }
+    O.Tp[t] = Tp; O.r[t] = radius; O.m_s[t] = m_s; O.kap[t] = kap; O.rc[t] = rc;
+    O.res[t] = res; O.actres[t] = actres; O.numact[t] = numact; O.mult[t] = multi; O.lid[t] = lid;
+    O.Tf[t] = Tf; O.qinf[t] = qinf; O.qstar[t] = qstar; O.Tpold[t] = Tpold; O.rold[t] = rold;
+    int key;
+    if (!alive) {
+        key = (int)B.g.ncells + 1;
+        cnt.v[C_DESTROY]++;
+    } else {
+        key = cell_key(B.g, x[0], x[1], x[2]);
+        if (in.write_payload) write_payload(B, p, t, x, v, vold, radius, rold, Tp, Tpold, Tf, m_s, multi, dt);
+    }
+    B.key[t] = key;
+}
+
+}  // namespace
+}  // namespace ntlp

@@ -1,0 +1,223 @@
+"""Parity of the CUDA droplet step (through the C ABI) with the oracle.
+
+FP64 path: every droplet quantity, every counter, the binning and the
+deposited sources are compared BIT FOR BIT with the restatement built on the
+same elementary functions (oracle/liboracle.so).  The flux tallies of mass
+and energy are exact fixed-point sums on the device while the oracle adds in
+list order, so those two are compared to 1e-12 of the sum of |terms|.
+Mixed path: errors against the FP64 oracle within the stated tolerances.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import cuda_available
+from helpers import RK3_KEYS, STATE_KEYS, bitwise_equal, clone, max_rel, small_case
+from ntlp_b200 import abi
+from ntlp_b200 import generator as gen
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not cuda_available(), reason="needs a CUDA device")]
+
+# mixed-precision tolerances (relative to the FP64 oracle, per quantity)
+MIXED_TOL = dict(radius=1e-6, Tp=1e-6, vp=1e-4, xp=1e-9, uf=1e-4, Tf=1e-6, qinf=1e-4)
+
+
+def _gpu(case, params=None, flow=False):
+    import ntlp_b200
+    p = dict(case.params if params is None else params)
+    s = ntlp_b200.DropletStep(case.grid, p, capacity=max(1, case.droplets["radius"].shape[0]))
+    if flow:
+        s.fill_ext(case.flow())
+    else:
+        s.set_fields_ext(case.ext())
+    s.set_droplets(case.droplets)
+    return s
+
+
+def _oracle(case, params=None):
+    import pyoracle
+    return pyoracle.Oracle(case.grid, dict(case.params if params is None else params), case.ext())
+
+
+def _assert_state_bitexact(g, o, keys=STATE_KEYS):
+    assert g["radius"].shape == o["radius"].shape
+    bad = {k: max_rel(g[k], o[k], 1e-300) for k in keys if k in o and not bitwise_equal(g[k], o[k])}
+    assert not bad, bad
+
+
+def _assert_sources_bitexact(gsrc, osrc):
+    for q in range(6):
+        assert bitwise_equal(np.asarray(gsrc[q]), osrc[q]), (q, max_rel(gsrc[q], osrc[q], 1e-300))
+
+
+@pytest.mark.parametrize("ilin", [1, 0])
+@pytest.mark.parametrize("icase", [1, 0])
+def test_be_fp64_bitexact(ilin, icase):
+    params = gen.default_params(ilin=ilin, icase=icase)
+    case = small_case(params=params, n=4000)
+    d = clone(case.droplets)
+    d["xp"][2][:40] = d["radius"][:40] * 0.3          # exercise the bottom boundary
+    d["vp"][2][:40] = -0.3
+    d["xp"][2][40:80] = case.grid["z"][case.grid["nnz"]] - d["radius"][40:80] * 1.01   # and the top
+    d["vp"][2][40:80] = 0.4
+    case.droplets = d
+    s = _gpu(case)
+    o = _oracle(case)
+    od = clone(case.droplets)
+    for it in (1, 2, 3):
+        gc = s.particle_update_BE(case.dt, it)
+        oc, ofl = o.step_be(od, case.dt, it)
+        assert gc == oc, (it, gc, oc)
+        gd = s.get_droplets()
+        _assert_state_bitexact(gd, od)
+        gfl = s.flux()
+        assert bitwise_equal(gfl[0], ofl[0])
+        for q in (1, 2):
+            scale = np.abs(ofl[q]).max() + 1e-300
+            assert np.max(np.abs(gfl[q] - ofl[q])) <= 1e-12 * scale
+    gsrc = s.particle_coupling_update(case.dt)
+    osrc, _ = o.coupling(od, case.dt)
+    _assert_sources_bitexact(gsrc, osrc)
+    s.close()
+
+
+@pytest.mark.parametrize("ilin", [1, 0])
+def test_rk3_fp64_bitexact(ilin):
+    # explicit RK3 needs dt below the droplet response time: 20-60 um
+    # droplets (taup ~ 5-50 ms) at dt = 1e-4 s
+    params = gen.default_params(ilin=ilin, ipart_method=1)
+    case = small_case(params=params, n=2500)
+    d = clone(case.droplets)
+    r = np.random.default_rng(9).uniform(20e-6, 60e-6, d["radius"].shape[0])
+    d["radius"] = r
+    d["m_s"] = (2.0 / 3.0) * gen.PI2 * (0.5 * r) ** 3 * 2000.0 * 1e-3
+    case.droplets = d
+    case.dt = 1e-4
+    s = _gpu(case)
+    o = _oracle(case)
+    od = clone(case.droplets)
+    for it in (1, 2):
+        for istage in (1, 2, 3):
+            gc = s.particle_update_rk3(istage, case.dt, it)
+            oc = o.step_rk3(od, istage, case.dt, it)
+            assert gc["numpart"] == oc["numpart"] and gc["num_destroy"] == oc["num_destroy"]
+            assert gc["bad_index"] == oc["bad_index"] == 0
+    gd = s.get_droplets()
+    _assert_state_bitexact(gd, od, STATE_KEYS + RK3_KEYS)
+    gsrc = s.particle_coupling_update(case.dt)
+    osrc, _ = o.coupling(od, case.dt)
+    _assert_sources_bitexact(gsrc, osrc)
+    s.close()
+
+
+def test_stretched_grid_exner_spray_top():
+    """Stretched vertical grid (ratio 1.02), iexner=1, icase=4 top rule."""
+    params = gen.default_params(ilin=0, iexner=1, icase=4)
+    case = gen.make_case("c2", n=3000, grid_n=(12, 12, 24), params=params)
+    s = _gpu(case)
+    o = _oracle(case)
+    od = clone(case.droplets)
+    for it in (1, 2):
+        gc = s.particle_update_BE(case.dt, it)
+        oc, _ = o.step_be(od, case.dt, it)
+        assert gc == oc
+    _assert_state_bitexact(s.get_droplets(), od)
+    _assert_sources_bitexact(s.particle_coupling_update(case.dt), o.coupling(od, case.dt)[0])
+
+
+def test_flow_layout_upload_matches_ext():
+    case = small_case(n=1500)
+    a = _gpu(case, flow=False)
+    b = _gpu(case, flow=True)
+    a.particle_update_BE(case.dt, 1)
+    b.particle_update_BE(case.dt, 1)
+    da, db = a.get_droplets(), b.get_droplets()
+    for k in STATE_KEYS:
+        assert bitwise_equal(da[k], db[k]), k
+
+
+def test_flow_layout_sources_are_transposed_columns():
+    case = small_case(n=1500)
+    s = _gpu(case)
+    s.particle_update_BE(case.dt, 1)
+    col = s.particle_coupling_update(case.dt, abi.NTLP_LAYOUT_COLUMN)
+    flow = s.particle_coupling_update(case.dt, abi.NTLP_LAYOUT_FLOW)
+    for q in range(6):
+        assert bitwise_equal(np.transpose(np.asarray(col[q]), (2, 1, 0)), np.asarray(flow[q]))
+
+
+def test_deterministic_run_to_run():
+    case = small_case(n=3000, grid_n=(8, 8, 8))   # many droplets per cell
+    outs = []
+    for _ in range(2):
+        s = _gpu(case)
+        for it in (1, 2):
+            s.particle_update_BE(case.dt, it)
+        outs.append(s.particle_coupling_update(case.dt))
+        s.close()
+    for q in range(6):
+        assert bitwise_equal(np.asarray(outs[0][q]), np.asarray(outs[1][q]))
+
+
+def test_droplet_exactly_on_the_periodic_edge():
+    case = small_case(n=64, params=gen.default_params(ilin=0))
+    d = clone(case.droplets)
+    d["xp"][0][:4] = case.grid["xl"]
+    d["xp"][1][:4] = case.grid["yl"]
+    d["xp"][0][4:8] = 0.0
+    d["vp"][0][:8] = 0.0
+    d["vp"][1][:8] = 0.0
+    case.droplets = d
+    s = _gpu(case)
+    o = _oracle(case)
+    od = clone(d)
+    gc = s.particle_update_BE(case.dt, 2)
+    oc, _ = o.step_be(od, case.dt, 2)
+    assert gc == oc and gc["bad_index"] == 0
+    _assert_state_bitexact(s.get_droplets(), od)
+    _assert_sources_bitexact(s.particle_coupling_update(case.dt), o.coupling(od, case.dt)[0])
+
+
+def test_empty_droplet_list():
+    case = small_case(n=1)
+    d = {k: (v[..., :0].copy() if isinstance(v, np.ndarray) else v) for k, v in case.droplets.items()}
+    import ntlp_b200
+    s = ntlp_b200.DropletStep(case.grid, case.params, capacity=8)
+    s.set_fields_ext(case.ext())
+    s.set_droplets(d)
+    c = s.particle_update_BE(case.dt, 1)
+    assert c["numpart"] == 0
+    src = s.particle_coupling_update(case.dt)
+    assert all(np.count_nonzero(np.asarray(a)) == 0 for a in src)
+
+
+def test_capacity_is_enforced():
+    import ntlp_b200
+    case = small_case(n=100)
+    s = ntlp_b200.DropletStep(case.grid, case.params, capacity=50)
+    with pytest.raises(ntlp_b200.NtlpError):
+        s.set_droplets(case.droplets)
+
+
+@pytest.mark.parametrize("ilin", [1, 0])
+def test_mixed_precision_within_tolerance(ilin):
+    params = gen.default_params(ilin=ilin)
+    case = small_case(params=params, n=4000)
+    pm = dict(params, precision=abi.NTLP_PREC_MIXED)
+    s = _gpu(case, pm)
+    o = _oracle(case)
+    od = clone(case.droplets)
+    for it in (1, 2, 3):
+        gc = s.particle_update_BE(case.dt, it)
+        oc, _ = o.step_be(od, case.dt, it)
+        assert gc["numpart"] == oc["numpart"]
+    gd = s.get_droplets()
+    assert np.array_equal(gd["lid"], od["lid"])
+    errs = {k: max_rel(gd[k], od[k], 1e-3 if k in ("vp", "uf") else 1e-300) for k in MIXED_TOL}
+    assert all(errs[k] <= MIXED_TOL[k] for k in MIXED_TOL), errs
+    gsrc = s.particle_coupling_update(case.dt)
+    osrc, oabs = o.coupling(od, case.dt, with_abs=True)
+    for q in range(6):
+        scale = np.abs(oabs[q]).max()
+        assert np.max(np.abs(np.asarray(gsrc[q]) - osrc[q])) <= 1e-3 * scale, q
