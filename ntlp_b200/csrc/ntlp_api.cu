@@ -447,7 +447,9 @@ int ntlp_fields_upload_ext(ntlp_ctx *c, const double *uext, const double *vext, 
     const size_t npad = (size_t)g.nz2 * g.ny5 * g.nx5;
     for (int k = 0; k < 5; ++k) {
         CK(cudaMemcpyAsync((void *)c->box.f[k], h[k], npad * 8, cudaMemcpyHostToDevice, c->stream));
-        if (c->box.f32[k]) launch_to_f32(c->box.f[k], (float *)c->box.f32[k], (long long)npad, c->stream);
+        if (c->box.f32[k])
+            launch_to_f32(c->box.f[k], (float *)c->box.f32[k], (long long)npad,
+                          1LL + (long long)g.nz2 * (2LL + (long long)g.ny5 * 2LL), c->stream);
     }
     CK(cudaGetLastError());
     c->have_fields = true;

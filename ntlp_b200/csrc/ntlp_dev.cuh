@@ -139,6 +139,13 @@ __device__ __forceinline__ long long ext_index(const DevGrid &g, int k, int j, i
 
 __device__ __forceinline__ double cube(double r) { return (r * r) * r; }
 
+// The FP32 field copies hold deviations from the value at the interior
+// point (k, j, i) = (1, 1, 1): T ~ 293 K would otherwise keep only ~3e-5 K
+// in FP32, and the saturation vapour pressure is exponential in T.
+__device__ __forceinline__ long long f32_ref_index(const DevGrid &g) {
+    return 1LL + (long long)g.nz2 * (2LL + (long long)g.ny5 * 2LL);
+}
+
 // Tile of work: (box, first element); blocks map to tiles.
 struct Tile {
     int box;

@@ -52,7 +52,7 @@ void launch_keys_initial(DevBox *boxes, const Tile *tiles, int ntiles, cudaStrea
 
 // halo fill from the flow layout (fill_ext on one domain) and FP32 copies
 void launch_fill_ext(const double *flow, double *ext, float *ext32, const DevGrid &g, cudaStream_t st);
-void launch_to_f32(const double *src, float *dst, long long n, cudaStream_t st);
+void launch_to_f32(const double *src, float *dst, long long n, long long ridx, cudaStream_t st);
 
 // download: position of each survivor in list order
 void launch_rank_alive(DevBox *boxes, int box, int *rank_by_lid, int nlid, cudaStream_t st);

@@ -2,7 +2,9 @@
 //
 // Interpolation weights and stencil products in FP32 with FP32 accumulation,
 // reading FP32 copies of the fields (half the bytes of the FP64 path); drag
-// in FP32.  Positions, the Newton radius/temperature solve and the source
+// in FP32.  The FP32 copies hold deviations from a reference value of each
+// field (its value at the interior point (1,1,1)), which is added back in
+// FP64 after the contraction.  Positions, the Newton radius/temperature solve and the source
 // accumulation stay FP64.  Offsets from the droplet to the stencil nodes are
 // formed in FP64 and only then rounded to FP32, so positions up to a few
 // hundred metres keep their sub-cell resolution.
@@ -126,7 +128,12 @@ __device__ void interp6_mixed(const DevBox &B, double x1, double x2, double x3, 
         sT = fmaf(cT, wx[i], sT);
         sq = fmaf(cq, wx[i], sq);
     }
-    o.uf[0] = su; o.uf[1] = sv; o.uf[2] = sw; o.Tf = sT; o.qinf = sq;
+    const long long ridx = f32_ref_index(g);
+    o.uf[0] = B.f[0][ridx] + (double)su;
+    o.uf[1] = B.f[1][ridx] + (double)sv;
+    o.uf[2] = B.f[2][ridx] + (double)sw;
+    o.Tf = B.f[3][ridx] + (double)sT;
+    o.qinf = B.f[4][ridx] + (double)sq;
 }
 
 __device__ void interp_lin_mixed(const DevBox &B, double x1, double x2, double x3, Interp &o, int &bad) {
@@ -179,7 +186,12 @@ __device__ void interp_lin_mixed(const DevBox &B, double x1, double x2, double x
             }
         }
     }
-    o.uf[0] = u1; o.uf[1] = u2; o.uf[2] = u3; o.Tf = T; o.qinf = q;
+    const long long ridx = f32_ref_index(g);
+    o.uf[0] = B.f[0][ridx] + (double)u1;
+    o.uf[1] = B.f[1][ridx] + (double)u2;
+    o.uf[2] = B.f[2][ridx] + (double)u3;
+    o.Tf = B.f[3][ridx] + (double)T;
+    o.qinf = B.f[4][ridx] + (double)q;
 }
 
 template <int ILIN>

@@ -232,6 +232,7 @@ __global__ void k_fill_ext(const double *__restrict__ flow, double *__restrict__
     const int i0 = (int)blockIdx.x * 32 - 1;           // ext i of tile start
     const int k0 = (int)blockIdx.y * 32;
     const int jsrc = ((j - 1) % g.nny + g.nny) % g.nny;  // 0-based source row
+    const double ref = flow[(long long)g.nnx * g.nny];     // flow(1,1,1) = ext(1,1,1)
     // load: threads along i (x fastest in flow)
     for (int r = threadIdx.y; r < 32; r += blockDim.y) {
         int k = k0 + r;
@@ -250,7 +251,7 @@ __global__ void k_fill_ext(const double *__restrict__ flow, double *__restrict__
             long long o = (long long)k + (long long)g.nz2 * ((long long)(j + 1) + (long long)g.ny5 * (i + 1));
             double val = tile[threadIdx.x][r];
             ext[o] = val;
-            if (ext32) ext32[o] = (float)val;
+            if (ext32) ext32[o] = (float)(val - ref);
         }
     }
 }
@@ -261,16 +262,17 @@ void launch_fill_ext(const double *flow, double *ext, float *ext32, const DevGri
     k_fill_ext<<<grid, block, 0, st>>>(flow, ext, ext32, g);
 }
 
-__global__ void k_to_f32(const double *__restrict__ s, float *__restrict__ d, long long n) {
+__global__ void k_to_f32(const double *__restrict__ s, float *__restrict__ d, long long n, long long ridx) {
+    const double ref = s[ridx];
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     long long stride = (long long)gridDim.x * blockDim.x;
-    for (; i < n; i += stride) d[i] = (float)s[i];
+    for (; i < n; i += stride) d[i] = (float)(s[i] - ref);
 }
 
-void launch_to_f32(const double *src, float *dst, long long n, cudaStream_t st) {
+void launch_to_f32(const double *src, float *dst, long long n, long long ridx, cudaStream_t st) {
     int blocks = (int)((n + 255) / 256);
     if (blocks > 148 * 16) blocks = 148 * 16;
-    if (blocks > 0) k_to_f32<<<blocks, 256, 0, st>>>(src, dst, n);
+    if (blocks > 0) k_to_f32<<<blocks, 256, 0, st>>>(src, dst, n, ridx);
 }
 
 // ---- download: list-order position of every survivor -----------------------
