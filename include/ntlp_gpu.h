@@ -176,6 +176,35 @@ int ntlp_profile_read(ntlp_ctx *ctx, double ms[4], int64_t *launches);
 int ntlp_crit_radius(const ntlp_params *params, int64_t n, const double *m_s,
                      const double *kappa_s, const double *T, double *rc);
 
+/* ---- deposition without allocation -------------------------------------
+ * No counterpart in the reference.  For hosts that cannot let a library
+ * allocate device memory inside their time loop -- their device memory
+ * belongs to another runtime (an OpenACC or CUDA Fortran data region) or to
+ * a pool sized at start-up -- this call deposits the two-way coupling
+ * sources of droplets the caller already holds in device memory, into six
+ * device arrays the caller provides (column layout (0:nnz+1,1:nny,1:nnx),
+ * partsrc components 1..3, partTsrc, partHsrc, partTEsrc), in FP64 and list
+ * order: the same values as ntlp_coupling on an FP64 context.  It calls no
+ * allocating routine; its working memory is one static device array of
+ * about 22 MB that every GPU loading the library holds until exit, which
+ * bounds the sizes below (larger inputs return NTLP_ERR_CAPACITY).  The
+ * first call on a device looks up that array's address (make it before any
+ * stream capture); all calls share the array, so calls whose work overlaps
+ * on the GPU race.  Work is queued on `stream` (a cudaStream_t, NULL for the
+ * default stream); the outputs are ready when that stream reaches them.    */
+#define NTLP_NOALLOC_MAX_DROPLETS 131072
+#define NTLP_NOALLOC_MAX_CELLS    1048576   /* (nnx+1)*(nny+1)*(nnz+1) */
+#define NTLP_NOALLOC_MAX_NNZ      1024
+typedef struct ntlp_device_droplets {
+    int64_t n;                                /* list order = array order  */
+    const double *xp[3], *vp[3], *vp_old[3];  /* device pointers           */
+    const double *radius, *radius_old, *Tp, *Tp_old, *Tf, *m_s;
+    const int64_t *mult;
+} ntlp_device_droplets;
+int ntlp_coupling_noalloc(const ntlp_grid *grid, const ntlp_params *params,
+                          const ntlp_device_droplets *d, double dt,
+                          double *const partsrc[6], void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -8,6 +8,7 @@ Compilation units:
   ntlp_mixed.cu  mixed-precision kernels (contraction allowed)
   ntlp_sort.cu   counting sort on cell keys, halo fill, bookkeeping
   ntlp_api.cu    the C ABI of include/ntlp_gpu.h
+  ntlp_noalloc.cu  the deposition entry point that allocates nothing
 Objects go to ntlp_b200/_build/, the library to ntlp_b200/_lib/.
 """
 from __future__ import annotations
@@ -29,6 +30,7 @@ UNITS = {
     "ntlp_mixed.cu": [],
     "ntlp_sort.cu": [],
     "ntlp_api.cu": [],
+    "ntlp_noalloc.cu": [],
 }
 HEADERS = ["ntlp_math.h", "ntlp_dev.cuh", "ntlp_kernels.h", "ntlp_physics.cuh"]
 
