@@ -186,7 +186,7 @@ int ntlp_crit_radius(const ntlp_params *params, int64_t n, const double *m_s,
  * partsrc components 1..3, partTsrc, partHsrc, partTEsrc), in FP64 and list
  * order: the same values as ntlp_coupling on an FP64 context.  It calls no
  * allocating routine; its working memory is one static device array of
- * about 22 MB that every GPU loading the library holds until exit, which
+ * about 24 MB that every GPU loading the library holds until exit, which
  * bounds the sizes below (larger inputs return NTLP_ERR_CAPACITY).  The
  * first call on a device looks up that array's address (make it before any
  * stream capture); all calls share the array, so calls whose work overlaps

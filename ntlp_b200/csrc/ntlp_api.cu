@@ -311,22 +311,29 @@ int ntlp_ctx_create(const ntlp_grid *grid, const ntlp_params *params, int64_t ca
         double *f;
         if ((rc = dalloc(c, &f, (size_t)npad))) return bail(rc);
         c->box.f[k] = f;
-        if (params->precision == NTLP_PREC_MIXED) {
-            float *f32;
-            if ((rc = dalloc(c, &f32, (size_t)npad))) return bail(rc);
-            c->box.f32[k] = f32;
-        }
+    }
+    if (params->precision == NTLP_PREC_MIXED) {
+        float4 *f4;
+        float *fw;
+        if ((rc = dalloc(c, &f4, (size_t)npad)) || (rc = dalloc(c, &fw, (size_t)npad))) return bail(rc);
+        c->box.f4 = f4;
+        c->box.fw = fw;
     }
     for (int b = 0; b < 2; ++b)
         if ((rc = alloc_state(c, c->box.st[b], false))) return bail(rc);
-    DevPayload &P = c->box.pay;
     const size_t n = (size_t)capacity;
-    for (int a = 0; a < 3; ++a) {
-        if ((rc = dalloc(c, &P.D[a], n)) || (rc = dalloc(c, &P.V[a], n))) return bail(rc);
+    if (params->precision == NTLP_PREC_MIXED) {
+        for (int q = 0; q < P32_N; ++q)
+            if ((rc = dalloc(c, &c->box.pay32.f[q], n))) return bail(rc);
+    } else {
+        DevPayload &P = c->box.pay;
+        for (int a = 0; a < 3; ++a) {
+            if ((rc = dalloc(c, &P.D[a], n)) || (rc = dalloc(c, &P.V[a], n))) return bail(rc);
+        }
+        if ((rc = dalloc(c, &P.T0, n)) || (rc = dalloc(c, &P.H0, n)) || (rc = dalloc(c, &P.E1, n)) ||
+            (rc = dalloc(c, &P.E2, n)) || (rc = dalloc(c, &P.mult, n)))
+            return bail(rc);
     }
-    if ((rc = dalloc(c, &P.T0, n)) || (rc = dalloc(c, &P.H0, n)) || (rc = dalloc(c, &P.E1, n)) ||
-        (rc = dalloc(c, &P.E2, n)) || (rc = dalloc(c, &P.mult, n)))
-        return bail(rc);
     c->box.cap = (int)capacity;
     if ((rc = dalloc(c, &c->box.n_alive, 1)) || (rc = dalloc(c, &c->box.perm, n)) ||
         (rc = dalloc(c, &c->box.key, n)) || (rc = dalloc(c, &c->box.sorted, n)) ||
@@ -334,7 +341,8 @@ int ntlp_ctx_create(const ntlp_grid *grid, const ntlp_params *params, int64_t ca
         (rc = dalloc(c, &c->box.cell_start, (size_t)g.ncells + 3)) ||
         (rc = dalloc(c, &c->box.counters, kNumCounters)) || (rc = dalloc(c, &c->box.pflux, g.nnz + 1)) ||
         (rc = dalloc(c, &c->box.flux_fx, (size_t)2 * (g.nnz + 1) * kFluxLimbs)) ||
-        (rc = dalloc(c, &c->box.err, 1)))
+        (rc = dalloc(c, &c->box.err, 1)) || (rc = dalloc(c, &c->box.defer, n)) ||
+        (rc = dalloc(c, &c->box.ndefer, 1)))
         return bail(rc);
     for (int q = 0; q < 6; ++q)
         if ((rc = dalloc(c, &c->box.src[q], (size_t)g.nnodes))) return bail(rc);
@@ -351,7 +359,7 @@ int ntlp_ctx_create(const ntlp_grid *grid, const ntlp_params *params, int64_t ca
 
     c->drop_tiles = make_tiles(capacity, kUpdateThreads);
     c->cell_tiles = make_tiles(g.ncells + 2, kScanTile);
-    c->node_tiles = make_tiles(g.nnodes, kDepositThreads);
+    c->node_tiles = make_tiles(deposit_tile_count(g.nnx, g.nny, g.nnz), 1);
     if ((rc = dalloc(c, &c->drop_tiles_d, c->drop_tiles.size())) ||
         (rc = dalloc(c, &c->cell_tiles_d, c->cell_tiles.size())) ||
         (rc = dalloc(c, &c->node_tiles_d, c->node_tiles.size())) ||
@@ -445,12 +453,9 @@ int ntlp_fields_upload_ext(ntlp_ctx *c, const double *uext, const double *vext, 
         if (!h[k]) return fail(c, NTLP_ERR_ARG, "field %d is NULL", k);
     const DevGrid &g = c->box.g;
     const size_t npad = (size_t)g.nz2 * g.ny5 * g.nx5;
-    for (int k = 0; k < 5; ++k) {
+    for (int k = 0; k < 5; ++k)
         CK(cudaMemcpyAsync((void *)c->box.f[k], h[k], npad * 8, cudaMemcpyHostToDevice, c->stream));
-        if (c->box.f32[k])
-            launch_to_f32(c->box.f[k], (float *)c->box.f32[k], (long long)npad,
-                          1LL + (long long)g.nz2 * (2LL + (long long)g.ny5 * 2LL), c->stream);
-    }
+    if (c->box.f4) launch_pack_f32(&c->box, (float4 *)c->box.f4, (float *)c->box.fw, c->stream);
     CK(cudaGetLastError());
     c->have_fields = true;
     return NTLP_OK;
@@ -466,8 +471,9 @@ int ntlp_fields_upload(ntlp_ctx *c, const double *u, const double *v, const doub
     const size_t nflow = (size_t)g.nnx * g.nny * g.nz2;
     for (int k = 0; k < 5; ++k) {
         CK(cudaMemcpyAsync(c->staging_d, h[k], nflow * 8, cudaMemcpyHostToDevice, c->stream));
-        launch_fill_ext(c->staging_d, (double *)c->box.f[k], (float *)c->box.f32[k], g, c->stream);
+        launch_fill_ext(c->staging_d, (double *)c->box.f[k], g, c->stream);
     }
+    if (c->box.f4) launch_pack_f32(&c->box, (float4 *)c->box.f4, (float *)c->box.fw, c->stream);
     CK(cudaGetLastError());
     c->have_fields = true;
     return NTLP_OK;
@@ -643,9 +649,10 @@ static int do_step(ntlp_ctx *c, int kind, int istage, double dt, int32_t it, ntl
     e0 = phase_begin(c);
     if (kind == 1) {
         if (c->params.precision == NTLP_PREC_MIXED)
-            launch_update_be_mixed(c->params.ilin, c->box_d, c->drop_tiles_d, ntiles, c->dp_d, in, c->stream);
+            launch_update_be_mixed(c->params.ilin, c->box_d, c->drop_tiles_d, ntiles, 1, c->dp_d, in, c->stream);
         else
-            launch_update_be64(c->params.ilin, c->box_d, c->drop_tiles_d, ntiles, c->dp_d, in, c->stream);
+            launch_update_be64(c->params.ilin, c->box_d, c->drop_tiles_d, ntiles, 1, c->dp_d, in, c->stream);
+        c->launches += kUpdateLaunches - 1;
     } else {
         launch_update_rk3_64(c->params.ilin, c->box_d, c->drop_tiles_d, ntiles, c->dp_d, in, c->stream);
     }
@@ -705,7 +712,10 @@ int ntlp_coupling(ntlp_ctx *c, double dt, int32_t layout, double *partsrc, doubl
     if (!(dt > 0.0)) return fail(c, NTLP_ERR_ARG, "dt must be positive");
     if (!c->payload_valid || c->last_dt != dt) {
         cudaEvent_t ep = phase_begin(c);
-        launch_payload64(c->box_d, c->drop_tiles_d, (int)c->drop_tiles.size(), c->dp_d, dt, c->stream);
+        if (c->params.precision == NTLP_PREC_MIXED)
+            launch_payload_mixed(c->box_d, c->drop_tiles_d, (int)c->drop_tiles.size(), c->dp_d, dt, c->stream);
+        else
+            launch_payload64(c->box_d, c->drop_tiles_d, (int)c->drop_tiles.size(), c->dp_d, dt, c->stream);
         phase_end(c, PH_OTHER, ep);
         c->launches += 1;
         c->payload_valid = true;

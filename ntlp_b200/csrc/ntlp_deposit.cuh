@@ -1,0 +1,286 @@
+// ntlp_deposit.cuh -- deterministic two-way-coupling deposition
+// (particle_coupling_update, particles.f90:1151-1276, and the single-domain
+// periodic fold of particle_coupling_exchange, :1078-1113).
+//
+// Every output node sums the contributions of the droplets in its (up to) 8
+// neighbouring cells in list order (ascending lid): the cell lists are
+// lid-sorted, so each node is an 8-way merge.  Nodes with ix <= 2 or iy <= 2
+// also receive their periodic images (ix+nnx, iy+nny), combined in the order
+// of the fold (x first, then y).
+//
+// The main kernel stages, per tile of TX x TY x TZ nodes, the droplets of
+// the tile's (TX+1)(TY+1)(TZ+1) cells in shared memory (each (x, y) column of
+// cells is one contiguous range of the sorted list) and merges from there;
+// tiles touching the periodic edges, or holding more droplets than the
+// shared buffer, merge straight from global memory.  Both paths perform the
+// same operations in the same order.
+//
+// MIXED=false: each contribution is formed as the reference writes it,
+// ((P*wtt)/dV)*mult with wtt = wtx*wty*wtz, subtracted term by term.
+// MIXED=true: the FP32 payload (cell-relative fractions, momentum/heat/
+// vapour factors, mult/dV), FP32 weights, FP64 sums.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "ntlp_dev.cuh"
+#include "ntlp_kernels.h"
+
+namespace ntlp {
+namespace {
+
+constexpr int kDepTX = 2, kDepTY = 4, kDepTZ = 32;                // 256 nodes per tile
+constexpr int kDepCols = (kDepTX + 1) * (kDepTY + 1);             // cell columns per tile
+constexpr int kDepCap64 = 640;                                    // droplets staged per tile (FP64)
+constexpr int kDepCapMixed = 1024;                                // droplets staged per tile (mixed)
+
+struct DropVals {
+    double x1, x2, x3, D[3], V[3], T0, H0, E1, E2, mult;
+};
+
+// FP64 contribution, formed as the reference writes it
+__device__ __forceinline__ void contribute64(const DevGrid &g, const DevParams &p, const DropVals &d, int kpt,
+                                             double xv, double yv, double zv, double acc[6]) {
+    const double wtx = (1.0 - fabs(d.x1 - xv) / g.dx);
+    const double wty = (1.0 - fabs(d.x2 - yv) / g.dy);
+    const double wtz = (1.0 - fabs(d.x3 - zv) / g.dzu[kpt + 1]);
+    const double wtt = wtx * wty * wtz;
+    const double dV = g.dx * g.dy * g.dzu[kpt + 1];
+    if (p.icouple == 1) {
+        for (int a = 0; a < 3; ++a) {
+            acc[a] = acc[a] - d.D[a] * wtt / dV * d.mult;
+            acc[a] = acc[a] - d.V[a] * wtt / dV * d.mult;
+        }
+    }
+    if (p.iTcouple == 1) acc[3] = acc[3] - d.T0 * wtt / dV * d.mult;
+    if (p.iHcouple == 1) {
+        acc[4] = acc[4] - d.H0 * wtt / dV * d.mult;
+        acc[5] = acc[5] - d.E1 * wtt / dV * d.mult + d.E2 * wtt / dV * d.mult;
+    }
+}
+
+// mixed contribution from the FP32 payload; (i, j, k) is the node's offset
+// from the droplet's cell, so the weight along x is fx (i = 1) or 1 - fx
+__device__ __forceinline__ void contribute32(const DevParams &p, const float *v, int i, int j, int k,
+                                             double acc[6]) {
+    const float wx = i ? v[P32_FX] : 1.0f - v[P32_FX];
+    const float wy = j ? v[P32_FY] : 1.0f - v[P32_FY];
+    const float wz = k ? v[P32_FZ] : 1.0f - v[P32_FZ];
+    const double c = (double)(wx * wy * wz * v[P32_FAC]);
+    if (p.icouple == 1)
+        for (int a = 0; a < 3; ++a) acc[a] -= (double)v[P32_DV0 + a] * c;
+    if (p.iTcouple == 1) acc[3] -= (double)v[P32_T0] * c;
+    if (p.iHcouple == 1) {
+        acc[4] -= (double)v[P32_H0] * c;
+        acc[5] += (double)v[P32_E] * c;
+    }
+}
+
+// Merge of up to 8 lid-sorted ranges.  Source: global memory through the
+// sorted list (STAGED false; positions index B.perm) or the shared-memory
+// stage (STAGED true; positions index the stage).
+template <bool MIXED, bool STAGED>
+__device__ __forceinline__ void merge_ranges(const DevBox &B, const DevParams &p, const int *s_lid,
+                                             const double *s_v, const float *s_f, int n, int pos[8],
+                                             const int end[8], const int ck[8], const int off[8], int px,
+                                             int py, int pz, double acc[6]) {
+    const DevGrid &g = B.g;
+    for (int q = 0; q < 6; ++q) acc[q] = 0.0;
+    if (n == 0) return;
+    const DevState &O = B.st[B.cur];
+    int head[8];
+    for (int c = 0; c < n; ++c) head[c] = STAGED ? s_lid[pos[c]] : O.lid[B.perm[pos[c]]];
+    const double xv = g.dx * (double)(px - 1);
+    const double yv = g.dy * (double)(py - 1);
+    const double zv = g.zz[pz];
+    while (true) {
+        int best = -1, bl = 0x7fffffff;
+        for (int c = 0; c < n; ++c)
+            if (pos[c] < end[c] && head[c] < bl) { bl = head[c]; best = c; }
+        if (best < 0) break;
+        const int at = pos[best];
+        const int kpt = ck[best];
+        const int o = off[best];
+        pos[best]++;
+        if (pos[best] < end[best]) head[best] = STAGED ? s_lid[pos[best]] : O.lid[B.perm[pos[best]]];
+        if (MIXED) {
+            float v[P32_N];
+            if (STAGED) {
+                for (int q = 0; q < P32_N; ++q) v[q] = s_f[q * kDepCapMixed + at];
+            } else {
+                const int t = B.perm[at];
+                for (int q = 0; q < P32_N; ++q) v[q] = B.pay32.f[q][t];
+            }
+            contribute32(p, v, o >> 2, (o >> 1) & 1, o & 1, acc);
+        } else {
+            DropVals d;
+            if (STAGED) {
+                d.x1 = s_v[at]; d.x2 = s_v[kDepCap64 + at]; d.x3 = s_v[2 * kDepCap64 + at];
+                for (int a = 0; a < 3; ++a) {
+                    d.D[a] = s_v[(3 + a) * kDepCap64 + at];
+                    d.V[a] = s_v[(6 + a) * kDepCap64 + at];
+                }
+                d.T0 = s_v[9 * kDepCap64 + at]; d.H0 = s_v[10 * kDepCap64 + at];
+                d.E1 = s_v[11 * kDepCap64 + at]; d.E2 = s_v[12 * kDepCap64 + at];
+                d.mult = s_v[13 * kDepCap64 + at];
+            } else {
+                const int t = B.perm[at];
+                const DevPayload &P = B.pay;
+                d.x1 = O.x[0][t]; d.x2 = O.x[1][t]; d.x3 = O.x[2][t];
+                for (int a = 0; a < 3; ++a) { d.D[a] = P.D[a][t]; d.V[a] = P.V[a][t]; }
+                d.T0 = P.T0[t]; d.H0 = P.H0[t]; d.E1 = P.E1[t]; d.E2 = P.E2[t]; d.mult = P.mult[t];
+            }
+            contribute64(g, p, d, kpt, xv, yv, zv, acc);
+        }
+    }
+}
+
+// one pre-fold node image from global memory
+template <bool MIXED>
+__device__ __forceinline__ void image_global(const DevBox &B, const DevParams &p, int px, int py, int pz,
+                                             double acc[6]) {
+    const DevGrid &g = B.g;
+    int pos[8], end[8], ck[8], off[8];
+    int n = 0;
+    for (int i = 0; i <= 1; ++i)
+        for (int j = 0; j <= 1; ++j)
+            for (int k = 0; k <= 1; ++k) {
+                const int ci = px - i, cj = py - j, ckk = pz - k;
+                if (ci < 1 || ci > g.nnx + 1 || cj < 1 || cj > g.nny + 1 || ckk < 0 || ckk > g.nnz) continue;
+                const int key = ckk + (g.nnz + 1) * ((cj - 1) + (g.nny + 1) * (ci - 1));
+                const int a = B.cell_start[key], b = B.cell_start[key + 1];
+                if (a < b) { pos[n] = a; end[n] = b; ck[n] = ckk; off[n] = (i << 2) | (j << 1) | k; n++; }
+            }
+    merge_ranges<MIXED, false>(B, p, nullptr, nullptr, nullptr, n, pos, end, ck, off, px, py, pz, acc);
+}
+
+// a whole output node (with its periodic images) from global memory
+template <bool MIXED>
+__device__ __forceinline__ void node_global(const DevBox &B, const DevParams &p, int ix, int iy, int iz,
+                                            double out[6]) {
+    const DevGrid &g = B.g;
+    double a1[6];
+    image_global<MIXED>(B, p, ix, iy, iz, out);
+    if (ix <= 2) {
+        image_global<MIXED>(B, p, ix + g.nnx, iy, iz, a1);
+        for (int q = 0; q < 6; ++q) out[q] = out[q] + a1[q];
+    }
+    if (iy <= 2) {
+        double b0[6];
+        image_global<MIXED>(B, p, ix, iy + g.nny, iz, b0);
+        if (ix <= 2) {
+            image_global<MIXED>(B, p, ix + g.nnx, iy + g.nny, iz, a1);
+            for (int q = 0; q < 6; ++q) b0[q] = b0[q] + a1[q];
+        }
+        for (int q = 0; q < 6; ++q) out[q] = out[q] + b0[q];
+    }
+}
+
+constexpr int kDepCSW = kDepTZ + 2;                                // cell starts per column
+constexpr int kDepSmem64 = kDepCap64 * 4 + 14 * kDepCap64 * 8 + kDepCols * kDepCSW * 4 + kDepCols * 4 + 16;
+constexpr int kDepSmemMixed = kDepCapMixed * 4 + P32_N * kDepCapMixed * 4 + kDepCols * kDepCSW * 4 + kDepCols * 4 + 16;
+
+// Tiled deposition: tiles enumerate (z fastest) the node tiles of each box.
+template <bool MIXED>
+__global__ void __launch_bounds__(kDepositThreads, MIXED ? 3 : 2)
+k_deposit_tiled(DevBox *boxes, const Tile *tiles, const DevParams *pp) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    constexpr int CAP = MIXED ? kDepCapMixed : kDepCap64;
+    // stage: values first (8-byte aligned), then lid, cell starts, column offsets
+    double *s_v = (double *)sm;                                         // FP64: [14][CAP]
+    float *s_f = (float *)sm;                                           // mixed: [P32_N][CAP]
+    int *s_lid = (int *)(sm + (MIXED ? P32_N * CAP * 4 : 14 * CAP * 8));
+    int *s_cs = s_lid + CAP;                                            // [cols][TZ+2], absolute
+    int *s_off = s_cs + kDepCols * kDepCSW;                             // [cols] stage offset
+    __shared__ int s_total;
+    const Tile tl = tiles[blockIdx.x];
+    const DevBox &B = boxes[tl.box];
+    const DevParams &p = pp[0];
+    const DevGrid &g = B.g;
+    const int ntz = (g.nz2 + kDepTZ - 1) / kDepTZ, nty = (g.nny + kDepTY - 1) / kDepTY;
+    const int tzi = tl.start % ntz, tyi = (tl.start / ntz) % nty, txi = tl.start / (ntz * nty);
+    const int x0 = 1 + txi * kDepTX, y0 = 1 + tyi * kDepTY, z0 = tzi * kDepTZ;
+    const int lz = threadIdx.x % kDepTZ, ly = (threadIdx.x / kDepTZ) % kDepTY, lx = threadIdx.x / (kDepTZ * kDepTY);
+    const int ix = x0 + lx, iy = y0 + ly, iz = z0 + lz;
+    const bool valid = ix <= g.nnx && iy <= g.nny && iz <= g.nnz + 1;
+    const long long node = (long long)iz + (long long)g.nz2 * ((long long)(iy - 1) + (long long)g.nny * (ix - 1));
+    double out[6];
+    bool staged = (x0 > 2) && (y0 > 2);
+    if (staged) {
+        const int ck_lo = max(z0 - 1, 0), ck_hi = min(z0 + kDepTZ - 1, g.nnz);
+        // cell starts of the tile's columns (absolute positions in the sorted list)
+        for (int e = threadIdx.x; e < kDepCols * kDepCSW; e += blockDim.x) {
+            const int cc = e / kDepCSW, lzz = e % kDepCSW;
+            const int ci = x0 - 1 + cc / (kDepTY + 1), cj = y0 - 1 + cc % (kDepTY + 1);
+            int v = 0;
+            if (ci <= g.nnx + 1 && cj <= g.nny + 1) {
+                const int ck = min(max(z0 - 1 + lzz, ck_lo), ck_hi + 1);
+                v = B.cell_start[ck + (g.nnz + 1) * ((cj - 1) + (g.nny + 1) * (ci - 1))];
+            }
+            s_cs[e] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int o = 0;
+            for (int cc = 0; cc < kDepCols; ++cc) {
+                s_off[cc] = o;
+                o += s_cs[cc * kDepCSW + kDepCSW - 1] - s_cs[cc * kDepCSW];
+            }
+            s_total = o;
+        }
+        __syncthreads();
+        staged = s_total <= CAP;
+        if (staged) {
+            const DevState &O = B.st[B.cur];
+            for (int k = threadIdx.x; k < s_total; k += blockDim.x) {
+                int cc = 0;
+                while (cc + 1 < kDepCols && s_off[cc + 1] <= k) ++cc;
+                const int t = B.perm[s_cs[cc * kDepCSW] + (k - s_off[cc])];
+                s_lid[k] = O.lid[t];
+                if (MIXED) {
+                    for (int q = 0; q < P32_N; ++q) s_f[q * CAP + k] = B.pay32.f[q][t];
+                } else {
+                    const DevPayload &P = B.pay;
+                    s_v[k] = O.x[0][t];
+                    s_v[CAP + k] = O.x[1][t];
+                    s_v[2 * CAP + k] = O.x[2][t];
+                    for (int q = 0; q < 3; ++q) {
+                        s_v[(3 + q) * CAP + k] = P.D[q][t];
+                        s_v[(6 + q) * CAP + k] = P.V[q][t];
+                    }
+                    s_v[9 * CAP + k] = P.T0[t];
+                    s_v[10 * CAP + k] = P.H0[t];
+                    s_v[11 * CAP + k] = P.E1[t];
+                    s_v[12 * CAP + k] = P.E2[t];
+                    s_v[13 * CAP + k] = P.mult[t];
+                }
+            }
+            __syncthreads();
+            if (valid) {
+                int pos[8], end[8], ck[8], off[8];
+                int n = 0;
+                for (int i = 0; i <= 1; ++i)
+                    for (int j = 0; j <= 1; ++j)
+                        for (int k = 0; k <= 1; ++k) {
+                            const int ckk = iz - k;
+                            if (ckk < 0 || ckk > g.nnz) continue;
+                            const int cc = (lx + 1 - i) * (kDepTY + 1) + (ly + 1 - j);
+                            const int lzz = lz + 1 - k;
+                            const int base = s_off[cc] - s_cs[cc * kDepCSW];
+                            const int a = base + s_cs[cc * kDepCSW + lzz];
+                            const int b = base + s_cs[cc * kDepCSW + lzz + 1];
+                            if (a < b) {
+                                pos[n] = a; end[n] = b; ck[n] = ckk; off[n] = (i << 2) | (j << 1) | k; n++;
+                            }
+                        }
+                merge_ranges<MIXED, true>(B, p, s_lid, s_v, s_f, n, pos, end, ck, off, ix, iy, iz, out);
+            }
+        }
+    }
+    if (!staged && valid) node_global<MIXED>(B, p, ix, iy, iz, out);
+    if (valid)
+        for (int q = 0; q < 6; ++q) B.src[q][node] = out[q];
+}
+
+}  // namespace
+}  // namespace ntlp

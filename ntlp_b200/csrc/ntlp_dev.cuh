@@ -65,12 +65,23 @@ struct DevPayload {
     double *D[3], *V[3], *T0, *H0, *E1, *E2, *mult;
 };
 
+// Mixed-precision payload, FP32: cell-relative position fractions
+// fx = (x - x_node)/dx etc. (the trilinear weights are fx and 1 - fx), the
+// momentum factors D+V, T0, H0, E2-E1 and mult/dV of the reference's
+// contribution P*wtt/dV*mult.
+enum { P32_FX = 0, P32_FY, P32_FZ, P32_DV0, P32_DV1, P32_DV2, P32_T0, P32_H0, P32_E, P32_FAC, P32_N };
+struct DevPayload32 {
+    float *f[P32_N];
+};
+
 struct DevBox {
     DevGrid g;
     const double *f[5];    // u v w T q, halo-padded FP64
-    const float *f32[5];   // FP32 copies (mixed path)
+    const float4 *f4;      // mixed path: (u, v, T, q) deviations packed per point
+    const float *fw;       // mixed path: w deviation
     DevState st[2];
     DevPayload pay;
+    DevPayload32 pay32;    // mixed path
     int cur;               // buffer holding the current state
     int cap;
     int *n_alive;          // droplets in the current state
@@ -84,6 +95,8 @@ struct DevBox {
     long long *flux_fx;    // [2][nnz+1][kFluxLimbs]
     double *src[6];        // [nnodes] each, column layout
     int *err;              // device error word (0 = fine)
+    int *defer;            // [cap] droplets whose Gauss-Newton solve failed this step
+    int *ndefer;           // their count
 };
 
 // ---- binning ---------------------------------------------------------------
@@ -142,7 +155,7 @@ __device__ __forceinline__ double cube(double r) { return (r * r) * r; }
 // The FP32 field copies hold deviations from the value at the interior
 // point (k, j, i) = (1, 1, 1): T ~ 293 K would otherwise keep only ~3e-5 K
 // in FP32, and the saturation vapour pressure is exponential in T.
-__device__ __forceinline__ long long f32_ref_index(const DevGrid &g) {
+__host__ __device__ __forceinline__ long long f32_ref_index(const DevGrid &g) {
     return 1LL + (long long)g.nz2 * (2LL + (long long)g.ny5 * 2LL);
 }
 

@@ -14,6 +14,7 @@
 #include "ntlp_dev.cuh"
 #include "ntlp_kernels.h"
 #include "ntlp_physics.cuh"
+#include "ntlp_deposit.cuh"
 
 namespace ntlp {
 
@@ -77,15 +78,19 @@ __device__ void interp_lin64(const DevBox &B, double x1, double x2, double x3, I
 }
 
 // Lagrange weights over 6 nodes (particles.f90:612-624 and 682-689):
-// w_j = prod_{k != j} (x - x_k)/(x_j - x_k), evaluated left to right.
+// w_j = prod_{k != j} (x - x_k)/(x_j - x_k) over k = first..last (Fortran
+// numbering), evaluated left to right; weights outside first..last are 0.
+// Fully unrolled with predicated factors so the arrays stay in registers.
 __device__ __forceinline__ void lagrange6(double x, const double xn[6], int first, int last, double w[6]) {
-    for (int j = 0; j < 6; ++j) w[j] = 0.0;
-    for (int j = first; j <= last && first > 0; ++j) {
-        double xj = xn[j - 1];
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+        const bool jin = (j + 1 >= first) && (j + 1 <= last);
         double pj = 1.0;
-        for (int k = first; k <= last; ++k)
-            if (j != k) pj = pj * (x - xn[k - 1]) / (xj - xn[k - 1]);
-        w[j - 1] = pj;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            if (k != j && jin && k + 1 >= first && k + 1 <= last) pj = pj * (x - xn[k]) / (xn[j] - xn[k]);
+        }
+        w[j] = jin ? pj : 0.0;
     }
 }
 
@@ -143,51 +148,108 @@ __device__ void interp6_64(const DevBox &B, double x1, double x2, double x3, Int
         }
         lagrange6(x3, zn, first, last, wzw);
     }
+    // index offsets per axis (x: periodic image of column nnx+4 and clamping
+    // of anything outside the padded array, as ext_index does per read)
+    long long xo[6];
+    int yo[6];
+#pragma unroll
+    for (int a = 0; a < 6; ++a) {
+        int ix = ip3 + (a - 2), iy = jp3 + (a - 2);
+        if (ix > g.nnx + 3) ix -= g.nnx;
+        if (iy > g.nny + 3) iy -= g.nny;
+        if (ix < -1 || ix > g.nnx + 3) { bad = 1; ix = ix < -1 ? -1 : g.nnx + 3; }
+        if (iy < -1 || iy > g.nny + 3) { bad = 1; iy = iy < -1 ? -1 : g.nny + 3; }
+        xo[a] = (long long)g.nz2 * g.ny5 * (ix + 1);
+        yo[a] = g.nz2 * (iy + 1);
+        if (ku[a] < 0 || ku[a] > nnz + 1) { bad = 1; ku[a] = ku[a] < 0 ? 0 : nnz + 1; }
+        if (kw[a] < 0 || kw[a] > nnz + 1) { bad = 1; kw[a] = kw[a] < 0 ? 0 : nnz + 1; }
+    }
     const double *fu = B.f[0], *fv = B.f[1], *fw = B.f[2], *fT = B.f[3], *fq = B.f[4];
     double u1 = 0.0, u2 = 0.0, u3 = 0.0, T = 0.0, q = 0.0;
+    // reference order: k outer, j, i inner; k and j stay rolled, their
+    // per-iteration values rotated through slot 0
+#pragma unroll 1
     for (int k = 0; k < 6; ++k) {
-        const int izuv = ku[k], izw = kw[k];
-        const double wk = wz[k], wkw = wzw[k];
+        const int izuv = ku[0], izw = kw[0];
+        const double wk = wz[0], wkw = wzw[0];
+        double wyr[6];
+        int yor[6];
+#pragma unroll
+        for (int r = 0; r < 6; ++r) { wyr[r] = wy[r]; yor[r] = yo[r]; }
+#pragma unroll 1
         for (int j = 0; j < 6; ++j) {
-            const int iy = jp3 + (j - 2);
-            const double wj = wy[j];
+            const double wj = wyr[0];
+            const long long bu = izuv + yor[0], bw = izw + yor[0];
+#pragma unroll
             for (int i = 0; i < 6; ++i) {
-                const int ix = ip3 + (i - 2);
                 const double wi = wx[i];
-                long long a = ext_index(g, izuv, iy, ix, bad);
-                long long aw = ext_index(g, izw, iy, ix, bad);
+                const long long a = bu + xo[i], aw = bw + xo[i];
                 u1 = u1 + __ldg(fu + a) * wi * wj * wk;
                 u2 = u2 + __ldg(fv + a) * wi * wj * wk;
                 u3 = u3 + __ldg(fw + aw) * wi * wj * wkw;
                 T = T + __ldg(fT + a) * wi * wj * wk;
                 q = q + __ldg(fq + a) * wi * wj * wk;
             }
+#pragma unroll
+            for (int r = 0; r < 5; ++r) { wyr[r] = wyr[r + 1]; yor[r] = yor[r + 1]; }
+        }
+#pragma unroll
+        for (int r = 0; r < 5; ++r) {
+            ku[r] = ku[r + 1]; kw[r] = kw[r + 1]; wz[r] = wz[r + 1]; wzw[r] = wzw[r + 1];
         }
     }
     o.uf[0] = u1; o.uf[1] = u2; o.uf[2] = u3; o.Tf = T; o.qinf = q;
 }
 
 // ---------------------------------------------------------------------------
-// backward-Euler droplet update (particles.f90:3043-3242, 3248-3260)
+// backward-Euler droplet update (particles.f90:3043-3242, 3248-3260) as three
+// launches: interpolation, droplet body with Gauss-Newton, deferred
+// Levenberg-Marquardt droplets.
 // ---------------------------------------------------------------------------
 template <int ILIN>
 __global__ void __launch_bounds__(kUpdateThreads)
-k_update_be64(DevBox *boxes, const Tile *tiles, const DevParams *pp, StepIn in) {
+k_interp64(DevBox *boxes, const Tile *tiles) {
     const Tile tl = tiles[blockIdx.x];
     const DevBox &B = boxes[tl.box];
-    const DevParams &p = pp[0];
+    const int t = tl.start + threadIdx.x;
+    if (t >= *B.n_alive) return;
+    const DevState &S = B.st[B.cur];
+    const DevState &O = B.st[1 - B.cur];
+    const int s = B.perm[t];
+    Interp I;
+    int bad = 0;
+    if (ILIN == 1) interp_lin64(B, S.x[0][s], S.x[1][s], S.x[2][s], I, bad);
+    else interp6_64(B, S.x[0][s], S.x[1][s], S.x[2][s], I, bad);
+    O.uf[0][t] = I.uf[0];
+    O.uf[1][t] = I.uf[1];
+    O.uf[2][t] = I.uf[2];
+    O.Tf[t] = I.Tf;
+    O.qinf[t] = I.qinf;
+    B.key[t] = bad;
+}
+
+__global__ void __launch_bounds__(kUpdateThreads, 4)
+k_be64(DevBox *boxes, const Tile *tiles, const DevParams *pp, StepIn in) {
+    const Tile tl = tiles[blockIdx.x];
+    const DevBox &B = boxes[tl.box];
     Counts cnt;
     for (int k = 0; k < kNumCounters; ++k) cnt.v[k] = 0;
     const int t = tl.start + threadIdx.x;
-    if (t < *B.n_alive) {
-        const DevState &S = B.st[B.cur];
-        const int s = B.perm[t];
-        double x[3] = {S.x[0][s], S.x[1][s], S.x[2][s]};
-        Interp I;
-        int bad = 0;
-        if (ILIN == 1) interp_lin64(B, x[0], x[1], x[2], I, bad);
-        else interp6_64(B, x[0], x[1], x[2], I, bad);
-        be_body<false>(B, p, in, t, s, x, I, bad, cnt);
+    if (t < *B.n_alive) be_body<false, false>(B, pp[0], in, t, B.perm[t], cnt);
+    block_add_counters(B, cnt);
+}
+
+// droplets whose Gauss-Newton solve failed: the full body with the
+// Levenberg-Marquardt fallback (grid.y = box)
+__global__ void __launch_bounds__(kUpdateThreads)
+k_be_defer64(DevBox *boxes, const DevParams *pp, StepIn in) {
+    const DevBox &B = boxes[blockIdx.y];
+    Counts cnt;
+    for (int k = 0; k < kNumCounters; ++k) cnt.v[k] = 0;
+    const int nd = *B.ndefer;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nd; i += gridDim.x * blockDim.x) {
+        const int t = B.defer[i];
+        be_body<false, true>(B, pp[0], in, t, B.perm[t], cnt);
     }
     block_add_counters(B, cnt);
 }
@@ -327,116 +389,17 @@ __global__ void k_payload64(DevBox *boxes, const Tile *tiles, const DevParams *p
 }
 
 // ---------------------------------------------------------------------------
-// deterministic deposition (particles.f90:1151-1276 + fold :1078-1113)
-// ---------------------------------------------------------------------------
-// One thread per output node.  The node's value is the reference's: the
-// sum, in list order (ascending lid), of the contributions of the droplets
-// in its (up to) 8 neighbouring cells at each of its pre-fold images
-// (ix, iy), (ix+nnx, iy), (ix, iy+nny), (ix+nnx, iy+nny), combined in the
-// order of the periodic fold.  Cell lists are lid-sorted, so each image is
-// an 8-way merge.
-struct Acc {
-    double s[6];
-};
-
-__device__ __forceinline__ void deposit_image(const DevBox &B, const DevParams &p, int px, int py, int pz,
-                                              Acc &acc) {
-    const DevGrid &g = B.g;
-    for (int q = 0; q < 6; ++q) acc.s[q] = 0.0;
-    int pos[8], end[8], head[8], ck[8];
-    int ncur = 0;
-    for (int i = 0; i <= 1; ++i)
-        for (int j = 0; j <= 1; ++j)
-            for (int k = 0; k <= 1; ++k) {
-                int ci = px - i, cj = py - j, ckk = pz - k;
-                if (ci < 1 || ci > g.nnx + 1 || cj < 1 || cj > g.nny + 1 || ckk < 0 || ckk > g.nnz) continue;
-                int key = ckk + (g.nnz + 1) * ((cj - 1) + (g.nny + 1) * (ci - 1));
-                int a = B.cell_start[key], b = B.cell_start[key + 1];
-                if (a < b) {
-                    pos[ncur] = a;
-                    end[ncur] = b;
-                    ck[ncur] = ckk;
-                    ncur++;
-                }
-            }
-    if (ncur == 0) return;
-    const DevState &O = B.st[B.cur];   // after the finish kernel: the new state, cell lists in perm
-    for (int c = 0; c < ncur; ++c) head[c] = O.lid[B.perm[pos[c]]];
-    const double dx = g.dx, dy = g.dy;
-    const double xv = dx * (double)(px - 1);
-    const double yv = dy * (double)(py - 1);
-    const double zv = g.zz[pz];
-    const DevPayload &P = B.pay;
-    while (true) {
-        int best = -1, bl = 0x7fffffff;
-        for (int c = 0; c < ncur; ++c)
-            if (pos[c] < end[c] && head[c] < bl) { bl = head[c]; best = c; }
-        if (best < 0) break;
-        const int t = B.perm[pos[best]];
-        const int kpt = ck[best];
-        pos[best]++;
-        if (pos[best] < end[best]) head[best] = O.lid[B.perm[pos[best]]];
-        const double x1 = O.x[0][t], x2 = O.x[1][t], x3 = O.x[2][t];
-        const double wtx = (1.0 - fabs(x1 - xv) / dx);
-        const double wty = (1.0 - fabs(x2 - yv) / dy);
-        const double wtz = (1.0 - fabs(x3 - zv) / g.dzu[kpt + 1]);
-        const double wtt = wtx * wty * wtz;
-        const double dV = dx * dy * g.dzu[kpt + 1];
-        const double mult = P.mult[t];
-        if (p.icouple == 1) {
-            for (int a = 0; a < 3; ++a) {
-                acc.s[a] = acc.s[a] - P.D[a][t] * wtt / dV * mult;
-                acc.s[a] = acc.s[a] - P.V[a][t] * wtt / dV * mult;
-            }
-        }
-        if (p.iTcouple == 1) acc.s[3] = acc.s[3] - P.T0[t] * wtt / dV * mult;
-        if (p.iHcouple == 1) {
-            acc.s[4] = acc.s[4] - P.H0[t] * wtt / dV * mult;
-            acc.s[5] = acc.s[5] - P.E1[t] * wtt / dV * mult + P.E2[t] * wtt / dV * mult;
-        }
-    }
-}
-
-__global__ void __launch_bounds__(kDepositThreads)
-k_deposit64(DevBox *boxes, const Tile *tiles, const DevParams *pp) {
-    const Tile tl = tiles[blockIdx.x];
-    const DevBox &B = boxes[tl.box];
-    const DevParams &p = pp[0];
-    const long long node = (long long)tl.start + threadIdx.x;
-    const DevGrid &g = B.g;
-    if (node >= g.nnodes) return;
-    const int iz = (int)(node % g.nz2);
-    const long long rest = node / g.nz2;
-    const int iy = (int)(rest % g.nny) + 1;
-    const int ix = (int)(rest / g.nny) + 1;
-    Acc a0, a1;
-    deposit_image(B, p, ix, iy, iz, a0);
-    if (ix <= 2) {
-        deposit_image(B, p, ix + g.nnx, iy, iz, a1);
-        for (int q = 0; q < 6; ++q) a0.s[q] = a0.s[q] + a1.s[q];
-    }
-    if (iy <= 2) {
-        Acc b0;
-        deposit_image(B, p, ix, iy + g.nny, iz, b0);
-        if (ix <= 2) {
-            deposit_image(B, p, ix + g.nnx, iy + g.nny, iz, a1);
-            for (int q = 0; q < 6; ++q) b0.s[q] = b0.s[q] + a1.s[q];
-        }
-        for (int q = 0; q < 6; ++q) a0.s[q] = a0.s[q] + b0.s[q];
-    }
-    for (int q = 0; q < 6; ++q) B.src[q][node] = a0.s[q];
-}
-
-// ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
-void launch_update_be64(int ilin, DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp,
+void launch_update_be64(int ilin, DevBox *boxes, const Tile *tiles, int ntiles, int nbox, const DevParams *pp,
                         StepIn in, cudaStream_t st) {
     if (ntiles <= 0) return;
     if (ilin == 1)
-        k_update_be64<1><<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles, pp, in);
+        k_interp64<1><<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles);
     else
-        k_update_be64<0><<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles, pp, in);
+        k_interp64<0><<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles);
+    k_be64<<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles, pp, in);
+    k_be_defer64<<<dim3(kDeferBlocks, nbox), kUpdateThreads, 0, st>>>(boxes, pp, in);
 }
 
 void launch_update_rk3_64(int ilin, DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp,
@@ -456,7 +419,12 @@ void launch_payload64(DevBox *boxes, const Tile *tiles, int ntiles, const DevPar
 
 void launch_deposit64(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp, cudaStream_t st) {
     if (ntiles <= 0) return;
-    k_deposit64<<<ntiles, kDepositThreads, 0, st>>>(boxes, tiles, pp);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_deposit_tiled<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (false ? kDepSmemMixed : kDepSmem64));
+        attr = true;
+    }
+    k_deposit_tiled<false><<<ntiles, kDepositThreads, (false ? kDepSmemMixed : kDepSmem64), st>>>(boxes, tiles, pp);
 }
 
 }  // namespace ntlp

@@ -19,24 +19,27 @@
 #include "ntlp_dev.cuh"
 #include "ntlp_kernels.h"
 #include "ntlp_physics.cuh"
+#include "ntlp_deposit.cuh"
 
 namespace ntlp {
 
 // Lagrange weights on six nodes from FP64 offsets d[k] = x - x_k and node
-// differences, in FP32.
+// differences, in FP32; unrolled with predicated factors (registers only).
 __device__ __forceinline__ void lagrange6_f(const double x, const double xn[6], int first, int last, float w[6]) {
-    for (int j = 0; j < 6; ++j) w[j] = 0.0f;
-    if (first <= 0) return;
     float d[6];
+#pragma unroll
     for (int k = 0; k < 6; ++k) d[k] = (float)(x - xn[k]);
-    for (int j = first; j <= last; ++j) {
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+        const bool jin = (j + 1 >= first) && (j + 1 <= last);
         float num = 1.0f, den = 1.0f;
-        for (int k = first; k <= last; ++k)
-            if (k != j) {
-                num *= d[k - 1];
-                den *= (float)(xn[j - 1] - xn[k - 1]);
-            }
-        w[j - 1] = num / den;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            const bool use = k != j && k + 1 >= first && k + 1 <= last;
+            num *= use ? d[k] : 1.0f;
+            den *= use ? (float)(xn[j] - xn[k]) : 1.0f;
+        }
+        w[j] = jin ? num / den : 0.0f;
     }
 }
 
@@ -94,13 +97,19 @@ __device__ void interp6_mixed(const DevBox &B, double x1, double x2, double x3, 
         lagrange6_f(x3, zn, first, last, wzw);
     }
     if (ku[2] < 0 || ku[2] > nnz + 1 || kw[2] < 0) bad = 1;
-    const float *fu = B.f32[0], *fv = B.f32[1], *fw = B.f32[2], *fT = B.f32[3], *fq = B.f32[4];
+    const float4 *f4 = B.f4;
+    const float *fw = B.fw;
     float su = 0.f, sv = 0.f, sw = 0.f, sT = 0.f, sq = 0.f;
+    // the x loop stays rolled (one column plane of loads in flight at a
+    // time); its weight is rotated through wx[0] so no array is indexed
+    // dynamically
+#pragma unroll 1
     for (int i = 0; i < 6; ++i) {
         int ix = ip3 + (i - 2);
         if (ix > g.nnx + 3) ix -= g.nnx;
         if (ix < -1 || ix > g.nnx + 3) { bad = 1; ix = ix < -1 ? -1 : g.nnx + 3; }
         float cu = 0.f, cv = 0.f, cw = 0.f, cT = 0.f, cq = 0.f;
+#pragma unroll
         for (int j = 0; j < 6; ++j) {
             int iy = jp3 + (j - 2);
             if (iy > g.nny + 3) iy -= g.nny;
@@ -109,11 +118,11 @@ __device__ void interp6_mixed(const DevBox &B, double x1, double x2, double x3, 
             float au = 0.f, av = 0.f, aT = 0.f, aq = 0.f, aw = 0.f;
 #pragma unroll
             for (int k = 0; k < 6; ++k) {
-                const long long a = base + ku[k];
-                au = fmaf(__ldg(fu + a), wz[k], au);
-                av = fmaf(__ldg(fv + a), wz[k], av);
-                aT = fmaf(__ldg(fT + a), wz[k], aT);
-                aq = fmaf(__ldg(fq + a), wz[k], aq);
+                const float4 val = __ldg(f4 + base + ku[k]);
+                au = fmaf(val.x, wz[k], au);
+                av = fmaf(val.y, wz[k], av);
+                aT = fmaf(val.z, wz[k], aT);
+                aq = fmaf(val.w, wz[k], aq);
                 aw = fmaf(__ldg(fw + base + kw[k]), wzw[k], aw);
             }
             cu = fmaf(au, wy[j], cu);
@@ -122,11 +131,13 @@ __device__ void interp6_mixed(const DevBox &B, double x1, double x2, double x3, 
             cT = fmaf(aT, wy[j], cT);
             cq = fmaf(aq, wy[j], cq);
         }
-        su = fmaf(cu, wx[i], su);
-        sv = fmaf(cv, wx[i], sv);
-        sw = fmaf(cw, wx[i], sw);
-        sT = fmaf(cT, wx[i], sT);
-        sq = fmaf(cq, wx[i], sq);
+        su = fmaf(cu, wx[0], su);
+        sv = fmaf(cv, wx[0], sv);
+        sw = fmaf(cw, wx[0], sw);
+        sT = fmaf(cT, wx[0], sT);
+        sq = fmaf(cq, wx[0], sq);
+#pragma unroll
+        for (int r = 0; r < 5; ++r) wx[r] = wx[r + 1];
     }
     const long long ridx = f32_ref_index(g);
     o.uf[0] = B.f[0][ridx] + (double)su;
@@ -157,7 +168,8 @@ __device__ void interp_lin_mixed(const DevBox &B, double x1, double x2, double x
         wz[i] = 1.0f - fabsf((float)(x3 - zv)) / (float)g.dzu[kpt + 1];
         wzw[i] = 1.0f - fabsf((float)(x3 - zwv)) / (float)g.dzw[kwpt + 1];
     }
-    const float *fu = B.f32[0], *fv = B.f32[1], *fw = B.f32[2], *fT = B.f32[3], *fq = B.f32[4];
+    const float4 *f4 = B.f4;
+    const float *fw = B.fw;
     float u1 = 0.f, u2 = 0.f, u3 = 0.f, T = 0.f, q = 0.f;
     int ix = 0, iy = 0;
     for (int i = 0; i <= 1; ++i) {
@@ -168,21 +180,18 @@ __device__ void interp_lin_mixed(const DevBox &B, double x1, double x2, double x
                 iy = jpt + j;
                 long long a = ext_index(g, kpt + k, iy, ix, bad);
                 long long aw = ext_index(g, kwpt + k, iy, ix, bad);
-                u1 = fmaf(__ldg(fu + a), wxy * wz[k], u1);
-                u2 = fmaf(__ldg(fv + a), wxy * wz[k], u2);
+                const float4 val = __ldg(f4 + a);
+                u1 = fmaf(val.x, wxy * wz[k], u1);
+                u2 = fmaf(val.y, wxy * wz[k], u2);
                 u3 = fmaf(__ldg(fw + aw), wxy * wzw[k], u3);
-                T = fmaf(__ldg(fT + a), wxy * wz[k], T);
-                q = fmaf(__ldg(fq + a), wxy * wz[k], q);
+                T = fmaf(val.z, wxy * wz[k], T);
+                q = fmaf(val.w, wxy * wz[k], q);
             }
             // zeroth order between the last u level and the wall (same
             // override rule as particles.f90:831-842)
-            if (kpt == g.nnz) {
-                long long a = ext_index(g, kpt, iy, ix, bad);
-                u1 = __ldg(fu + a); u2 = __ldg(fv + a); T = __ldg(fT + a); q = __ldg(fq + a);
-            }
-            if (kpt == 0) {
-                long long a = ext_index(g, 1, iy, ix, bad);
-                u1 = __ldg(fu + a); u2 = __ldg(fv + a); T = __ldg(fT + a); q = __ldg(fq + a);
+            if (kpt == g.nnz || kpt == 0) {
+                const float4 val = __ldg(f4 + ext_index(g, kpt == 0 ? 1 : kpt, iy, ix, bad));
+                u1 = val.x; u2 = val.y; T = val.z; q = val.w;
             }
         }
     }
@@ -195,119 +204,92 @@ __device__ void interp_lin_mixed(const DevBox &B, double x1, double x2, double x
 }
 
 template <int ILIN>
-__global__ void __launch_bounds__(kUpdateThreads)
-k_update_be_mixed(DevBox *boxes, const Tile *tiles, const DevParams *pp, StepIn in) {
+__global__ void __launch_bounds__(kUpdateThreads, 4)
+k_interp_mixed(DevBox *boxes, const Tile *tiles) {
     const Tile tl = tiles[blockIdx.x];
     const DevBox &B = boxes[tl.box];
-    const DevParams &p = pp[0];
+    const int t = tl.start + threadIdx.x;
+    if (t >= *B.n_alive) return;
+    const DevState &S = B.st[B.cur];
+    const DevState &O = B.st[1 - B.cur];
+    const int s = B.perm[t];
+    Interp I;
+    int bad = 0;
+    if (ILIN == 1) interp_lin_mixed(B, S.x[0][s], S.x[1][s], S.x[2][s], I, bad);
+    else interp6_mixed(B, S.x[0][s], S.x[1][s], S.x[2][s], I, bad);
+    O.uf[0][t] = I.uf[0];
+    O.uf[1][t] = I.uf[1];
+    O.uf[2][t] = I.uf[2];
+    O.Tf[t] = I.Tf;
+    O.qinf[t] = I.qinf;
+    B.key[t] = bad;
+}
+
+__global__ void __launch_bounds__(kUpdateThreads, 4)
+k_be_mixed(DevBox *boxes, const Tile *tiles, const DevParams *pp, StepIn in) {
+    const Tile tl = tiles[blockIdx.x];
+    const DevBox &B = boxes[tl.box];
     Counts cnt;
     for (int k = 0; k < kNumCounters; ++k) cnt.v[k] = 0;
     const int t = tl.start + threadIdx.x;
-    if (t < *B.n_alive) {
-        const DevState &S = B.st[B.cur];
-        const int s = B.perm[t];
-        double x[3] = {S.x[0][s], S.x[1][s], S.x[2][s]};
-        Interp I;
-        int bad = 0;
-        if (ILIN == 1) interp_lin_mixed(B, x[0], x[1], x[2], I, bad);
-        else interp6_mixed(B, x[0], x[1], x[2], I, bad);
-        be_body<true>(B, p, in, t, s, x, I, bad, cnt);
+    if (t < *B.n_alive) be_body<true, false>(B, pp[0], in, t, B.perm[t], cnt);
+    block_add_counters(B, cnt);
+}
+
+__global__ void __launch_bounds__(kUpdateThreads)
+k_be_defer_mixed(DevBox *boxes, const DevParams *pp, StepIn in) {
+    const DevBox &B = boxes[blockIdx.y];
+    Counts cnt;
+    for (int k = 0; k < kNumCounters; ++k) cnt.v[k] = 0;
+    const int nd = *B.ndefer;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nd; i += gridDim.x * blockDim.x) {
+        const int t = B.defer[i];
+        be_body<true, true>(B, pp[0], in, t, B.perm[t], cnt);
     }
     block_add_counters(B, cnt);
 }
 
-// Deposition with FP32 weights and one FP64 divide per contribution; the
-// accumulation is FP64 and in list order, as in the FP64 kernel.
-__device__ __forceinline__ void deposit_image_mixed(const DevBox &B, const DevParams &p, int px, int py, int pz,
-                                                    double acc[6]) {
-    const DevGrid &g = B.g;
-    for (int q = 0; q < 6; ++q) acc[q] = 0.0;
-    int pos[8], end[8], head[8], ck[8];
-    int ncur = 0;
-    for (int i = 0; i <= 1; ++i)
-        for (int j = 0; j <= 1; ++j)
-            for (int k = 0; k <= 1; ++k) {
-                int ci = px - i, cj = py - j, ckk = pz - k;
-                if (ci < 1 || ci > g.nnx + 1 || cj < 1 || cj > g.nny + 1 || ckk < 0 || ckk > g.nnz) continue;
-                int key = ckk + (g.nnz + 1) * ((cj - 1) + (g.nny + 1) * (ci - 1));
-                int a = B.cell_start[key], b = B.cell_start[key + 1];
-                if (a < b) {
-                    pos[ncur] = a; end[ncur] = b; ck[ncur] = ckk; ncur++;
-                }
-            }
-    if (ncur == 0) return;
-    const DevState &O = B.st[B.cur];
-    for (int c = 0; c < ncur; ++c) head[c] = O.lid[B.perm[pos[c]]];
-    const double xv = g.dx * (double)(px - 1);
-    const double yv = g.dy * (double)(py - 1);
-    const double zv = g.zz[pz];
-    const float rdx = (float)(1.0 / g.dx), rdy = (float)(1.0 / g.dy);
-    const DevPayload &P = B.pay;
-    while (true) {
-        int best = -1, bl = 0x7fffffff;
-        for (int c = 0; c < ncur; ++c)
-            if (pos[c] < end[c] && head[c] < bl) { bl = head[c]; best = c; }
-        if (best < 0) break;
-        const int t = B.perm[pos[best]];
-        const int kpt = ck[best];
-        pos[best]++;
-        if (pos[best] < end[best]) head[best] = O.lid[B.perm[pos[best]]];
-        const float wtx = 1.0f - fabsf((float)(O.x[0][t] - xv)) * rdx;
-        const float wty = 1.0f - fabsf((float)(O.x[1][t] - yv)) * rdy;
-        const float wtz = 1.0f - fabsf((float)(O.x[2][t] - zv)) / (float)g.dzu[kpt + 1];
-        const double fac = ((double)(wtx * wty * wtz) * P.mult[t]) / (g.dx * g.dy * g.dzu[kpt + 1]);
-        if (p.icouple == 1)
-            for (int a = 0; a < 3; ++a) acc[a] -= (P.D[a][t] + P.V[a][t]) * fac;
-        if (p.iTcouple == 1) acc[3] -= P.T0[t] * fac;
-        if (p.iHcouple == 1) {
-            acc[4] -= P.H0[t] * fac;
-            acc[5] += (P.E2[t] - P.E1[t]) * fac;
-        }
-    }
-}
-
-__global__ void __launch_bounds__(kDepositThreads)
-k_deposit_mixed(DevBox *boxes, const Tile *tiles, const DevParams *pp) {
-    const Tile tl = tiles[blockIdx.x];
-    const DevBox &B = boxes[tl.box];
-    const DevParams &p = pp[0];
-    const long long node = (long long)tl.start + threadIdx.x;
-    const DevGrid &g = B.g;
-    if (node >= g.nnodes) return;
-    const int iz = (int)(node % g.nz2);
-    const long long rest = node / g.nz2;
-    const int iy = (int)(rest % g.nny) + 1;
-    const int ix = (int)(rest / g.nny) + 1;
-    double a0[6], a1[6];
-    deposit_image_mixed(B, p, ix, iy, iz, a0);
-    if (ix <= 2) {
-        deposit_image_mixed(B, p, ix + g.nnx, iy, iz, a1);
-        for (int q = 0; q < 6; ++q) a0[q] += a1[q];
-    }
-    if (iy <= 2) {
-        double b0[6];
-        deposit_image_mixed(B, p, ix, iy + g.nny, iz, b0);
-        if (ix <= 2) {
-            deposit_image_mixed(B, p, ix + g.nnx, iy + g.nny, iz, a1);
-            for (int q = 0; q < 6; ++q) b0[q] += a1[q];
-        }
-        for (int q = 0; q < 6; ++q) a0[q] += b0[q];
-    }
-    for (int q = 0; q < 6; ++q) B.src[q][node] = a0[q];
-}
-
-void launch_update_be_mixed(int ilin, DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp,
-                            StepIn in, cudaStream_t st) {
+void launch_update_be_mixed(int ilin, DevBox *boxes, const Tile *tiles, int ntiles, int nbox,
+                            const DevParams *pp, StepIn in, cudaStream_t st) {
     if (ntiles <= 0) return;
     if (ilin == 1)
-        k_update_be_mixed<1><<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles, pp, in);
+        k_interp_mixed<1><<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles);
     else
-        k_update_be_mixed<0><<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles, pp, in);
+        k_interp_mixed<0><<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles);
+    k_be_mixed<<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles, pp, in);
+    k_be_defer_mixed<<<dim3(kDeferBlocks, nbox), kUpdateThreads, 0, st>>>(boxes, pp, in);
+}
+
+// Mixed payload from the stored state, for a coupling call whose dt differs
+// from the step's (runs after the finish kernel: st[cur] is the new state).
+__global__ void k_payload_mixed(DevBox *boxes, const Tile *tiles, const DevParams *pp, double dt) {
+    const Tile tl = tiles[blockIdx.x];
+    const DevBox &B = boxes[tl.box];
+    const int t = tl.start + threadIdx.x;
+    if (t >= *B.n_alive) return;
+    const DevState &S = B.st[B.cur];
+    const int s = B.perm[t];
+    double x[3], v[3], vold[3];
+    for (int a = 0; a < 3; ++a) { x[a] = S.x[a][s]; v[a] = S.v[a][s]; vold[a] = S.vold[a][s]; }
+    int ipt, jpt, kpt;
+    if (cell_key(B.g, x[0], x[1], x[2], &ipt, &jpt, &kpt) >= (int)B.g.ncells) return;
+    write_payload_mixed(B, pp[0], s, ipt, jpt, kpt, x, v, vold, S.r[s], S.rold[s], S.Tp[s], S.Tpold[s], S.Tf[s],
+                        S.m_s[s], S.mult[s], dt);
+}
+
+void launch_payload_mixed(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp, double dt,
+                          cudaStream_t st) {
+    if (ntiles > 0) k_payload_mixed<<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles, pp, dt);
 }
 
 void launch_deposit_mixed(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp, cudaStream_t st) {
     if (ntiles <= 0) return;
-    k_deposit_mixed<<<ntiles, kDepositThreads, 0, st>>>(boxes, tiles, pp);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_deposit_tiled<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (true ? kDepSmemMixed : kDepSmem64));
+        attr = true;
+    }
+    k_deposit_tiled<true><<<ntiles, kDepositThreads, (true ? kDepSmemMixed : kDepSmem64), st>>>(boxes, tiles, pp);
 }
 
 }  // namespace ntlp

@@ -55,7 +55,7 @@ constexpr long long kOffPay = kOffInts + align256(4 * kMaxN * 4);               
 constexpr long long kOffCells = kOffPay + align256(11 * kMaxN * 8);
 constexpr long long kDropTiles = kMaxN / kUpdateThreads + 1;
 constexpr long long kCellTiles = (kMaxCells + 2) / kScanTile + 2;
-constexpr long long kNodeTiles = kMaxNodes / kDepositThreads + 2;
+constexpr long long kNodeTiles = kMaxCells / 4 + 2;   // deposit tiles <= cells/4
 constexpr long long kOffTiles = kOffCells + align256((2 * kMaxCells + 5) * 4);
 constexpr long long kOffSums = kOffTiles + align256((kDropTiles + kCellTiles + kNodeTiles) * sizeof(Tile));
 constexpr long long kScratchBytes = kOffSums + align256(kCellTiles * 8 + 2 * 4);
@@ -119,6 +119,8 @@ extern "C" int ntlp_coupling_noalloc(const ntlp_grid *grid, const ntlp_params *p
     if (grid->nnz > kMaxNz) return reject("nnz", grid->nnz, kMaxNz);
     if (ncells > kMaxCells) return reject("cell count (nnx+1)(nny+1)(nnz+1)", ncells, kMaxCells);
     if (nnodes > kMaxNodes) return reject("node count (nnz+2)*nny*nnx", nnodes, kMaxNodes);
+    if (deposit_tile_count(grid->nnx, grid->nny, grid->nnz) > kNodeTiles)
+        return reject("deposition tiles", deposit_tile_count(grid->nnx, grid->nny, grid->nnz), kNodeTiles);
     if (n > 0) {
         for (int a = 0; a < 3; ++a)
             if (!d->xp[a] || !d->vp[a] || !d->vp_old[a]) return NTLP_ERR_ARG;
@@ -191,7 +193,7 @@ extern "C" int ntlp_coupling_noalloc(const ntlp_grid *grid, const ntlp_params *p
     Tile *tiles = (Tile *)(S + kOffTiles);
     const int nd = (int)((n + kUpdateThreads - 1) / kUpdateThreads) + (n == 0 ? 1 : 0);
     const int nc = (int)((ncells + 2 + kScanTile - 1) / kScanTile);
-    const int nn = (int)((nnodes + kDepositThreads - 1) / kDepositThreads);
+    const int nn = (int)deposit_tile_count(grid->nnx, grid->nny, grid->nnz);
     Tile *drop_tiles = tiles, *cell_tiles = tiles + kDropTiles, *node_tiles = tiles + kDropTiles + kCellTiles;
     long long *sums = (long long *)(S + kOffSums);
     int *box_first = (int *)(S + kOffSums + kCellTiles * 8);
@@ -218,7 +220,7 @@ extern "C" int ntlp_coupling_noalloc(const ntlp_grid *grid, const ntlp_params *p
     }
     k_na_tiles<<<(nd + 255) / 256, 256, 0, st>>>(drop_tiles, nd, kUpdateThreads);
     k_na_tiles<<<(nc + 255) / 256, 256, 0, st>>>(cell_tiles, nc, kScanTile);
-    k_na_tiles<<<(nn + 255) / 256, 256, 0, st>>>(node_tiles, nn, kDepositThreads);
+    k_na_tiles<<<(nn + 255) / 256, 256, 0, st>>>(node_tiles, nn, 1);
     if (n_int > 0) k_na_iota<<<(n_int + 255) / 256, 256, 0, st>>>(lid, n_int);
 
     SortPlan plan{};

@@ -345,77 +345,138 @@ __device__ __forceinline__ void write_payload(const DevBox &B, const DevParams &
 
 // ---------------------------------------------------------------------------
 // backward-Euler droplet body (particles.f90:3043-3242 + 3248-3260): all of
-// the per-droplet work after the interpolation.  MIXED computes the drag
+// the per-droplet work after the interpolation, which an earlier kernel has
+// written to the output buffer at the droplet's slot t (uf, Tf before the
+// Exner factor, qinf; out-of-range flag in key[t]).  MIXED computes the drag
 // (taup_i and the implicit velocity update) in FP32; positions, the Newton
 // radius/temperature solve and everything else stay FP64.
+//
+// With ALLOW_LM false, a droplet whose Gauss-Newton solve fails is appended
+// to the box's defer list and left untouched (no output, no counter, no
+// tally); a second pass re-runs it with ALLOW_LM true, where the rare
+// Levenberg-Marquardt fallback (up to 1000 iterations) does not hold back
+// the 31 other droplets of a warp.  Returns 1 if deferred.
 // ---------------------------------------------------------------------------
+// Mixed-precision payload: the same FP64 factors as write_payload, stored
+// as FP32 with the cell-relative fractions that make the trilinear weights.
+__device__ __forceinline__ void write_payload_mixed(const DevBox &B, const DevParams &p, int t, int ipt, int jpt,
+                                                    int kpt, const double x[3], const double v[3],
+                                                    const double vold[3], double r, double rold, double Tp,
+                                                    double Tpold, double Tf, double m_s, long long mult, double dt) {
+    const DevGrid &g = B.g;
+    const double pi2 = p.pi2;
+    double vrhs[3];
+    for (int a = 0; a < 3; ++a) vrhs[a] = (v[a] - vold[a]) / dt;
+    const double radrhs = (r - rold) / dt;
+    const double Tprhs_L = 3.0 * p.Lv / p.Cpp / r * radrhs;
+    const double Tprhs_s = (Tp - Tpold) / dt - Tprhs_L;
+    const double rhoa =
+        (p.iexner == 1) ? func_p_base64(p, p.surf_p, p.tsfcc1, x[2]) / p.Rd / Tf : p.surf_rho;
+    const double rhop = (m_s + pi2 * 2.0 / 3.0 * cube(r) * p.rhow) / (pi2 * 2.0 / 3.0 * cube(r));
+    const double partmass = rhop * 2.0 / 3.0 * pi2 * cube(r);
+    const double taup_i = 18.0 * rhoa * p.nuf / rhop / ((2.0 * r) * (2.0 * r));
+    const double H0 = p.rhow / rhoa * pi2 * 2.0 * (r * r) * radrhs;
+    float *const *f = B.pay32.f;
+    f[P32_FX][t] = (float)((x[0] - g.dx * (double)(ipt - 1)) / g.dx);
+    f[P32_FY][t] = (float)((x[1] - g.dy * (double)(jpt - 1)) / g.dy);
+    f[P32_FZ][t] = (float)((x[2] - g.zz[kpt]) / g.dzu[kpt + 1]);
+    for (int a = 0; a < 3; ++a) f[P32_DV0 + a][t] = (float)(partmass / rhoa * (vrhs[a] - p.g[a]) + H0 * v[a]);
+    f[P32_T0][t] = (float)(Tprhs_s * 6.0 * p.rhow / rhop / p.CpaCpp / taup_i * (pi2 / 2.0) * r * p.nuf);
+    f[P32_H0][t] = (float)H0;
+    f[P32_E][t] = (float)(H0 * p.Cpv / p.Cpa * Tf - H0 * p.Cpv / p.Cpa * Tp);
+    f[P32_FAC][t] = (float)((double)mult / (g.dx * g.dy * g.dzu[kpt + 1]));
+}
+
+// Backward-Euler drag update of the velocity (particles.f90:3083-3100);
+// returns Rep of the old velocity.  MIXED evaluates it in FP32.
 template <bool MIXED>
-__device__ __forceinline__ void be_body(const DevBox &B, const DevParams &p, const StepIn &in, int t, int s,
-                                        const double xin[3], const Interp &I, int bad, Counts &cnt) {
-    const DevState &S = B.st[B.cur];
-    const DevState &O = B.st[1 - B.cur];
-    double x[3] = {xin[0], xin[1], xin[2]};
-    double v[3], vold[3];
-    for (int a = 0; a < 3; ++a) v[a] = S.v[a][s];
-    double Tp = S.Tp[s], radius = S.r[s];
-    const double m_s = S.m_s[s], kap = S.kap[s], rc = S.rc[s];
-    double res = S.res[s], actres = S.actres[s], numact = S.numact[s];
-    const long long multi = S.mult[s];
-    const int lid = S.lid[s];
-    const double mult = (double)multi;
-    const double dt = in.dt;
-    for (int a = 0; a < 3; ++a) vold[a] = v[a];
-    const double Tpold = Tp, rold = radius;
-
-    double Tf = I.Tf, qinf = I.qinf;
-    if (in.it <= 1) { v[0] = I.uf[0]; v[1] = I.uf[1]; v[2] = I.uf[2]; }
-    double rhoa;
-    if (p.iexner == 1) {
-        Tf = Tf * exner64(p, p.surf_p, func_p_base64(p, p.surf_p, p.tsfcc1, x[2]));
-        rhoa = func_p_base64(p, p.surf_p, p.tsfcc1, x[2]) / p.Rd / Tf;
-    } else {
-        rhoa = p.surf_rho;
-    }
-    if (qinf < 0.0) cnt.v[C_NEGQ]++;
-
-    double Volp = p.pi2 * 2.0 / 3.0 * cube(radius);
-    double rhop = (m_s + Volp * p.rhow) / Volp;
-    double Rep = 0.0;
-    const double xp3i = x[2];
-    for (int a = 0; a < 3; ++a) x[a] = x[a] + dt * v[a];
+__device__ __forceinline__ double be_drag(const DevParams &p, double radius, double m_s, double rhoa, double dt,
+                                          double v[3], const double uf[3]) {
+    const double Volp = p.pi2 * 2.0 / 3.0 * cube(radius);
+    const double rhop = (m_s + Volp * p.rhow) / Volp;
     if (MIXED) {
         const float rr = (float)radius;
         const float taup_if = 18.0f * (float)rhoa * (float)p.nuf / (float)rhop / ((2.0f * rr) * (2.0f * rr));
         const float dtf = (float)dt;
         const float den = 1.0f + dtf * taup_if;
-        float d0 = (float)(v[0] - I.uf[0]), d1 = (float)(v[1] - I.uf[1]), d2 = (float)(v[2] - I.uf[2]);
-        Rep = (double)(2.0f * rr * sqrtf(d0 * d0 + d1 * d1 + d2 * d2) / (float)p.nuf);
+        float d0 = (float)(v[0] - uf[0]), d1 = (float)(v[1] - uf[1]), d2 = (float)(v[2] - uf[2]);
+        const double Rep = (double)(2.0f * rr * sqrtf(d0 * d0 + d1 * d1 + d2 * d2) / (float)p.nuf);
         for (int a = 0; a < 3; ++a)
-            v[a] = (double)(((float)v[a] + taup_if * dtf * (float)I.uf[a] + dtf * (float)p.g[a]) / den);
+            v[a] = (double)(((float)v[a] + taup_if * dtf * (float)uf[a] + dtf * (float)p.g[a]) / den);
+        return Rep;
     } else {
-        double d0 = v[0] - I.uf[0], d1 = v[1] - I.uf[1], d2 = v[2] - I.uf[2];
+        double d0 = v[0] - uf[0], d1 = v[1] - uf[1], d2 = v[2] - uf[2];
         double diffnorm = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
         double taup_i = 18.0 * rhoa * p.nuf / rhop / ((2.0 * radius) * (2.0 * radius));
-        Rep = 2.0 * radius * diffnorm / p.nuf;
+        const double Rep = 2.0 * radius * diffnorm / p.nuf;
         const double corrfac = 1.0;
         for (int a = 0; a < 3; ++a)
-            v[a] = (v[a] + taup_i * dt * corrfac * I.uf[a] + dt * p.g[a]) / (1.0 + dt * corrfac * taup_i);
+            v[a] = (v[a] + taup_i * dt * corrfac * uf[a] + dt * p.g[a]) / (1.0 + dt * corrfac * taup_i);
+        return Rep;
     }
-    const double taup0 = taup0_64(p, m_s, rhoa);
-    const double dt_taup0 = dt / taup0;
+}
 
-    if (p.ievap == 1 && qinf > 0.0) {
+// Air density and temperature at the droplet (particles.f90:3064-3072).
+__device__ __forceinline__ double air_density(const DevParams &p, double x3, double &Tf) {
+    if (p.iexner == 1) {
+        Tf = Tf * exner64(p, p.surf_p, func_p_base64(p, p.surf_p, p.tsfcc1, x3));
+        return func_p_base64(p, p.surf_p, p.tsfcc1, x3) / p.Rd / Tf;
+    }
+    return p.surf_rho;
+}
+
+// ---------------------------------------------------------------------------
+// backward-Euler droplet body (particles.f90:3043-3242 + 3248-3260): all of
+// the per-droplet work after the interpolation, which an earlier kernel has
+// written to the output buffer at the droplet's slot t (uf, Tf before the
+// Exner factor, qinf; out-of-range flag in key[t]).  MIXED computes the drag
+// (taup_i and the implicit velocity update) in FP32; positions, the Newton
+// radius/temperature solve and everything else stay FP64.
+//
+// The Newton solve runs first with only its own inputs loaded; everything
+// else is (re)loaded and (re)computed after it with the same operations, so
+// little state is live across the solve's loop (registers, not results).
+//
+// With ALLOW_LM false, a droplet whose Gauss-Newton solve fails is appended
+// to the box's defer list and left untouched (no output, no counter, no
+// tally); a second pass re-runs it with ALLOW_LM true, where the rare
+// Levenberg-Marquardt fallback (up to 1000 iterations) does not hold back
+// the 31 other droplets of a warp.  Returns 1 if deferred.
+// ---------------------------------------------------------------------------
+template <bool MIXED, bool ALLOW_LM>
+__device__ __forceinline__ int be_body(const DevBox &B, const DevParams &p, const StepIn &in, int t, int s,
+                                       Counts &cnt) {
+    const DevState &S = B.st[B.cur];
+    const DevState &O = B.st[1 - B.cur];
+    const double dt = in.dt;
+
+    // ---- phase 1: the radius/temperature solve --------------------------
+    int solved = 0;                 // 1: rtz holds the solve's result
+    double rtz[2] = {1.0, 1.0};
+    int n100 = 0, nimpos = 0;
+    if (p.ievap == 1 && O.qinf[t] > 0.0) {
+        double Tf = O.Tf[t];
+        const double qinf = O.qinf[t];
+        const double rhoa = air_density(p, S.x[2][s], Tf);
+        const double radius = S.r[s], Tp = S.Tp[s], m_s = S.m_s[s], kap = S.kap[s];
+        double v[3], uf[3];
+        for (int a = 0; a < 3; ++a) {
+            uf[a] = O.uf[a][t];
+            v[a] = (in.it <= 1) ? uf[a] : S.v[a][s];
+        }
+        be_drag<MIXED>(p, radius, m_s, rhoa, dt, v, uf);
+        const double taup0 = taup0_64(p, m_s, rhoa);
         const double esa = mod_magnus64(Tf);
         int mflag;
         double guess = rad_solver2_64(p, Tf, qinf, rhoa, m_s, kap, radius, esa, mflag);
-        double rt_start[2], rtz[2];
+        double rt_start[2];
         if (mflag == 0) { rt_start[0] = guess / radius; rt_start[1] = Tf / Tp; }
         else { rt_start[0] = 1.0; rt_start[1] = 1.0; }
         Drop D;
         D.Tf = Tf; D.qinf = qinf; D.m_s = m_s; D.radius = radius; D.Tp = Tp; D.rhoa = rhoa;
-        D.h = dt_taup0;
+        D.h = dt / taup0;
         {
-            double e0 = I.uf[0] - v[0], e1 = I.uf[1] - v[1], e2 = I.uf[2] - v[2];
+            double e0 = uf[0] - v[0], e1 = uf[1] - v[1], e2 = uf[2] - v[2];
             D.diffnorm = sqrt(e0 * e0 + e1 * e1 + e2 * e2);
         }
         D.esa = esa;
@@ -428,25 +489,64 @@ __device__ __forceinline__ void be_body(const DevBox &B, const DevParams &p, con
         D.t0T = taup0 / Tp;
         int flag = gauss_newton64(p, D, rt_start, rtz);
         if (flag == 1) {
-            cnt.v[C_NUM100]++;
+            if (!ALLOW_LM) {
+                B.defer[atomicAdd(B.ndefer, 1)] = t;
+                return 1;
+            }
+            n100 = 1;
             flag = lv_solver64(p, D, rt_start, rtz);
         }
         if ((flag == 1) || ntlp_isnan(rtz[0]) || (rtz[0] * radius < 0) || ntlp_isnan(rtz[1]) ||
             (rtz[1] < 0) || (rtz[0] * radius > 1.0e-2)) {
-            cnt.v[C_NUMIMPOS]++;
+            nimpos = 1;
             rtz[0] = 1.0;
             rtz[1] = Tf / Tp;
         }
+        solved = 1;
+    }
+
+    // ---- phase 2: everything else ------------------------------------------
+    Counts dc;
+    for (int k = 0; k < kNumCounters; ++k) dc.v[k] = 0;
+    dc.v[C_NUM100] = n100;
+    dc.v[C_NUMIMPOS] = nimpos;
+    double x[3], v[3], vold[3], uf[3];
+    for (int a = 0; a < 3; ++a) {
+        x[a] = S.x[a][s];
+        v[a] = S.v[a][s];
+        uf[a] = O.uf[a][t];
+    }
+    double Tp = S.Tp[s], radius = S.r[s];
+    const double m_s = S.m_s[s], kap = S.kap[s], rc = S.rc[s];
+    double res = S.res[s], actres = S.actres[s], numact = S.numact[s];
+    const long long multi = S.mult[s];
+    const double mult = (double)multi;
+    const int bad = B.key[t];
+    for (int a = 0; a < 3; ++a) vold[a] = v[a];
+    const double Tpold = Tp, rold = radius;
+    double Tf = O.Tf[t];
+    const double qinf = O.qinf[t];
+    if (in.it <= 1) { v[0] = uf[0]; v[1] = uf[1]; v[2] = uf[2]; }
+    const double rhoa = air_density(p, x[2], Tf);
+    if (qinf < 0.0) dc.v[C_NEGQ]++;
+    const double xp3i = x[2];
+    for (int a = 0; a < 3; ++a) x[a] = x[a] + dt * v[a];
+    const double Rep = be_drag<MIXED>(p, radius, m_s, rhoa, dt, v, uf);
+
+    double Volp, rhop;
+    if (solved) {
         if (radius > rc && radius * rtz[0] < rc) {
-            cnt.v[C_DENUM]++;
+            dc.v[C_DENUM]++;
         } else if (radius < rc && radius * rtz[0] > rc) {
-            cnt.v[C_ACTNUM]++;
+            dc.v[C_ACTNUM]++;
             numact = numact + 1.0;
             actres = 0.0;
         }
         radius = rtz[0] * radius;
         Tp = rtz[1] * Tp;
     } else {
+        Volp = p.pi2 * 2.0 / 3.0 * cube(radius);
+        rhop = (m_s + Volp * p.rhow) / Volp;
         double taup_i = 18.0 * rhoa * p.nuf / rhop / ((2.0 * radius) * (2.0 * radius));
         double Nup = 2.0 + 0.6 * sqrt(Rep) * p.Pra13;
         double tmp_coeff = Nup / 3.0 / p.Pra * p.CpaCpp * rhop / p.rhow * taup_i;
@@ -494,25 +594,32 @@ __device__ __forceinline__ void be_body(const DevBox &B, const DevParams &p, con
     }
 
     const int alive = apply_bcs(B, p, x, v, radius);
-    if (bad) cnt.v[C_BAD]++;
+    if (bad) dc.v[C_BAD]++;
     for (int a = 0; a < 3; ++a) {
         O.x[a][t] = x[a];
         O.v[a][t] = v[a];
-        O.uf[a][t] = I.uf[a];
         O.vold[a][t] = vold[a];
     }
     O.Tp[t] = Tp; O.r[t] = radius; O.m_s[t] = m_s; O.kap[t] = kap; O.rc[t] = rc;
-    O.res[t] = res; O.actres[t] = actres; O.numact[t] = numact; O.mult[t] = multi; O.lid[t] = lid;
-    O.Tf[t] = Tf; O.qinf[t] = qinf; O.qstar[t] = qstar; O.Tpold[t] = Tpold; O.rold[t] = rold;
+    O.res[t] = res; O.actres[t] = actres; O.numact[t] = numact; O.mult[t] = multi; O.lid[t] = S.lid[s];
+    O.Tf[t] = Tf; O.qstar[t] = qstar; O.Tpold[t] = Tpold; O.rold[t] = rold;
     int key;
     if (!alive) {
         key = (int)B.g.ncells + 1;
-        cnt.v[C_DESTROY]++;
+        dc.v[C_DESTROY]++;
     } else {
-        key = cell_key(B.g, x[0], x[1], x[2]);
-        if (in.write_payload) write_payload(B, p, t, x, v, vold, radius, rold, Tp, Tpold, Tf, m_s, multi, dt);
+        int ipt, jpt, kpt;
+        key = cell_key(B.g, x[0], x[1], x[2], &ipt, &jpt, &kpt);
+        if (in.write_payload && key < (int)B.g.ncells) {
+            if (MIXED)
+                write_payload_mixed(B, p, t, ipt, jpt, kpt, x, v, vold, radius, rold, Tp, Tpold, Tf, m_s, multi, dt);
+            else
+                write_payload(B, p, t, x, v, vold, radius, rold, Tp, Tpold, Tf, m_s, multi, dt);
+        }
     }
     B.key[t] = key;
+    for (int k = 0; k < kNumCounters; ++k) cnt.v[k] += dc.v[k];
+    return 0;
 }
 
 }  // namespace

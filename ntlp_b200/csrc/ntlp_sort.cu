@@ -200,7 +200,10 @@ __global__ void k_reset_step(DevBox *boxes, int nbox) {
     for (int i = threadIdx.x; i < kNumCounters; i += blockDim.x) B.counters[i] = 0;
     for (int i = threadIdx.x; i < nz1; i += blockDim.x) B.pflux[i] = 0.0;
     for (int i = threadIdx.x; i < 2 * nz1 * kFluxLimbs; i += blockDim.x) B.flux_fx[i] = 0;
-    if (threadIdx.x == 0) *B.err = 0;
+    if (threadIdx.x == 0) {
+        *B.err = 0;
+        *B.ndefer = 0;
+    }
 }
 
 void launch_reset_step(DevBox *boxes, int nbox, cudaStream_t st) {
@@ -225,14 +228,12 @@ void launch_keys_initial(DevBox *boxes, const Tile *tiles, int ntiles, cudaStrea
 // ---- halo fill: flow layout u(1:nnx,1:nny,0:nnz+1) -> ext(0:nnz+1,-1:nny+3,-1:nnx+3)
 // 32x32 tiles of the (i, k) plane per output row j, staged through shared
 // memory so both the x-fastest read and the z-fastest write are coalesced.
-__global__ void k_fill_ext(const double *__restrict__ flow, double *__restrict__ ext, float *__restrict__ ext32,
-                           DevGrid g) {
+__global__ void k_fill_ext(const double *__restrict__ flow, double *__restrict__ ext, DevGrid g) {
     __shared__ double tile[32][33];
     const int j = (int)blockIdx.z - 1;                 // -1 .. nny+3
     const int i0 = (int)blockIdx.x * 32 - 1;           // ext i of tile start
     const int k0 = (int)blockIdx.y * 32;
     const int jsrc = ((j - 1) % g.nny + g.nny) % g.nny;  // 0-based source row
-    const double ref = flow[(long long)g.nnx * g.nny];     // flow(1,1,1) = ext(1,1,1)
     // load: threads along i (x fastest in flow)
     for (int r = threadIdx.y; r < 32; r += blockDim.y) {
         int k = k0 + r;
@@ -249,30 +250,40 @@ __global__ void k_fill_ext(const double *__restrict__ flow, double *__restrict__
         int k = k0 + (int)threadIdx.x;
         if (k <= g.nnz + 1 && i <= g.nnx + 3) {
             long long o = (long long)k + (long long)g.nz2 * ((long long)(j + 1) + (long long)g.ny5 * (i + 1));
-            double val = tile[threadIdx.x][r];
-            ext[o] = val;
-            if (ext32) ext32[o] = (float)(val - ref);
+            ext[o] = tile[threadIdx.x][r];
         }
     }
 }
 
-void launch_fill_ext(const double *flow, double *ext, float *ext32, const DevGrid &g, cudaStream_t st) {
+void launch_fill_ext(const double *flow, double *ext, const DevGrid &g, cudaStream_t st) {
     dim3 grid((g.nnx + 5 + 31) / 32, (g.nnz + 2 + 31) / 32, g.nny + 5);
     dim3 block(32, 8);
-    k_fill_ext<<<grid, block, 0, st>>>(flow, ext, ext32, g);
+    k_fill_ext<<<grid, block, 0, st>>>(flow, ext, g);
 }
 
-__global__ void k_to_f32(const double *__restrict__ s, float *__restrict__ d, long long n, long long ridx) {
-    const double ref = s[ridx];
+// FP32 copies for the mixed path: (u, v, T, q) packed per point as float4,
+// w separately, each as the deviation from its value at point (1,1,1).
+__global__ void k_pack_f32(const double *__restrict__ u, const double *__restrict__ v,
+                           const double *__restrict__ w, const double *__restrict__ T,
+                           const double *__restrict__ q, float4 *__restrict__ f4, float *__restrict__ fw,
+                           long long n, long long ridx) {
+    const double ru = u[ridx], rv = v[ridx], rw = w[ridx], rT = T[ridx], rq = q[ridx];
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    long long stride = (long long)gridDim.x * blockDim.x;
-    for (; i < n; i += stride) d[i] = (float)(s[i] - ref);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (; i < n; i += stride) {
+        f4[i] = make_float4((float)(u[i] - ru), (float)(v[i] - rv), (float)(T[i] - rT), (float)(q[i] - rq));
+        fw[i] = (float)(w[i] - rw);
+    }
 }
 
-void launch_to_f32(const double *src, float *dst, long long n, long long ridx, cudaStream_t st) {
+void launch_pack_f32(const DevBox *hb, float4 *f4, float *fw, cudaStream_t st) {
+    const DevGrid &g = hb->g;
+    const long long n = (long long)g.nz2 * g.ny5 * g.nx5;
     int blocks = (int)((n + 255) / 256);
     if (blocks > 148 * 16) blocks = 148 * 16;
-    if (blocks > 0) k_to_f32<<<blocks, 256, 0, st>>>(src, dst, n, ridx);
+    if (blocks > 0)
+        k_pack_f32<<<blocks, 256, 0, st>>>(hb->f[0], hb->f[1], hb->f[2], hb->f[3], hb->f[4], f4, fw, n,
+                                            f32_ref_index(g));
 }
 
 // ---- download: list-order position of every survivor -----------------------
