@@ -44,6 +44,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 B_D = {"fp64": 248, "mixed": 224}       # algorithmic bytes per droplet
+# DRAM bytes per droplet of the update phase (interpolation + droplet body)
+# measured by ncu at 1M droplets / 128^3 (fields subtracted), used to scale
+# the measured traffic to the bench workload; see
+# profiles/k_update_mixed_1M_droplets_128cube.md
+NCU_BYTES_PER_DROPLET = {"mixed": 400.0}
 METRIC = "droplet-updates/s (mixed precision, 16M droplets, 6th-order BE step + coupling)"
 
 
@@ -367,9 +372,13 @@ def main():
                    "l2": "state (~3.5 GB) >> L2; no flush needed", "parallelism": f"{ws} replica(s)"},
         "phases_ms_per_step": {k: v / args.steps for k, v in r["prof"].items() if k.endswith("_ms")},
         "gpu_launches": int(r["prof"]["launches"]),
-        "roofline": {"bound": "hbm", "kernel": "k_update_be_" + ("mixed" if head == "mixed" else "64"),
+        "roofline": {"bound": "hbm",
+                     "kernel": ("update phase: k_interp_mixed + k_be_mixed + k_be_defer_mixed" if head == "mixed"
+                                else "update phase: k_interp64 + k_be64 + k_be_defer64"),
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "peak_source": src, "traffic": None,
+                     "peak_source": src,
+                     "traffic": (NCU_BYTES_PER_DROPLET[head] * n + npad * 5 * sf) if head in NCU_BYTES_PER_DROPLET else None,
+                     "traffic_source": "ncu DRAM bytes at 1M droplets/128^3, scaled per droplet (+ fields)",
                      "alg_bytes_per_launch": alg_update,
                      "step_frac": (step_alg / (r["ms"] / args.steps * 1e-3) / 1e9) / hbm},
         "clocks": r["clocks"],
