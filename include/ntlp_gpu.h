@@ -9,12 +9,15 @@
  * plus the single-domain meaning of fill_ext (particles.f90:91-328) and
  * particle_coupling_exchange (particles.f90:1066-1149).  The entry points
  * below replace those bodies; the Fortran host keeps its time loop and
- * passes its arrays by address (ISO_C_BINDING shim: INTEGRATION.md).
+ * passes its arrays by address through an ISO_C_BINDING interface module.
  *
  * Conventions
  *   - Every function returns 0 (NTLP_OK) or a negative NTLP_ERR_* code; on
  *     error ntlp_last_error(ctx) describes it.  Nothing calls exit/abort.
  *   - The caller owns every host array; the library owns device memory.
+ *     Array arguments of the upload, download and source calls may also
+ *     be device pointers (the copies use unified addressing); device data
+ *     written on another stream must be complete before the call.
  *   - Arrays are contiguous, column-major (Fortran order), FP64 unless
  *     stated.  Grid index ranges are the reference's.
  *   - A context is used by one host thread at a time; many contexts may
@@ -160,6 +163,11 @@ int ntlp_sync(ntlp_ctx *ctx);
 /* The context's CUDA stream (a cudaStream_t), for callers that order their
  * own work or events after the step.                                      */
 void *ntlp_stream(ntlp_ctx *ctx);
+/* Issue the context's work on the caller's stream (a cudaStream_t, e.g. one
+ * created with a scheduling priority) from now on; NULL returns to the
+ * context's own stream.  Waits for the current stream first.  The caller
+ * keeps the stream alive until the context is destroyed or switched back. */
+int ntlp_use_stream(ntlp_ctx *ctx, void *stream);
 
 /* ---- instrumentation (phase timers; measurement.f90's named phases) ----- */
 /* When enabled, every step records CUDA events around its kernels on the
@@ -168,6 +176,47 @@ void *ntlp_stream(ntlp_ctx *ctx);
  * launches since the last reset, then resets them.                        */
 int ntlp_profile_enable(ntlp_ctx *ctx, int enable);
 int ntlp_profile_read(ntlp_ctx *ctx, double ms[4], int64_t *launches);
+
+/* ---- many boxes in one context ------------------------------------------
+ * No counterpart in the reference (one process steps one domain).  A batch
+ * context holds nbox independent periodic boxes, each with its own grid,
+ * fields and droplets, sharing the flags and constants; every kernel of a
+ * step covers all boxes at once.  The single-box calls above act on box 0,
+ * except ntlp_step_be / ntlp_step_rk3 / ntlp_coupling, which advance every
+ * box (their counters are summed over boxes).                              */
+int ntlp_batch_create(int32_t nbox, const ntlp_grid *grids, const ntlp_params *params,
+                      const int64_t *capacities, ntlp_ctx **out);
+int32_t ntlp_nbox(const ntlp_ctx *ctx);
+/* Device bytes that ntlp_batch_create (nbox = 1: ntlp_ctx_create) would
+ * take for these grids, precision and capacities, without a device or an
+ * allocation; -1 for invalid arguments.  For admission by memory budget. */
+int64_t ntlp_bytes_required(int32_t nbox, const ntlp_grid *grids, const ntlp_params *params,
+                            const int64_t *capacities);
+int ntlp_box_fields_upload_ext(ntlp_ctx *ctx, int32_t box, const double *uext, const double *vext,
+                               const double *wext, const double *Text, const double *T2ext);
+int ntlp_box_fields_upload(ntlp_ctx *ctx, int32_t box, const double *u, const double *v,
+                           const double *w, const double *t, const double *q);
+int ntlp_box_droplets_upload(ntlp_ctx *ctx, int32_t box, const ntlp_droplets *d);
+int ntlp_box_droplets_download(ntlp_ctx *ctx, int32_t box, ntlp_droplets *d);
+int64_t ntlp_box_numpart(ntlp_ctx *ctx, int32_t box);
+/* counters of the last step of one box */
+int ntlp_box_counters(ntlp_ctx *ctx, int32_t box, ntlp_counters *c);
+/* sources of one box from the last deposition (ntlp_coupling or the graph) */
+int ntlp_box_sources(ntlp_ctx *ctx, int32_t box, int32_t layout, double *partsrc,
+                     double *partTsrc, double *partHsrc, double *partTEsrc);
+/* nsteps backward-Euler steps, each followed by the deposition, for every
+ * box, recorded once as a CUDA graph and replayed as one graph launch.
+ * it is the step counter of the first of them and must be >= 2 (the it <= 1
+ * rule vp = uf belongs to an eagerly run first step).  Returns when queued. */
+int ntlp_advance_graph(ntlp_ctx *ctx, double dt, int32_t it, int32_t nsteps);
+/* Autotuner: times each deposition tile shape (NTLP_TUNE_VARIANTS of them:
+ * 2x4x32, 4x4x16, 2x2x64 nodes) and each droplet block size (128, 256) on
+ * this context's boxes over `steps` steps (state advances), keeps the
+ * fastest, and reports the per-variant milliseconds per step (ms[i] for
+ * deposition shape i, ms[3+j] for block size j).                          */
+#define NTLP_TUNE_VARIANTS 5
+int ntlp_autotune(ntlp_ctx *ctx, double dt, int32_t it, int32_t steps, int32_t choice[2],
+                  double ms[NTLP_TUNE_VARIANTS]);
 
 /* ---- droplet creation helper ------------------------------------------- */
 /* Koehler critical radius rc of n droplets (crit_radius with the radval

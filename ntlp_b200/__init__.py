@@ -61,8 +61,25 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.ntlp_crit_radius.argtypes = [P(abi.NtlpParams), C.c_int64, dp, dp, dp, dp]
     L.ntlp_stream.argtypes = [C.c_void_p]
     L.ntlp_stream.restype = C.c_void_p
+    L.ntlp_use_stream.argtypes = [C.c_void_p, C.c_void_p]
     L.ntlp_profile_enable.argtypes = [C.c_void_p, C.c_int]
     L.ntlp_profile_read.argtypes = [C.c_void_p, dp, P(C.c_int64)]
+    # many boxes in one context
+    L.ntlp_batch_create.argtypes = [C.c_int32, P(abi.NtlpGrid), P(abi.NtlpParams), P(C.c_int64), P(C.c_void_p)]
+    L.ntlp_nbox.argtypes = [C.c_void_p]
+    L.ntlp_nbox.restype = C.c_int32
+    L.ntlp_bytes_required.argtypes = [C.c_int32, P(abi.NtlpGrid), P(abi.NtlpParams), P(C.c_int64)]
+    L.ntlp_bytes_required.restype = C.c_int64
+    L.ntlp_box_fields_upload_ext.argtypes = [C.c_void_p, C.c_int32] + [dp] * 5
+    L.ntlp_box_fields_upload.argtypes = [C.c_void_p, C.c_int32] + [dp] * 5
+    L.ntlp_box_droplets_upload.argtypes = [C.c_void_p, C.c_int32, P(abi.NtlpDroplets)]
+    L.ntlp_box_droplets_download.argtypes = [C.c_void_p, C.c_int32, P(abi.NtlpDroplets)]
+    L.ntlp_box_numpart.argtypes = [C.c_void_p, C.c_int32]
+    L.ntlp_box_numpart.restype = C.c_int64
+    L.ntlp_box_counters.argtypes = [C.c_void_p, C.c_int32, P(abi.NtlpCounters)]
+    L.ntlp_box_sources.argtypes = [C.c_void_p, C.c_int32, C.c_int32, dp, dp, dp, dp]
+    L.ntlp_advance_graph.argtypes = [C.c_void_p, C.c_double, C.c_int32, C.c_int32]
+    L.ntlp_autotune.argtypes = [C.c_void_p, C.c_double, C.c_int32, C.c_int32, P(C.c_int32), dp]
     _lib = L
     return L
 
@@ -80,6 +97,32 @@ def crit_radius(params: dict, m_s, kappa_s, T) -> np.ndarray:
     return out
 
 
+def _field(a):
+    """A field argument: a contiguous float64 device tensor is passed as is
+    (its pointer goes to the library), anything else becomes a contiguous
+    float64 numpy array."""
+    if hasattr(a, "data_ptr"):
+        return a
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def bytes_required(grids: list, params: dict, capacities: list) -> int:
+    """Device bytes a context of these boxes would take (no allocation)."""
+    L = load_library()
+    structs, keep = [], []
+    for g in grids:
+        gs, k = abi.make_grid_struct(g)
+        structs.append(gs)
+        keep.append(k)
+    arr = (abi.NtlpGrid * len(grids))(*structs)
+    p = abi.make_params_struct(params)
+    caps = (C.c_int64 * len(grids))(*[int(c) for c in capacities])
+    n = int(L.ntlp_bytes_required(len(grids), arr, C.byref(p), caps))
+    if n < 0:
+        raise NtlpError("ntlp_bytes_required: invalid arguments")
+    return n
+
+
 class DropletStep:
     """One box (periodic domain) with its fields and droplets resident on
     the current CUDA device."""
@@ -87,6 +130,7 @@ class DropletStep:
     def __init__(self, grid: dict, params: dict, capacity: int):
         self.L = load_library()
         self.grid = grid
+        self.grids = [grid]
         self.params = dict(params)
         self._g, self._gkeep = abi.make_grid_struct(grid)
         self._p = abi.make_params_struct(params)
@@ -131,6 +175,10 @@ class DropletStep:
         """cudaStream_t of the context (for events on the launching stream)."""
         return int(self.L.ntlp_stream(self.h) or 0)
 
+    def use_stream(self, stream_handle: int | None):
+        """Issue this context's work on an external cudaStream_t (None: its own)."""
+        self._check(self.L.ntlp_use_stream(self.h, C.c_void_p(stream_handle or None)), "ntlp_use_stream")
+
     def profile(self, enable: bool = True):
         self._check(self.L.ntlp_profile_enable(self.h, 1 if enable else 0), "ntlp_profile_enable")
 
@@ -142,7 +190,7 @@ class DropletStep:
 
     # -- fields (fill_ext) --
     def set_fields_ext(self, ext: dict):
-        arrs = [np.ascontiguousarray(ext[k], dtype=np.float64) for k in ("u", "v", "w", "T", "q")]
+        arrs = [_field(ext[k]) for k in ("u", "v", "w", "T", "q")]
         self._ext_keep = arrs
         self._check(self.L.ntlp_fields_upload_ext(self.h, *(abi.as_dptr(a) for a in arrs)),
                     "ntlp_fields_upload_ext")
@@ -150,7 +198,7 @@ class DropletStep:
 
     def fill_ext(self, flow: dict):
         """Flow-layout fields u(1:nnx,1:nny,0:nnz+1) -> device halo fill."""
-        arrs = [np.ascontiguousarray(flow[k], dtype=np.float64) for k in ("u", "v", "w", "T", "q")]
+        arrs = [_field(flow[k]) for k in ("u", "v", "w", "T", "q")]
         self._flow_keep = arrs
         self._check(self.L.ntlp_fields_upload(self.h, *(abi.as_dptr(a) for a in arrs)), "ntlp_fields_upload")
         self.sync()
@@ -212,3 +260,100 @@ class DropletStep:
         out = [np.zeros(nz1) for _ in range(3)]
         self._check(self.L.ntlp_flux(self.h, *(abi.as_dptr(a) for a in out)), "ntlp_flux")
         return out
+
+
+class DropletBatch(DropletStep):
+    """Many independent boxes (each its own grid, fields and droplets; shared
+    flags and constants) in one context: every kernel of a step covers all
+    boxes, and multi-step advances replay as one CUDA graph.  The reference
+    steps one domain per process; this has no counterpart there."""
+
+    def __init__(self, grids: list, params: dict, capacities: list):
+        if len(grids) != len(capacities) or not grids:
+            raise ValueError("need one capacity per grid")
+        self.L = load_library()
+        self.grid = grids[0]
+        self.grids = list(grids)
+        self.params = dict(params)
+        nbox = len(grids)
+        structs, self._gkeep = [], []
+        for g in grids:
+            gs, keep = abi.make_grid_struct(g)
+            structs.append(gs)
+            self._gkeep.append(keep)
+        self._g = (abi.NtlpGrid * nbox)(*structs)
+        self._p = abi.make_params_struct(params)
+        caps = (C.c_int64 * nbox)(*[int(c) for c in capacities])
+        h = C.c_void_p()
+        rc = self.L.ntlp_batch_create(nbox, self._g, C.byref(self._p), caps, C.byref(h))
+        if rc != 0 or not h.value:
+            raise NtlpError(f"ntlp_batch_create failed ({rc})")
+        self.h = h
+        self.capacities = [int(c) for c in capacities]
+        self.capacity = max(self.capacities)
+        self.last_counters = {}
+        self._keep = {}
+
+    @property
+    def nbox(self) -> int:
+        return int(self.L.ntlp_nbox(self.h))
+
+    def box_numpart(self, b: int) -> int:
+        return int(self.L.ntlp_box_numpart(self.h, int(b)))
+
+    def set_box_fields_ext(self, b: int, ext: dict, sync: bool = True):
+        arrs = [_field(ext[k]) for k in ("u", "v", "w", "T", "q")]
+        self._keep[("ext", b)] = arrs
+        self._check(self.L.ntlp_box_fields_upload_ext(self.h, int(b), *(abi.as_dptr(a) for a in arrs)),
+                    "ntlp_box_fields_upload_ext")
+        if sync:
+            self.sync()
+
+    def box_fill_ext(self, b: int, flow: dict, sync: bool = True):
+        arrs = [_field(flow[k]) for k in ("u", "v", "w", "T", "q")]
+        self._keep[("flow", b)] = arrs
+        self._check(self.L.ntlp_box_fields_upload(self.h, int(b), *(abi.as_dptr(a) for a in arrs)),
+                    "ntlp_box_fields_upload")
+        if sync:
+            self.sync()
+
+    def set_box_droplets(self, b: int, d: dict):
+        s = abi.make_droplets_struct(d)
+        self._check(self.L.ntlp_box_droplets_upload(self.h, int(b), C.byref(s)), "ntlp_box_droplets_upload")
+
+    def get_box_droplets(self, b: int) -> dict:
+        n = self.box_numpart(b)
+        d = abi.empty_droplets(max(n, 1))
+        s = abi.make_droplets_struct(d, n=n)
+        self._check(self.L.ntlp_box_droplets_download(self.h, int(b), C.byref(s)), "ntlp_box_droplets_download")
+        n = int(s.n)
+        return {k: np.ascontiguousarray(v[..., :n] if v.ndim == 2 else v[:n]) for k, v in d.items()}
+
+    def box_counters(self, b: int) -> dict:
+        c = abi.NtlpCounters()
+        self._check(self.L.ntlp_box_counters(self.h, int(b), C.byref(c)), "ntlp_box_counters")
+        return c.as_dict()
+
+    def box_sources(self, b: int, layout: int = abi.NTLP_LAYOUT_COLUMN) -> list:
+        g = self.grids[b]
+        nx, ny, nz2 = g["nnx"], g["nny"], g["nnz"] + 2
+        shape = (nx, ny, nz2) if layout == abi.NTLP_LAYOUT_COLUMN else (nz2, ny, nx)
+        mom = np.empty((3,) + shape)
+        rest = [np.empty(shape) for _ in range(3)]
+        self._check(self.L.ntlp_box_sources(self.h, int(b), int(layout), abi.as_dptr(mom.reshape(-1)),
+                                            *(abi.as_dptr(a.reshape(-1)) for a in rest)), "ntlp_box_sources")
+        return [mom[0], mom[1], mom[2], rest[0], rest[1], rest[2]]
+
+    def advance_graph(self, dt: float, it: int, nsteps: int):
+        """nsteps of particle_update_BE + particle_coupling_update for every
+        box, replayed as one CUDA graph launch (queued, not waited for)."""
+        self._check(self.L.ntlp_advance_graph(self.h, float(dt), int(it), int(nsteps)), "ntlp_advance_graph")
+
+    def autotune(self, dt: float, it: int, steps: int = 2) -> dict:
+        """Time the deposition tile shapes and droplet block sizes on these
+        boxes (the state advances by 5 * (steps + 1) steps) and keep the
+        fastest."""
+        choice = (C.c_int32 * 2)()
+        ms = (C.c_double * 5)()
+        self._check(self.L.ntlp_autotune(self.h, float(dt), int(it), int(steps), choice, ms), "ntlp_autotune")
+        return dict(deposit_variant=int(choice[0]), block_variant=int(choice[1]), ms=list(ms))

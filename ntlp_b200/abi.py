@@ -84,9 +84,18 @@ SCALAR_FIELDS = ("Tp", "Tprhs_s", "Tprhs_L", "Tf", "radius", "radrhs", "qinf", "
                  "res", "m_s", "kappa_s", "rc", "actres", "numact", "Tp_old", "radius_old")
 
 
-def as_dptr(a: np.ndarray | None):
+def _device_ptr(a, dtype_name: str, ctype):
+    """Pointer of a contiguous device tensor (anything with data_ptr())."""
+    assert str(a.dtype).endswith(dtype_name) and a.is_contiguous(), f"contiguous {dtype_name} tensor expected"
+    return C.cast(C.c_void_p(a.data_ptr()), C.POINTER(ctype))
+
+
+def as_dptr(a):
+    """double* of a float64 numpy array or of a float64 device tensor."""
     if a is None:
         return None
+    if hasattr(a, "data_ptr"):
+        return _device_ptr(a, "float64", C.c_double)
     assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"], "float64 contiguous array expected"
     return a.ctypes.data_as(_dp)
 
@@ -130,11 +139,17 @@ def make_droplets_struct(d: dict, n: int | None = None) -> NtlpDroplets:
         if f in d and d[f] is not None:
             setattr(s, f, as_dptr(d[f]))
     if d.get("mult") is not None:
-        assert d["mult"].dtype == np.int64
-        s.mult = d["mult"].ctypes.data_as(C.POINTER(C.c_int64))
+        if hasattr(d["mult"], "data_ptr"):
+            s.mult = _device_ptr(d["mult"], "int64", C.c_int64)
+        else:
+            assert d["mult"].dtype == np.int64
+            s.mult = d["mult"].ctypes.data_as(C.POINTER(C.c_int64))
     if d.get("lid") is not None:
-        assert d["lid"].dtype == np.int32
-        s.lid = d["lid"].ctypes.data_as(C.POINTER(C.c_int32))
+        if hasattr(d["lid"], "data_ptr"):
+            s.lid = _device_ptr(d["lid"], "int32", C.c_int32)
+        else:
+            assert d["lid"].dtype == np.int32
+            s.lid = d["lid"].ctypes.data_as(C.POINTER(C.c_int32))
     return s
 
 

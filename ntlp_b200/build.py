@@ -32,7 +32,7 @@ UNITS = {
     "ntlp_api.cu": [],
     "ntlp_noalloc.cu": [],
 }
-HEADERS = ["ntlp_math.h", "ntlp_dev.cuh", "ntlp_kernels.h", "ntlp_physics.cuh"]
+HEADERS = ["ntlp_math.h", "ntlp_dev.cuh", "ntlp_kernels.h", "ntlp_physics.cuh", "ntlp_deposit.cuh"]
 
 
 def nvcc() -> str:

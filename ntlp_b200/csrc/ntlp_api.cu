@@ -1,20 +1,27 @@
-// ntlp_api.cu -- the C ABI (include/ntlp_gpu.h): contexts, device memory,
-// upload/download and the sequencing of one droplet step.
+// ntlp_api.cu -- the C ABI (include/ntlp_gpu.h): contexts of one or many
+// boxes, device memory, upload/download and the sequencing of a step.
 //
-// One step of particle_update_BE (particles.f90:3000-3280) is four launches
-// on the context's stream:
+// One step of particle_update_BE (particles.f90:3000-3280) is a fixed
+// sequence of launches on the context's stream, each covering every box:
 //   reset      counters and flux tallies to zero
-//   update     interpolation, BE advance, Newton solve, flux tallies,
-//              boundaries, new cell key, deposition payload (one thread per
-//              droplet, reading the state through the cell-sorted permutation)
+//   update     interpolation; droplet body (BE advance, Gauss-Newton, flux
+//              tallies, boundaries, new cell key, deposition payload);
+//              deferred Levenberg-Marquardt droplets
 //   sort       histogram + scan + scatter + per-cell lid order
 //   finish     adopt the new buffer and order, count survivors
-// particle_coupling_update is one more launch (deposition) that reads the
-// payload through the cell lists.
+// particle_coupling_update adds the deposition.  Because every per-step
+// decision (buffer parity, droplet counts) lives in device memory, the same
+// sequence can be recorded once as a CUDA graph and replayed.
+//
+// Memory: each box's arrays are carved out of one allocation taken from the
+// device's stream-ordered memory pool (cudaMallocAsync), which keeps freed
+// blocks for reuse, so creating and destroying contexts (the serving loop
+// does so per job) does not go back to the driver each time.
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <cstdarg>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -27,34 +34,58 @@
 
 using namespace ntlp;
 
-struct ntlp_ctx {
-    int device = 0;
-    cudaStream_t stream = nullptr;
+namespace {
+
+struct BoxHost {
     ntlp_grid grid{};
     std::vector<double> z, zz, dzw, dzu;
+    int64_t cap = 0;
+    int n_uploaded = 0;
+    bool have_fields = false, have_droplets = false;
+    void *arena = nullptr, *arena_rk3 = nullptr;
+    size_t arena_bytes = 0;
+    double *staging = nullptr;      // flow-field / source transposes, upload tile tables
+    int *rank = nullptr;            // download: list-order position by lid
+};
+
+enum Phase { PH_UPDATE = 0, PH_SORT = 1, PH_DEPOSIT = 2, PH_OTHER = 3 };
+
+}  // namespace
+
+struct ntlp_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;       // where all work of the context goes
+    cudaStream_t own_stream = nullptr;   // the stream the context created
+    int nbox = 0;
     ntlp_params params{};
     DevParams dp{};
     DevParams *dp_d = nullptr;
-    DevBox box{};
+    std::vector<BoxHost> bh;
+    std::vector<DevBox> box;        // host mirror of the device descriptors
     DevBox *box_d = nullptr;
-    std::vector<void *> allocs;
-    int64_t cap = 0;
-    int n_uploaded = 0;
-    bool have_fields = false, have_droplets = false, have_rk3 = false;
+    bool have_rk3 = false;
     bool payload_valid = false;
     double last_dt = 0.0;
-    int last_kind = 0;            // 1 = BE, 2 = RK3 stage 3
-    std::vector<Tile> drop_tiles, cell_tiles, node_tiles;
-    Tile *drop_tiles_d = nullptr, *cell_tiles_d = nullptr, *node_tiles_d = nullptr;
+    // launch tiles
+    Tile *drop_tiles_d[kNtVariants] = {};
+    int n_drop_tiles[kNtVariants] = {};
+    Tile *cell_tiles_d = nullptr;
+    int n_cell_tiles = 0;
+    Tile *dep_tiles_d[kDepVariants] = {};
+    int n_dep_tiles[kDepVariants] = {};
     long long *tile_sums_d = nullptr;
     int *box_first_tile_d = nullptr;
+    void *small_arena = nullptr;
     SortPlan plan{};
-    long long *counters_h = nullptr;   // pinned
-    double *staging_d = nullptr;       // max(cap, nnodes, flow field) doubles
-    int *rank_d = nullptr;
+    int dep_variant = 0, nt_variant = 0;
+    long long *counters_h = nullptr;   // pinned [nbox][kNumCounters]
+    // CUDA graph of nsteps (update + sort + finish + deposit)
+    cudaGraphExec_t gexec = nullptr;
+    double g_dt = 0.0;
+    int g_nsteps = 0, g_dep = -1, g_nt = -1;
     int64_t bytes = 0;
     std::string err;
-    // instrumentation: CUDA events around each phase on the context's stream
+    // instrumentation
     bool prof = false;
     struct PhaseRec {
         int phase;
@@ -85,60 +116,153 @@ int fail(ntlp_ctx *c, int code, const char *fmt, ...) {
                         __LINE__);                                                                 \
     } while (0)
 
-template <class T>
-int dalloc(ntlp_ctx *c, T **p, size_t count) {
+// Two-pass carving of one allocation: the first pass (base == nullptr) only
+// sums sizes, the second hands out 256-byte aligned pointers.
+struct Carver {
+    unsigned char *base = nullptr;
+    size_t off = 0;
+    template <class T>
+    void take(T **p, size_t count) {
+        const size_t bytes = ((count ? count : 1) * sizeof(T) + 255) / 256 * 256;
+        *p = base ? (T *)(base + off) : nullptr;
+        off += bytes;
+    }
+};
+
+void carve_state(Carver &cv, DevState &s, size_t n) {
+    for (int a = 0; a < 3; ++a) {
+        cv.take(&s.x[a], n); cv.take(&s.v[a], n); cv.take(&s.uf[a], n); cv.take(&s.vold[a], n);
+    }
+    cv.take(&s.Tp, n); cv.take(&s.r, n); cv.take(&s.m_s, n); cv.take(&s.kap, n); cv.take(&s.rc, n);
+    cv.take(&s.res, n); cv.take(&s.actres, n); cv.take(&s.numact, n); cv.take(&s.mult, n); cv.take(&s.lid, n);
+    cv.take(&s.Tf, n); cv.take(&s.qinf, n); cv.take(&s.qstar, n); cv.take(&s.Tpold, n); cv.take(&s.rold, n);
+}
+
+void carve_rk3(Carver &cv, DevState &s, size_t n) {
+    for (int a = 0; a < 3; ++a) { cv.take(&s.xrhs[a], n); cv.take(&s.vrhs[a], n); }
+    cv.take(&s.Tprhs_s, n); cv.take(&s.Tprhs_L, n); cv.take(&s.radrhs, n);
+}
+
+// everything one box owns
+void carve_box(Carver &cv, BoxHost &h, DevBox &B, bool mixed) {
+    const DevGrid &g = B.g;
+    const size_t npad = (size_t)g.nz2 * g.ny5 * g.nx5;
+    const size_t n = (size_t)h.cap;
+    double *zg;
+    cv.take(&zg, 2 * (size_t)g.nz2 + 2 * ((size_t)g.nnz + 3));
+    if (cv.base) {
+        B.g.z = zg; B.g.zz = zg + g.nz2; B.g.dzw = zg + 2 * g.nz2; B.g.dzu = zg + 2 * g.nz2 + (g.nnz + 3);
+    }
+    for (int k = 0; k < 5; ++k) {
+        double *f;
+        cv.take(&f, npad);
+        B.f[k] = f;
+    }
+    if (mixed) {
+        float4 *f4;
+        float *fw;
+        cv.take(&f4, npad);
+        cv.take(&fw, npad);
+        B.f4 = f4;
+        B.fw = fw;
+    }
+    carve_state(cv, B.st[0], n);
+    carve_state(cv, B.st[1], n);
+    if (mixed) {
+        for (int q = 0; q < P32_N; ++q) cv.take(&B.pay32.f[q], n);
+    } else {
+        for (int a = 0; a < 3; ++a) { cv.take(&B.pay.D[a], n); cv.take(&B.pay.V[a], n); }
+        cv.take(&B.pay.T0, n); cv.take(&B.pay.H0, n); cv.take(&B.pay.E1, n); cv.take(&B.pay.E2, n);
+        cv.take(&B.pay.mult, n);
+    }
+    cv.take(&B.n_alive, 1);
+    cv.take(&B.perm, n);
+    cv.take(&B.key, n);
+    cv.take(&B.sorted, n);
+    cv.take(&B.cell_cnt, (size_t)g.ncells + 2);
+    cv.take(&B.cell_start, (size_t)g.ncells + 3);
+    cv.take(&B.counters, kNumCounters);
+    cv.take(&B.pflux, (size_t)g.nnz + 1);
+    cv.take(&B.flux_fx, (size_t)2 * (g.nnz + 1) * kFluxLimbs);
+    for (int q = 0; q < 6; ++q) cv.take(&B.src[q], (size_t)g.nnodes);
+    cv.take(&B.err, 1);
+    cv.take(&B.defer, n);
+    cv.take(&B.ndefer, 1);
+    // staging: the largest of a droplet array, a source array, a flow field
+    // and the one-box tile tables of an upload
+    size_t stage = n;
+    const size_t flow_n = (size_t)g.nnx * g.nny * g.nz2;
+    const size_t tiles = (n / kUpdateThreads + 2 + (size_t)(g.ncells + 2) / kScanTile + 2) * 4 + 8;
+    if ((size_t)g.nnodes > stage) stage = (size_t)g.nnodes;
+    if (flow_n > stage) stage = flow_n;
+    if (tiles > stage) stage = tiles;
+    cv.take(&h.staging, stage);
+    cv.take(&h.rank, n);
+}
+
+int check_grid(ntlp_ctx *c, const ntlp_grid *g) {
+    if (!g || g->nnx < 2 || g->nny < 2 || g->nnz < 3)
+        return fail(c, NTLP_ERR_ARG, "grid must have nnx, nny >= 2 and nnz >= 3");
+    if (!g->z || !g->zz || !g->dzw || !g->dzu) return fail(c, NTLP_ERR_ARG, "grid arrays must not be NULL");
+    if (!(g->xl > 0 && g->yl > 0 && g->zl > 0)) return fail(c, NTLP_ERR_ARG, "domain lengths must be positive");
+    for (int i = 1; i < g->nnz + 2; ++i) {
+        if (!(g->z[i] > g->z[i - 1]) || !(g->zz[i] > g->zz[i - 1]))
+            return fail(c, NTLP_ERR_ARG, "z and zz must increase strictly (level %d)", i);
+    }
+    long long ncells = (long long)(g->nnx + 1) * (g->nny + 1) * (g->nnz + 1);
+    long long npad = (long long)(g->nnx + 5) * (g->nny + 5) * (g->nnz + 2);
+    if (ncells + 3 > 0x7fffffffLL || npad > 0x7fffffffLL)
+        return fail(c, NTLP_ERR_ARG, "grid too large for 32-bit cell indices");
+    return NTLP_OK;
+}
+
+// Stream-ordered allocation from the device's default pool.  Freed blocks
+// stay in the pool for reuse; if a request cannot be met, the pool's unused
+// memory is returned to the device once and the request retried.
+cudaError_t pool_alloc(ntlp_ctx *c, void **p, size_t bytes) {
+    cudaError_t e = cudaMallocAsync(p, bytes, c->stream);
+    if (e == cudaSuccess) return e;
+    cudaGetLastError();
     *p = nullptr;
-    if (count == 0) count = 1;
-    cudaError_t e = cudaMalloc((void **)p, count * sizeof(T));
+    cudaMemPool_t mp;
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess || cudaDeviceGetDefaultMemPool(&mp, c->device) != cudaSuccess)
+        return e;
+    cudaMemPoolTrimTo(mp, 0);
+    e = cudaMallocAsync(p, bytes, c->stream);
     if (e != cudaSuccess) {
+        cudaGetLastError();
         *p = nullptr;
-        return fail(c, NTLP_ERR_NOMEM, "cudaMalloc of %zu bytes failed: %s", count * sizeof(T),
-                    cudaGetErrorString(e));
     }
-    c->allocs.push_back((void *)*p);
-    c->bytes += (int64_t)(count * sizeof(T));
+    return e;
+}
+
+void fill_devparams(const ntlp_params *p, DevParams &d) {
+    d.ilin = p->ilin; d.icouple = p->icouple; d.iTcouple = p->iTcouple; d.iHcouple = p->iHcouple;
+    d.ievap = p->ievap; d.iexner = p->iexner; d.icase = p->icase; d.precision = p->precision;
+    d.nuf = p->nuf; d.Cpa = p->Cpa; d.Cpp = p->Cpp; d.Pra = p->Pra; d.Sc = p->Sc; d.Rd = p->Rd;
+    d.rhow = p->rhow; d.rhos = p->rhos; d.Mw = p->Mw; d.Ru = p->Ru; d.Gam = p->Gam; d.Lv = p->Lv;
+    d.Cpv = p->Cpv; d.grav = p->grav;
+    for (int a = 0; a < 3; ++a) d.g[a] = p->part_grav[a];
+    d.radius_init = p->radius_init; d.surf_rho = p->surf_rho; d.surf_p = p->surf_p;
+    d.tsfcc1 = p->tsfcc1; d.pi2 = p->pi2;
+    d.CpaCpp = p->Cpa / p->Cpp;                       // les.F:10759
+    d.Sc13 = ntlp_pow(p->Sc, 1.0 / 3.0);              // Sc**(1./3.)
+    d.Pra13 = ntlp_pow(p->Pra, 1.0 / 3.0);            // Pra**(1./3.)
+}
+
+int push_boxes(ntlp_ctx *c) {
+    CK(cudaMemcpyAsync(c->box_d, c->box.data(), sizeof(DevBox) * c->nbox, cudaMemcpyHostToDevice, c->stream));
     return NTLP_OK;
 }
 
-#define DA(ptr, n)                                \
-    do {                                          \
-        int r_ = dalloc(c, &(ptr), (size_t)(n));  \
-        if (r_) return r_;                        \
-    } while (0)
-
-std::vector<Tile> make_tiles(long long n, int per) {
-    std::vector<Tile> v;
-    for (long long s = 0; s < n; s += per) v.push_back(Tile{0, (int)s});
-    if (v.empty()) v.push_back(Tile{0, 0});
-    return v;
-}
-
-int alloc_state(ntlp_ctx *c, DevState &s, bool rk3) {
-    const size_t n = (size_t)c->cap;
-    for (int a = 0; a < 3; ++a) { DA(s.x[a], n); DA(s.v[a], n); DA(s.uf[a], n); DA(s.vold[a], n); }
-    DA(s.Tp, n); DA(s.r, n); DA(s.m_s, n); DA(s.kap, n); DA(s.rc, n); DA(s.res, n);
-    DA(s.actres, n); DA(s.numact, n); DA(s.mult, n); DA(s.lid, n);
-    DA(s.Tf, n); DA(s.qinf, n); DA(s.qstar, n); DA(s.Tpold, n); DA(s.rold, n);
-    if (rk3) {
-        for (int a = 0; a < 3; ++a) { DA(s.xrhs[a], n); DA(s.vrhs[a], n); }
-        DA(s.Tprhs_s, n); DA(s.Tprhs_L, n); DA(s.radrhs, n);
-    }
-    return NTLP_OK;
-}
-
-int push_box(ntlp_ctx *c) {
-    CK(cudaMemcpyAsync(c->box_d, &c->box, sizeof(DevBox), cudaMemcpyHostToDevice, c->stream));
-    return NTLP_OK;
-}
-
-int pull_box(ntlp_ctx *c) {
-    CK(cudaMemcpyAsync(&c->box, c->box_d, sizeof(DevBox), cudaMemcpyDeviceToHost, c->stream));
+int pull_boxes(ntlp_ctx *c) {
+    CK(cudaMemcpyAsync(c->box.data(), c->box_d, sizeof(DevBox) * c->nbox, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return NTLP_OK;
 }
 
-int read_n_alive(ntlp_ctx *c, int *n) {
-    CK(cudaMemcpyAsync(n, c->box.n_alive, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+int read_n_alive(ntlp_ctx *c, int b, int *n) {
+    CK(cudaMemcpyAsync(n, c->box[b].n_alive, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return NTLP_OK;
 }
@@ -193,38 +317,6 @@ __global__ void k_col_to_flow(const double *__restrict__ col, double *__restrict
     }
 }
 
-int check_grid(ntlp_ctx *c, const ntlp_grid *g) {
-    if (!g || g->nnx < 2 || g->nny < 2 || g->nnz < 3)
-        return fail(c, NTLP_ERR_ARG, "grid must have nnx, nny >= 2 and nnz >= 3");
-    if (!g->z || !g->zz || !g->dzw || !g->dzu) return fail(c, NTLP_ERR_ARG, "grid arrays must not be NULL");
-    if (!(g->xl > 0 && g->yl > 0 && g->zl > 0)) return fail(c, NTLP_ERR_ARG, "domain lengths must be positive");
-    for (int i = 1; i < g->nnz + 2; ++i) {
-        if (!(g->z[i] > g->z[i - 1]) || !(g->zz[i] > g->zz[i - 1]))
-            return fail(c, NTLP_ERR_ARG, "z and zz must increase strictly (level %d)", i);
-    }
-    long long ncells = (long long)(g->nnx + 1) * (g->nny + 1) * (g->nnz + 1);
-    long long npad = (long long)(g->nnx + 5) * (g->nny + 5) * (g->nnz + 2);
-    if (ncells + 3 > 0x7fffffffLL || npad > 0x7fffffffLL)
-        return fail(c, NTLP_ERR_ARG, "grid too large for 32-bit cell indices");
-    return NTLP_OK;
-}
-
-void fill_devparams(const ntlp_params *p, DevParams &d) {
-    d.ilin = p->ilin; d.icouple = p->icouple; d.iTcouple = p->iTcouple; d.iHcouple = p->iHcouple;
-    d.ievap = p->ievap; d.iexner = p->iexner; d.icase = p->icase; d.precision = p->precision;
-    d.nuf = p->nuf; d.Cpa = p->Cpa; d.Cpp = p->Cpp; d.Pra = p->Pra; d.Sc = p->Sc; d.Rd = p->Rd;
-    d.rhow = p->rhow; d.rhos = p->rhos; d.Mw = p->Mw; d.Ru = p->Ru; d.Gam = p->Gam; d.Lv = p->Lv;
-    d.Cpv = p->Cpv; d.grav = p->grav;
-    for (int a = 0; a < 3; ++a) d.g[a] = p->part_grav[a];
-    d.radius_init = p->radius_init; d.surf_rho = p->surf_rho; d.surf_p = p->surf_p;
-    d.tsfcc1 = p->tsfcc1; d.pi2 = p->pi2;
-    d.CpaCpp = p->Cpa / p->Cpp;                       // les.F:10759
-    d.Sc13 = ntlp_pow(p->Sc, 1.0 / 3.0);              // Sc**(1./3.)
-    d.Pra13 = ntlp_pow(p->Pra, 1.0 / 3.0);            // Pra**(1./3.)
-}
-
-enum Phase { PH_UPDATE = 0, PH_SORT = 1, PH_DEPOSIT = 2, PH_OTHER = 3 };
-
 cudaEvent_t ev_get(ntlp_ctx *c) {
     cudaEvent_t e = nullptr;
     if (!c->pool.empty()) {
@@ -236,7 +328,6 @@ cudaEvent_t ev_get(ntlp_ctx *c) {
     return e;
 }
 
-// returns the start event (or null when profiling is off)
 cudaEvent_t phase_begin(ntlp_ctx *c) {
     if (!c->prof) return nullptr;
     cudaEvent_t a = ev_get(c);
@@ -251,168 +342,540 @@ void phase_end(ntlp_ctx *c, int phase, cudaEvent_t a) {
     c->recs.push_back({phase, a, b});
 }
 
+bool box_ok(ntlp_ctx *c, int b) { return c && b >= 0 && b < c->nbox; }
+
 }  // namespace
 
-extern "C" {
-
-int ntlp_ctx_create(const ntlp_grid *grid, const ntlp_params *params, int64_t capacity, ntlp_ctx **out) {
-    if (!out) return NTLP_ERR_ARG;
-    *out = nullptr;
-    ntlp_ctx *c = new ntlp_ctx();
-    auto bail = [&](int code) {
-        ntlp_ctx_destroy(c);
-        return code;
-    };
-    static thread_local std::string create_err;
-    int rc = check_grid(c, grid);
-    if (!rc && !params) rc = fail(c, NTLP_ERR_ARG, "params must not be NULL");
-    if (!rc && (capacity < 1 || capacity > 0x7fffffffLL)) rc = fail(c, NTLP_ERR_ARG, "capacity out of range");
-    if (!rc && params->precision != NTLP_PREC_FP64 && params->precision != NTLP_PREC_MIXED)
-        rc = fail(c, NTLP_ERR_ARG, "unknown precision %d", params->precision);
-    if (rc) {
-        fprintf(stderr, "ntlp_ctx_create: %s\n", c->err.c_str());
-        return bail(rc);
-    }
-    if (cudaGetDevice(&c->device) != cudaSuccess) {
-        fprintf(stderr, "ntlp_ctx_create: no CUDA device\n");
-        return bail(NTLP_ERR_CUDA);
-    }
-    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(NTLP_ERR_CUDA);
-    c->grid = *grid;
-    const int nz2 = grid->nnz + 2, nz3 = grid->nnz + 3;
-    c->z.assign(grid->z, grid->z + nz2);
-    c->zz.assign(grid->zz, grid->zz + nz2);
-    c->dzw.assign(grid->dzw, grid->dzw + nz3);
-    c->dzu.assign(grid->dzu, grid->dzu + nz3);
-    c->params = *params;
-    c->cap = capacity;
-    fill_devparams(params, c->dp);
-
-    DevGrid &g = c->box.g;
-    g.nnx = grid->nnx; g.nny = grid->nny; g.nnz = grid->nnz;
-    g.nz2 = nz2; g.ny5 = grid->nny + 5; g.nx5 = grid->nnx + 5;
-    g.dx = grid->xl / grid->nnx;   // les.F:5491
-    g.dy = grid->yl / grid->nny;   // les.F:5492
-    g.xl = grid->xl; g.yl = grid->yl; g.zl = grid->zl;
-    g.ncells = (long long)(grid->nnx + 1) * (grid->nny + 1) * (grid->nnz + 1);
-    g.nnodes = (long long)nz2 * grid->nny * grid->nnx;
-    double *z_d, *zz_d, *dzw_d, *dzu_d;
-    if ((rc = dalloc(c, &z_d, nz2)) || (rc = dalloc(c, &zz_d, nz2)) || (rc = dalloc(c, &dzw_d, nz3)) ||
-        (rc = dalloc(c, &dzu_d, nz3)))
-        return bail(rc);
-    cudaMemcpy(z_d, c->z.data(), nz2 * 8, cudaMemcpyHostToDevice);
-    cudaMemcpy(zz_d, c->zz.data(), nz2 * 8, cudaMemcpyHostToDevice);
-    cudaMemcpy(dzw_d, c->dzw.data(), nz3 * 8, cudaMemcpyHostToDevice);
-    cudaMemcpy(dzu_d, c->dzu.data(), nz3 * 8, cudaMemcpyHostToDevice);
-    g.z = z_d; g.zz = zz_d; g.dzw = dzw_d; g.dzu = dzu_d;
-
-    const long long npad = (long long)g.nz2 * g.ny5 * g.nx5;
-    for (int k = 0; k < 5; ++k) {
-        double *f;
-        if ((rc = dalloc(c, &f, (size_t)npad))) return bail(rc);
-        c->box.f[k] = f;
-    }
-    if (params->precision == NTLP_PREC_MIXED) {
-        float4 *f4;
-        float *fw;
-        if ((rc = dalloc(c, &f4, (size_t)npad)) || (rc = dalloc(c, &fw, (size_t)npad))) return bail(rc);
-        c->box.f4 = f4;
-        c->box.fw = fw;
-    }
-    for (int b = 0; b < 2; ++b)
-        if ((rc = alloc_state(c, c->box.st[b], false))) return bail(rc);
-    const size_t n = (size_t)capacity;
-    if (params->precision == NTLP_PREC_MIXED) {
-        for (int q = 0; q < P32_N; ++q)
-            if ((rc = dalloc(c, &c->box.pay32.f[q], n))) return bail(rc);
-    } else {
-        DevPayload &P = c->box.pay;
-        for (int a = 0; a < 3; ++a) {
-            if ((rc = dalloc(c, &P.D[a], n)) || (rc = dalloc(c, &P.V[a], n))) return bail(rc);
-        }
-        if ((rc = dalloc(c, &P.T0, n)) || (rc = dalloc(c, &P.H0, n)) || (rc = dalloc(c, &P.E1, n)) ||
-            (rc = dalloc(c, &P.E2, n)) || (rc = dalloc(c, &P.mult, n)))
-            return bail(rc);
-    }
-    c->box.cap = (int)capacity;
-    if ((rc = dalloc(c, &c->box.n_alive, 1)) || (rc = dalloc(c, &c->box.perm, n)) ||
-        (rc = dalloc(c, &c->box.key, n)) || (rc = dalloc(c, &c->box.sorted, n)) ||
-        (rc = dalloc(c, &c->box.cell_cnt, (size_t)g.ncells + 2)) ||
-        (rc = dalloc(c, &c->box.cell_start, (size_t)g.ncells + 3)) ||
-        (rc = dalloc(c, &c->box.counters, kNumCounters)) || (rc = dalloc(c, &c->box.pflux, g.nnz + 1)) ||
-        (rc = dalloc(c, &c->box.flux_fx, (size_t)2 * (g.nnz + 1) * kFluxLimbs)) ||
-        (rc = dalloc(c, &c->box.err, 1)) || (rc = dalloc(c, &c->box.defer, n)) ||
-        (rc = dalloc(c, &c->box.ndefer, 1)))
-        return bail(rc);
-    for (int q = 0; q < 6; ++q)
-        if ((rc = dalloc(c, &c->box.src[q], (size_t)g.nnodes))) return bail(rc);
-    cudaMemset(c->box.cell_cnt, 0, sizeof(int) * (size_t)(g.ncells + 2));
-    cudaMemset(c->box.n_alive, 0, sizeof(int));
-    cudaMemset(c->box.counters, 0, sizeof(long long) * kNumCounters);
-    c->box.cur = 0;
-
-    size_t stage = (size_t)capacity;
-    size_t flow_n = (size_t)grid->nnx * grid->nny * nz2;
-    if ((size_t)g.nnodes > stage) stage = (size_t)g.nnodes;
-    if (flow_n > stage) stage = flow_n;
-    if ((rc = dalloc(c, &c->staging_d, stage)) || (rc = dalloc(c, &c->rank_d, n))) return bail(rc);
-
-    c->drop_tiles = make_tiles(capacity, kUpdateThreads);
-    c->cell_tiles = make_tiles(g.ncells + 2, kScanTile);
-    c->node_tiles = make_tiles(deposit_tile_count(g.nnx, g.nny, g.nnz), 1);
-    if ((rc = dalloc(c, &c->drop_tiles_d, c->drop_tiles.size())) ||
-        (rc = dalloc(c, &c->cell_tiles_d, c->cell_tiles.size())) ||
-        (rc = dalloc(c, &c->node_tiles_d, c->node_tiles.size())) ||
-        (rc = dalloc(c, &c->tile_sums_d, c->cell_tiles.size())) || (rc = dalloc(c, &c->box_first_tile_d, 2)) ||
-        (rc = dalloc(c, &c->dp_d, 1)) || (rc = dalloc(c, &c->box_d, 1)))
-        return bail(rc);
-    cudaMemcpy(c->drop_tiles_d, c->drop_tiles.data(), c->drop_tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice);
-    cudaMemcpy(c->cell_tiles_d, c->cell_tiles.data(), c->cell_tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice);
-    cudaMemcpy(c->node_tiles_d, c->node_tiles.data(), c->node_tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice);
-    int bft[2] = {0, (int)c->cell_tiles.size()};
-    cudaMemcpy(c->box_first_tile_d, bft, sizeof bft, cudaMemcpyHostToDevice);
-    cudaMemcpy(c->dp_d, &c->dp, sizeof(DevParams), cudaMemcpyHostToDevice);
-    c->plan.drop_tiles = c->drop_tiles_d;
-    c->plan.n_drop_tiles = (int)c->drop_tiles.size();
-    c->plan.cell_tiles = c->cell_tiles_d;
-    c->plan.n_cell_tiles = (int)c->cell_tiles.size();
-    c->plan.tile_sums = c->tile_sums_d;
-    c->plan.box_first_tile = c->box_first_tile_d;
-    c->plan.nbox = 1;
-    if (cudaMallocHost((void **)&c->counters_h, sizeof(long long) * kNumCounters) != cudaSuccess)
-        return bail(NTLP_ERR_NOMEM);
-    if (push_box(c)) return bail(NTLP_ERR_CUDA);
-    if (cudaStreamSynchronize(c->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess)
-        return bail(NTLP_ERR_CUDA);
-    *out = c;
-    return NTLP_OK;
-}
-
-void ntlp_ctx_destroy(ntlp_ctx *c) {
+extern "C" void ntlp_ctx_destroy(ntlp_ctx *c) {
     if (!c) return;
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->gexec) cudaGraphExecDestroy(c->gexec);
     for (auto &r : c->recs) {
         cudaEventDestroy(r.a);
         cudaEventDestroy(r.b);
     }
     for (cudaEvent_t e : c->pool) cudaEventDestroy(e);
-    for (void *p : c->allocs) cudaFree(p);
+    for (auto &h : c->bh) {
+        if (h.arena) cudaFreeAsync(h.arena, c->stream);
+        if (h.arena_rk3) cudaFreeAsync(h.arena_rk3, c->stream);
+    }
+    if (c->small_arena) cudaFreeAsync(c->small_arena, c->stream);
+    if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->counters_h) cudaFreeHost(c->counters_h);
-    if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
+}
+
+namespace {
+
+void box_geometry(const ntlp_grid &grid, int64_t cap, DevBox &B) {
+    DevGrid &g = B.g;
+    g.nnx = grid.nnx; g.nny = grid.nny; g.nnz = grid.nnz;
+    g.nz2 = grid.nnz + 2; g.ny5 = grid.nny + 5; g.nx5 = grid.nnx + 5;
+    g.dx = grid.xl / grid.nnx;   // les.F:5491
+    g.dy = grid.yl / grid.nny;   // les.F:5492
+    g.xl = grid.xl; g.yl = grid.yl; g.zl = grid.zl;
+    g.ncells = (long long)(grid.nnx + 1) * (grid.nny + 1) * (grid.nnz + 1);
+    g.nnodes = (long long)g.nz2 * grid.nny * grid.nnx;
+    B.cap = (int)cap;
+    B.cur = 0;
+}
+
+int create(int nbox, const ntlp_grid *grids, const ntlp_params *params, const int64_t *caps, ntlp_ctx **out) {
+    if (!out) return NTLP_ERR_ARG;
+    *out = nullptr;
+    ntlp_ctx *c = new ntlp_ctx();
+    auto bail = [&](int code) {
+        if (!c->err.empty()) fprintf(stderr, "ntlp context creation: %s\n", c->err.c_str());
+        ntlp_ctx_destroy(c);
+        return code;
+    };
+    int rc = NTLP_OK;
+    if (nbox < 1 || !grids || !caps) rc = fail(c, NTLP_ERR_ARG, "need nbox >= 1, grids and capacities");
+    if (!rc && !params) rc = fail(c, NTLP_ERR_ARG, "params must not be NULL");
+    if (!rc && params->precision != NTLP_PREC_FP64 && params->precision != NTLP_PREC_MIXED)
+        rc = fail(c, NTLP_ERR_ARG, "unknown precision %d", params->precision);
+    for (int b = 0; !rc && b < nbox; ++b) {
+        rc = check_grid(c, &grids[b]);
+        if (!rc && (caps[b] < 1 || caps[b] > 0x7fffffffLL))
+            rc = fail(c, NTLP_ERR_ARG, "capacity of box %d out of range", b);
+    }
+    if (rc) return bail(rc);
+    if (cudaGetDevice(&c->device) != cudaSuccess) return bail(fail(c, NTLP_ERR_CUDA, "no CUDA device"));
+    if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        c->own_stream = nullptr;
+        return bail(fail(c, NTLP_ERR_CUDA, "stream creation failed"));
+    }
+    c->stream = c->own_stream;
+    {
+        // keep freed pool memory for reuse instead of returning it to the driver
+        cudaMemPool_t mp;
+        if (cudaDeviceGetDefaultMemPool(&mp, c->device) == cudaSuccess) {
+            uint64_t thr = UINT64_MAX;
+            cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &thr);
+        }
+    }
+    c->nbox = nbox;
+    c->params = *params;
+    fill_devparams(params, c->dp);
+    c->bh.resize(nbox);
+    c->box.assign(nbox, DevBox{});
+    const bool mixed = params->precision == NTLP_PREC_MIXED;
+    for (int b = 0; b < nbox; ++b) {
+        BoxHost &h = c->bh[b];
+        const ntlp_grid *grid = &grids[b];
+        h.grid = *grid;
+        const int nz2 = grid->nnz + 2, nz3 = grid->nnz + 3;
+        h.z.assign(grid->z, grid->z + nz2);
+        h.zz.assign(grid->zz, grid->zz + nz2);
+        h.dzw.assign(grid->dzw, grid->dzw + nz3);
+        h.dzu.assign(grid->dzu, grid->dzu + nz3);
+        h.cap = caps[b];
+        DevBox &B = c->box[b];
+        const DevGrid &g = B.g;
+        box_geometry(*grid, h.cap, B);
+        Carver cv;
+        carve_box(cv, h, B, mixed);
+        h.arena_bytes = cv.off;
+        if (pool_alloc(c, &h.arena, cv.off) != cudaSuccess) {
+            return bail(fail(c, NTLP_ERR_NOMEM, "device allocation of %zu bytes for box %d refused", cv.off, b));
+        }
+        c->bytes += (int64_t)cv.off;
+        Carver cv2;
+        cv2.base = (unsigned char *)h.arena;
+        carve_box(cv2, h, B, mixed);
+        if (cudaMemcpyAsync((void *)B.g.z, h.z.data(), nz2 * 8, cudaMemcpyHostToDevice, c->stream) ||
+            cudaMemcpyAsync((void *)B.g.zz, h.zz.data(), nz2 * 8, cudaMemcpyHostToDevice, c->stream) ||
+            cudaMemcpyAsync((void *)B.g.dzw, h.dzw.data(), nz3 * 8, cudaMemcpyHostToDevice, c->stream) ||
+            cudaMemcpyAsync((void *)B.g.dzu, h.dzu.data(), nz3 * 8, cudaMemcpyHostToDevice, c->stream) ||
+            cudaMemsetAsync(B.cell_cnt, 0, sizeof(int) * (size_t)(g.ncells + 2), c->stream) ||
+            cudaMemsetAsync(B.n_alive, 0, sizeof(int), c->stream) ||
+            cudaMemsetAsync(B.counters, 0, sizeof(long long) * kNumCounters, c->stream))
+            return bail(fail(c, NTLP_ERR_CUDA, "initialising box %d failed", b));
+    }
+    // tiles: droplets (128 and 256 per tile), cells (scan tiles), deposition (3 shapes)
+    std::vector<Tile> dt[kNtVariants], ct, dpt[kDepVariants];
+    std::vector<int> bft;
+    for (int b = 0; b < nbox; ++b) {
+        const DevGrid &g = c->box[b].g;
+        for (int v = 0; v < kNtVariants; ++v)
+            for (long long s = 0; s < c->bh[b].cap; s += kNtValues[v]) dt[v].push_back(Tile{b, (int)s});
+        bft.push_back((int)ct.size());
+        for (long long s = 0; s < g.ncells + 2; s += kScanTile) ct.push_back(Tile{b, (int)s});
+        for (int v = 0; v < kDepVariants; ++v) {
+            long long nt = deposit_tile_count(v, g.nnx, g.nny, g.nnz);
+            for (long long s = 0; s < nt; ++s) dpt[v].push_back(Tile{b, (int)s});
+        }
+    }
+    bft.push_back((int)ct.size());
+    {
+        auto lay = [&](Carver &k) {
+            for (int v = 0; v < kNtVariants; ++v) k.take(&c->drop_tiles_d[v], dt[v].size());
+            k.take(&c->cell_tiles_d, ct.size());
+            for (int v = 0; v < kDepVariants; ++v) k.take(&c->dep_tiles_d[v], dpt[v].size());
+            k.take(&c->tile_sums_d, ct.size());
+            k.take(&c->box_first_tile_d, bft.size());
+            k.take(&c->dp_d, 1);
+            k.take(&c->box_d, (size_t)nbox);
+        };
+        Carver cv;
+        lay(cv);
+        if (pool_alloc(c, &c->small_arena, cv.off) != cudaSuccess) {
+            return bail(fail(c, NTLP_ERR_NOMEM, "device allocation of the tile tables refused"));
+        }
+        c->bytes += (int64_t)cv.off;
+        Carver cv2;
+        cv2.base = (unsigned char *)c->small_arena;
+        lay(cv2);
+    }
+    bool bad = false;
+    for (int v = 0; v < kNtVariants; ++v) {
+        c->n_drop_tiles[v] = (int)dt[v].size();
+        bad |= cudaMemcpyAsync(c->drop_tiles_d[v], dt[v].data(), dt[v].size() * sizeof(Tile), cudaMemcpyHostToDevice,
+                               c->stream) != cudaSuccess;
+    }
+    c->n_cell_tiles = (int)ct.size();
+    bad |= cudaMemcpyAsync(c->cell_tiles_d, ct.data(), ct.size() * sizeof(Tile), cudaMemcpyHostToDevice,
+                           c->stream) != cudaSuccess;
+    for (int v = 0; v < kDepVariants; ++v) {
+        c->n_dep_tiles[v] = (int)dpt[v].size();
+        bad |= cudaMemcpyAsync(c->dep_tiles_d[v], dpt[v].data(), dpt[v].size() * sizeof(Tile),
+                               cudaMemcpyHostToDevice, c->stream) != cudaSuccess;
+    }
+    bad |= cudaMemcpyAsync(c->box_first_tile_d, bft.data(), bft.size() * sizeof(int), cudaMemcpyHostToDevice,
+                           c->stream) != cudaSuccess;
+    bad |= cudaMemcpyAsync(c->dp_d, &c->dp, sizeof(DevParams), cudaMemcpyHostToDevice, c->stream) != cudaSuccess;
+    if (bad) return bail(fail(c, NTLP_ERR_CUDA, "uploading the tile tables failed"));
+    c->plan.drop_tiles = c->drop_tiles_d[0];
+    c->plan.n_drop_tiles = c->n_drop_tiles[0];
+    c->plan.cell_tiles = c->cell_tiles_d;
+    c->plan.n_cell_tiles = c->n_cell_tiles;
+    c->plan.tile_sums = c->tile_sums_d;
+    c->plan.box_first_tile = c->box_first_tile_d;
+    c->plan.nbox = nbox;
+    if (cudaMallocHost((void **)&c->counters_h, sizeof(long long) * kNumCounters * nbox) != cudaSuccess)
+        return bail(fail(c, NTLP_ERR_NOMEM, "pinned counter buffer refused"));
+    if (push_boxes(c)) return bail(NTLP_ERR_CUDA);
+    if (mixed) prepare_kernels_mixed(); else prepare_kernels64();
+    // the host vectors above are copied from: wait before they go out of scope
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess)
+        return bail(fail(c, NTLP_ERR_CUDA, "context set-up failed"));
+    *out = c;
+    return NTLP_OK;
+}
+
+int alloc_rk3(ntlp_ctx *c) {
+    if (c->have_rk3) return NTLP_OK;
+    CK(cudaStreamSynchronize(c->stream));
+    if (pull_boxes(c)) return NTLP_ERR_CUDA;
+    for (int b = 0; b < c->nbox; ++b) {
+        BoxHost &h = c->bh[b];
+        DevBox &B = c->box[b];
+        Carver cv;
+        carve_rk3(cv, B.st[0], (size_t)h.cap);
+        carve_rk3(cv, B.st[1], (size_t)h.cap);
+        if (pool_alloc(c, &h.arena_rk3, cv.off) != cudaSuccess) {
+            return fail(c, NTLP_ERR_NOMEM, "device allocation of the RK3 state refused");
+        }
+        c->bytes += (int64_t)cv.off;
+        CK(cudaMemsetAsync(h.arena_rk3, 0, cv.off, c->stream));
+        Carver cv2;
+        cv2.base = (unsigned char *)h.arena_rk3;
+        carve_rk3(cv2, B.st[0], (size_t)h.cap);
+        carve_rk3(cv2, B.st[1], (size_t)h.cap);
+    }
+    c->have_rk3 = true;
+    return push_boxes(c);
+}
+
+int fields_ext(ntlp_ctx *c, int b, const double *const h[5]) {
+    if (!box_ok(c, b)) return fail(c, NTLP_ERR_ARG, "box %d out of range", b);
+    for (int k = 0; k < 5; ++k)
+        if (!h[k]) return fail(c, NTLP_ERR_ARG, "field %d is NULL", k);
+    const DevBox &B = c->box[b];
+    const size_t npad = (size_t)B.g.nz2 * B.g.ny5 * B.g.nx5;
+    for (int k = 0; k < 5; ++k)
+        CK(cudaMemcpyAsync((void *)B.f[k], h[k], npad * 8, cudaMemcpyDefault, c->stream));
+    if (B.f4) launch_pack_f32(&B, (float4 *)B.f4, (float *)B.fw, c->stream);
+    CK(cudaGetLastError());
+    c->bh[b].have_fields = true;
+    return NTLP_OK;
+}
+
+int fields_flow(ntlp_ctx *c, int b, const double *const h[5]) {
+    if (!box_ok(c, b)) return fail(c, NTLP_ERR_ARG, "box %d out of range", b);
+    for (int k = 0; k < 5; ++k)
+        if (!h[k]) return fail(c, NTLP_ERR_ARG, "field %d is NULL", k);
+    const DevBox &B = c->box[b];
+    const size_t nflow = (size_t)B.g.nnx * B.g.nny * B.g.nz2;
+    double *stg = c->bh[b].staging;
+    for (int k = 0; k < 5; ++k) {
+        CK(cudaMemcpyAsync(stg, h[k], nflow * 8, cudaMemcpyDefault, c->stream));
+        launch_fill_ext(stg, (double *)B.f[k], B.g, c->stream);
+    }
+    if (B.f4) launch_pack_f32(&B, (float4 *)B.f4, (float *)B.fw, c->stream);
+    CK(cudaGetLastError());
+    c->bh[b].have_fields = true;
+    return NTLP_OK;
+}
+
+int droplets_upload(ntlp_ctx *c, int b, const ntlp_droplets *d) {
+    if (!box_ok(c, b) || !d) return fail(c, NTLP_ERR_ARG, "bad box or droplet structure");
+    BoxHost &h = c->bh[b];
+    if (d->n < 0 || d->n > h.cap)
+        return fail(c, NTLP_ERR_CAPACITY, "%lld droplets exceed capacity %lld", (long long)d->n, (long long)h.cap);
+    if (!d->xp[0] || !d->xp[1] || !d->xp[2] || !d->vp[0] || !d->vp[1] || !d->vp[2] || !d->Tp || !d->radius ||
+        !d->m_s || !d->kappa_s || !d->mult)
+        return fail(c, NTLP_ERR_ARG, "xp, vp, Tp, radius, m_s, kappa_s and mult are required");
+    const int n = (int)d->n;
+    bool rk3_given = d->xrhs[0] || d->vrhs[0] || d->Tprhs_s || d->Tprhs_L || d->radrhs;
+    if (rk3_given && alloc_rk3(c)) return NTLP_ERR_NOMEM;
+    if (pull_boxes(c)) return NTLP_ERR_CUDA;
+    // the uploaded state goes into st[1-cur] in list order; the initial sort
+    // and the finish kernel then make it current
+    const DevState &O = c->box[b].st[1 - c->box[b].cur];
+    auto up = [&](void *dst, const void *src, size_t esz) -> int {
+        if (!dst) return NTLP_OK;
+        if (src) {
+            CK(cudaMemcpyAsync(dst, src, (size_t)n * esz, cudaMemcpyDefault, c->stream));
+        } else {
+            CK(cudaMemsetAsync(dst, 0, (size_t)n * esz, c->stream));
+        }
+        return NTLP_OK;
+    };
+    int rc = 0;
+    for (int a = 0; a < 3; ++a) {
+        rc |= up(O.x[a], d->xp[a], 8);
+        rc |= up(O.v[a], d->vp[a], 8);
+        rc |= up(O.uf[a], d->uf[a], 8);
+        rc |= up(O.vold[a], d->vp_old[a], 8);
+        rc |= up(O.xrhs[a], d->xrhs[a], 8);
+        rc |= up(O.vrhs[a], d->vrhs[a], 8);
+    }
+    rc |= up(O.Tp, d->Tp, 8); rc |= up(O.r, d->radius, 8); rc |= up(O.m_s, d->m_s, 8);
+    rc |= up(O.kap, d->kappa_s, 8); rc |= up(O.rc, d->rc, 8); rc |= up(O.res, d->res, 8);
+    rc |= up(O.actres, d->actres, 8); rc |= up(O.numact, d->numact, 8); rc |= up(O.Tf, d->Tf, 8);
+    rc |= up(O.qinf, d->qinf, 8); rc |= up(O.qstar, d->qstar, 8); rc |= up(O.Tpold, d->Tp_old, 8);
+    rc |= up(O.rold, d->radius_old, 8); rc |= up(O.Tprhs_s, d->Tprhs_s, 8);
+    rc |= up(O.Tprhs_L, d->Tprhs_L, 8); rc |= up(O.radrhs, d->radrhs, 8); rc |= up(O.mult, d->mult, 8);
+    if (rc) return rc;
+    if (n > 0) k_iota<<<(n + 255) / 256, 256, 0, c->stream>>>(O.lid, n);
+    // sort this box alone (a one-box view of the descriptor array, with tile
+    // tables held in the box's staging buffer for the duration of the call)
+    DevBox *view = c->box_d + b;
+    CK(cudaMemcpyAsync(c->box[b].n_alive, &n, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    std::vector<Tile> dtl, ctl;
+    for (long long s = 0; s < h.cap; s += kUpdateThreads) dtl.push_back(Tile{0, (int)s});
+    for (long long s = 0; s < c->box[b].g.ncells + 2; s += kScanTile) ctl.push_back(Tile{0, (int)s});
+    Tile *dtd = (Tile *)h.staging;
+    Tile *ctd = dtd + dtl.size();
+    long long *sums = (long long *)(ctd + ctl.size());
+    int *bft = (int *)(sums + ctl.size());
+    const int bf[2] = {0, (int)ctl.size()};
+    CK(cudaMemcpyAsync(dtd, dtl.data(), dtl.size() * sizeof(Tile), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(ctd, ctl.data(), ctl.size() * sizeof(Tile), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(bft, bf, sizeof bf, cudaMemcpyHostToDevice, c->stream));
+    SortPlan plan{dtd, (int)dtl.size(), ctd, (int)ctl.size(), sums, bft, 1};
+    launch_keys_initial(view, dtd, (int)dtl.size(), c->stream);
+    launch_sort(view, plan, c->stream);
+    launch_finish(view, 1, c->stream);
+    CK(cudaGetLastError());
+    if (pull_boxes(c)) return NTLP_ERR_CUDA;   // also waits for the host vectors' copies
+    h.n_uploaded = n;
+    h.have_droplets = true;
+    c->payload_valid = false;
+    return NTLP_OK;
+}
+
+int droplets_download(ntlp_ctx *c, int b, ntlp_droplets *d) {
+    if (!box_ok(c, b) || !d) return fail(c, NTLP_ERR_ARG, "bad box or droplet structure");
+    BoxHost &h = c->bh[b];
+    if (!h.have_droplets) return fail(c, NTLP_ERR_STATE, "no droplets uploaded");
+    if (pull_boxes(c)) return NTLP_ERR_CUDA;
+    int n = 0;
+    if (read_n_alive(c, b, &n)) return NTLP_ERR_CUDA;
+    d->n = n;
+    if (n == 0) return NTLP_OK;
+    const DevBox &B = c->box[b];
+    const DevState &S = B.st[B.cur];
+    launch_rank_alive(c->box_d, b, h.rank, h.n_uploaded, c->stream);
+    const int blocks = (n + 255) / 256;
+    auto get = [&](const double *src, double *host) -> int {
+        if (!host || !src) return NTLP_OK;
+        k_gather_d<<<blocks, 256, 0, c->stream>>>(src, B.perm, S.lid, h.rank, h.staging, n);
+        CK(cudaMemcpyAsync(host, h.staging, (size_t)n * 8, cudaMemcpyDefault, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        return NTLP_OK;
+    };
+    int rc = 0;
+    for (int a = 0; a < 3; ++a) {
+        rc |= get(S.x[a], d->xp[a]);
+        rc |= get(S.v[a], d->vp[a]);
+        rc |= get(S.uf[a], d->uf[a]);
+        rc |= get(S.vold[a], d->vp_old[a]);
+        rc |= get(S.xrhs[a], d->xrhs[a]);
+        rc |= get(S.vrhs[a], d->vrhs[a]);
+    }
+    rc |= get(S.Tp, d->Tp); rc |= get(S.r, d->radius); rc |= get(S.m_s, d->m_s);
+    rc |= get(S.kap, d->kappa_s); rc |= get(S.rc, d->rc); rc |= get(S.res, d->res);
+    rc |= get(S.actres, d->actres); rc |= get(S.numact, d->numact); rc |= get(S.Tf, d->Tf);
+    rc |= get(S.qinf, d->qinf); rc |= get(S.qstar, d->qstar); rc |= get(S.Tpold, d->Tp_old);
+    rc |= get(S.rold, d->radius_old); rc |= get(S.Tprhs_s, d->Tprhs_s); rc |= get(S.Tprhs_L, d->Tprhs_L);
+    rc |= get(S.radrhs, d->radrhs);
+    if (rc) return rc;
+    if (d->mult) {
+        k_gather_i64<<<blocks, 256, 0, c->stream>>>(S.mult, B.perm, S.lid, h.rank, (long long *)h.staging, n);
+        CK(cudaMemcpyAsync(d->mult, h.staging, (size_t)n * 8, cudaMemcpyDefault, c->stream));
+    }
+    if (d->lid) {
+        k_gather_lid<<<blocks, 256, 0, c->stream>>>(B.perm, S.lid, h.rank, (int *)h.staging, n);
+        CK(cudaMemcpyAsync(d->lid, h.staging, (size_t)n * 4, cudaMemcpyDefault, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaGetLastError());
+    return NTLP_OK;
+}
+
+// launch the kernels of one step (no synchronisation; graph-capturable)
+int launch_step(ntlp_ctx *c, int kind, int istage, double dt, int32_t it, bool with_deposit) {
+    const int nt = kNtValues[c->nt_variant];
+    StepIn in;
+    in.dt = dt;
+    in.it = it;
+    in.istage = istage;
+    in.write_payload = (kind == 1 || istage == 3) ? 1 : 0;
+    cudaEvent_t e0 = phase_begin(c);
+    launch_reset_step(c->box_d, c->nbox, c->stream);
+    phase_end(c, PH_OTHER, e0);
+    e0 = phase_begin(c);
+    if (kind == 1) {
+        if (c->params.precision == NTLP_PREC_MIXED)
+            launch_update_be_mixed(c->params.ilin, nt, c->box_d, c->drop_tiles_d[c->nt_variant],
+                                   c->n_drop_tiles[c->nt_variant], c->nbox, c->dp_d, in, c->stream);
+        else
+            launch_update_be64(c->params.ilin, nt, c->box_d, c->drop_tiles_d[c->nt_variant],
+                               c->n_drop_tiles[c->nt_variant], c->nbox, c->dp_d, in, c->stream);
+        c->launches += kUpdateLaunches;
+    } else {
+        launch_update_rk3_64(c->params.ilin, c->box_d, c->drop_tiles_d[0], c->n_drop_tiles[0], c->dp_d, in,
+                             c->stream);
+        c->launches += 1;
+    }
+    phase_end(c, PH_UPDATE, e0);
+    e0 = phase_begin(c);
+    launch_sort(c->box_d, c->plan, c->stream);
+    launch_finish(c->box_d, c->nbox, c->stream);
+    phase_end(c, PH_SORT, e0);
+    c->launches += 1 + kSortLaunches + 1;
+    if (with_deposit) {
+        e0 = phase_begin(c);
+        const int v = c->dep_variant;
+        if (c->params.precision == NTLP_PREC_MIXED)
+            launch_deposit_mixed(v, c->box_d, c->dep_tiles_d[v], c->n_dep_tiles[v], c->dp_d, c->stream);
+        else
+            launch_deposit64(v, c->box_d, c->dep_tiles_d[v], c->n_dep_tiles[v], c->dp_d, c->stream);
+        phase_end(c, PH_DEPOSIT, e0);
+        c->launches += 1;
+    }
+    CK(cudaGetLastError());
+    return NTLP_OK;
+}
+
+// the host mirror follows the device's buffer flips
+void mirror_flip(ntlp_ctx *c, int nflips) {
+    if (nflips & 1) {
+        for (auto &B : c->box) {
+            B.cur = 1 - B.cur;
+            std::swap(B.perm, B.sorted);
+        }
+    }
+}
+
+int check_ready(ntlp_ctx *c, double dt) {
+    if (!(dt > 0.0)) return fail(c, NTLP_ERR_ARG, "dt must be positive");
+    bool any = false;
+    for (int b = 0; b < c->nbox; ++b) {
+        if (c->bh[b].have_droplets && !c->bh[b].have_fields)
+            return fail(c, NTLP_ERR_STATE, "box %d has droplets but no fields", b);
+        any = any || c->bh[b].have_droplets;
+    }
+    if (!any) return fail(c, NTLP_ERR_STATE, "droplets not uploaded");
+    return NTLP_OK;
+}
+
+int read_counters(ntlp_ctx *c) {
+    for (int b = 0; b < c->nbox; ++b)
+        CK(cudaMemcpyAsync(c->counters_h + (size_t)b * kNumCounters, c->box[b].counters,
+                           sizeof(long long) * kNumCounters, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return NTLP_OK;
+}
+
+void counters_of(const long long *v, ntlp_counters *out) {
+    out->numpart = v[C_NUMPART];
+    out->num_destroy = v[C_DESTROY];
+    out->denum = v[C_DENUM];
+    out->actnum = v[C_ACTNUM];
+    out->num100 = v[C_NUM100];
+    out->numimpos = v[C_NUMIMPOS];
+    out->neg_qinf = v[C_NEGQ];
+    out->bad_index = v[C_BAD];
+}
+
+int do_step(ntlp_ctx *c, int kind, int istage, double dt, int32_t it, ntlp_counters *counters) {
+    if (!c) return NTLP_ERR_ARG;
+    int rc = check_ready(c, dt);
+    if (rc) return rc;
+    if (kind == 2 && (rc = alloc_rk3(c))) return rc;
+    if ((rc = launch_step(c, kind, istage, dt, it, false))) return rc;
+    mirror_flip(c, 1);
+    const bool payload = (kind == 1 || istage == 3);
+    c->payload_valid = payload;
+    if (payload) c->last_dt = dt;
+    if (!counters) return NTLP_OK;
+    if ((rc = read_counters(c))) return rc;
+    long long sum[kNumCounters] = {0};
+    for (int b = 0; b < c->nbox; ++b)
+        for (int k = 0; k < kNumCounters; ++k) sum[k] += c->counters_h[(size_t)b * kNumCounters + k];
+    counters_of(sum, counters);
+    return NTLP_OK;
+}
+
+int sources_out(ntlp_ctx *c, int b, int32_t layout, double *const host[6]) {
+    const DevBox &B = c->box[b];
+    const DevGrid &g = B.g;
+    const size_t nn = (size_t)g.nnodes;
+    bool any = false;
+    for (int q = 0; q < 6; ++q) {
+        if (!host[q]) continue;
+        any = true;
+        const double *src = B.src[q];
+        if (layout == NTLP_LAYOUT_FLOW) {
+            dim3 grid((g.nnx + 31) / 32, (g.nz2 + 31) / 32, g.nny);
+            k_col_to_flow<<<grid, dim3(32, 8), 0, c->stream>>>(src, c->bh[b].staging, g.nnx, g.nny, g.nz2);
+            c->launches += 1;
+            src = c->bh[b].staging;
+        }
+        CK(cudaMemcpyAsync(host[q], src, nn * 8, cudaMemcpyDefault, c->stream));
+        if (layout == NTLP_LAYOUT_FLOW) CK(cudaStreamSynchronize(c->stream));
+    }
+    if (any) CK(cudaStreamSynchronize(c->stream));
+    CK(cudaGetLastError());
+    return NTLP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ntlp_ctx_create(const ntlp_grid *grid, const ntlp_params *params, int64_t capacity, ntlp_ctx **out) {
+    return create(1, grid, params, &capacity, out);
+}
+
+int ntlp_batch_create(int32_t nbox, const ntlp_grid *grids, const ntlp_params *params, const int64_t *capacities,
+                      ntlp_ctx **out) {
+    return create(nbox, grids, params, capacities, out);
+}
+
+int32_t ntlp_nbox(const ntlp_ctx *c) { return c ? c->nbox : 0; }
+
+int64_t ntlp_bytes_required(int32_t nbox, const ntlp_grid *grids, const ntlp_params *params,
+                            const int64_t *capacities) {
+    if (nbox < 1 || !grids || !params || !capacities) return -1;
+    const bool mixed = params->precision == NTLP_PREC_MIXED;
+    size_t total = 0;
+    for (int b = 0; b < nbox; ++b) {
+        if (check_grid(nullptr, &grids[b]) || capacities[b] < 1 || capacities[b] > 0x7fffffffLL) return -1;
+        BoxHost h;
+        h.cap = capacities[b];
+        DevBox B{};
+        box_geometry(grids[b], h.cap, B);
+        Carver cv;
+        carve_box(cv, h, B, mixed);
+        total += cv.off;
+        // tile tables of this box (all variants), descriptors
+        const DevGrid &g = B.g;
+        size_t tiles = 0;
+        for (int v = 0; v < kNtVariants; ++v) tiles += (size_t)(h.cap + kNtValues[v] - 1) / kNtValues[v];
+        tiles += 2 * (size_t)((g.ncells + 2 + kScanTile - 1) / kScanTile);
+        for (int v = 0; v < kDepVariants; ++v) tiles += (size_t)deposit_tile_count(v, g.nnx, g.nny, g.nnz);
+        total += tiles * sizeof(Tile) + sizeof(DevBox) + 64;
+    }
+    return (int64_t)(total + 16 * 256 + sizeof(DevParams));
 }
 
 const char *ntlp_last_error(const ntlp_ctx *c) { return c ? c->err.c_str() : "null context"; }
 
 int64_t ntlp_device_bytes(const ntlp_ctx *c) { return c ? c->bytes : 0; }
 
-int64_t ntlp_numpart(const ntlp_ctx *cc) {
-    ntlp_ctx *c = const_cast<ntlp_ctx *>(cc);
-    if (!c || !c->have_droplets) return 0;
+int64_t ntlp_box_numpart(ntlp_ctx *c, int32_t b) {
+    if (!box_ok(c, b) || !c->bh[b].have_droplets) return 0;
     int n = 0;
-    if (read_n_alive(c, &n)) return -1;
+    if (read_n_alive(c, b, &n)) return -1;
     return n;
 }
+
+int64_t ntlp_numpart(const ntlp_ctx *cc) { return ntlp_box_numpart(const_cast<ntlp_ctx *>(cc), 0); }
 
 int ntlp_sync(ntlp_ctx *c) {
     if (!c) return NTLP_ERR_ARG;
@@ -421,6 +884,13 @@ int ntlp_sync(ntlp_ctx *c) {
 }
 
 void *ntlp_stream(ntlp_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+int ntlp_use_stream(ntlp_ctx *c, void *stream) {
+    if (!c) return NTLP_ERR_ARG;
+    CK(cudaStreamSynchronize(c->stream));
+    c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+    return NTLP_OK;
+}
 
 int ntlp_profile_enable(ntlp_ctx *c, int enable) {
     if (!c) return NTLP_ERR_ARG;
@@ -447,231 +917,40 @@ int ntlp_profile_read(ntlp_ctx *c, double ms[4], int64_t *launches) {
 
 int ntlp_fields_upload_ext(ntlp_ctx *c, const double *uext, const double *vext, const double *wext,
                            const double *Text, const double *T2ext) {
+    return ntlp_box_fields_upload_ext(c, 0, uext, vext, wext, Text, T2ext);
+}
+
+int ntlp_box_fields_upload_ext(ntlp_ctx *c, int32_t box, const double *uext, const double *vext, const double *wext,
+                               const double *Text, const double *T2ext) {
     if (!c) return NTLP_ERR_ARG;
     const double *h[5] = {uext, vext, wext, Text, T2ext};
-    for (int k = 0; k < 5; ++k)
-        if (!h[k]) return fail(c, NTLP_ERR_ARG, "field %d is NULL", k);
-    const DevGrid &g = c->box.g;
-    const size_t npad = (size_t)g.nz2 * g.ny5 * g.nx5;
-    for (int k = 0; k < 5; ++k)
-        CK(cudaMemcpyAsync((void *)c->box.f[k], h[k], npad * 8, cudaMemcpyHostToDevice, c->stream));
-    if (c->box.f4) launch_pack_f32(&c->box, (float4 *)c->box.f4, (float *)c->box.fw, c->stream);
-    CK(cudaGetLastError());
-    c->have_fields = true;
-    return NTLP_OK;
+    return fields_ext(c, box, h);
 }
 
 int ntlp_fields_upload(ntlp_ctx *c, const double *u, const double *v, const double *w, const double *t,
                        const double *q) {
+    return ntlp_box_fields_upload(c, 0, u, v, w, t, q);
+}
+
+int ntlp_box_fields_upload(ntlp_ctx *c, int32_t box, const double *u, const double *v, const double *w,
+                           const double *t, const double *q) {
     if (!c) return NTLP_ERR_ARG;
     const double *h[5] = {u, v, w, t, q};
-    for (int k = 0; k < 5; ++k)
-        if (!h[k]) return fail(c, NTLP_ERR_ARG, "field %d is NULL", k);
-    const DevGrid &g = c->box.g;
-    const size_t nflow = (size_t)g.nnx * g.nny * g.nz2;
-    for (int k = 0; k < 5; ++k) {
-        CK(cudaMemcpyAsync(c->staging_d, h[k], nflow * 8, cudaMemcpyHostToDevice, c->stream));
-        launch_fill_ext(c->staging_d, (double *)c->box.f[k], g, c->stream);
-    }
-    if (c->box.f4) launch_pack_f32(&c->box, (float4 *)c->box.f4, (float *)c->box.fw, c->stream);
-    CK(cudaGetLastError());
-    c->have_fields = true;
-    return NTLP_OK;
+    return fields_flow(c, box, h);
 }
 
-int ntlp_droplets_upload(ntlp_ctx *c, const ntlp_droplets *d) {
-    if (!c || !d) return NTLP_ERR_ARG;
-    if (d->n < 0 || d->n > c->cap) return fail(c, NTLP_ERR_CAPACITY, "%lld droplets exceed capacity %lld",
-                                              (long long)d->n, (long long)c->cap);
-    if (!d->xp[0] || !d->xp[1] || !d->xp[2] || !d->vp[0] || !d->vp[1] || !d->vp[2] || !d->Tp || !d->radius ||
-        !d->m_s || !d->kappa_s || !d->mult)
-        return fail(c, NTLP_ERR_ARG, "xp, vp, Tp, radius, m_s, kappa_s and mult are required");
-    const int n = (int)d->n;
-    CK(cudaStreamSynchronize(c->stream));
-    // the uploaded state goes into st[1-cur] in list order; the initial sort
-    // and the finish kernel then make it current
-    if (pull_box(c)) return NTLP_ERR_CUDA;
-    const DevState &O = c->box.st[1 - c->box.cur];
-    auto up = [&](double *dst, const double *src, double fill) -> int {
-        if (src) {
-            CK(cudaMemcpyAsync(dst, src, (size_t)n * 8, cudaMemcpyHostToDevice, c->stream));
-        } else if (fill == 0.0) {
-            CK(cudaMemsetAsync(dst, 0, (size_t)n * 8, c->stream));
-        }
-        return NTLP_OK;
-    };
-    int rc = 0;
-    for (int a = 0; a < 3 && !rc; ++a) {
-        rc |= up(O.x[a], d->xp[a], 0.0);
-        rc |= up(O.v[a], d->vp[a], 0.0);
-        rc |= up(O.uf[a], d->uf[a], 0.0);
-        rc |= up(O.vold[a], d->vp_old[a], 0.0);
-    }
-    rc |= up(O.Tp, d->Tp, 0.0);
-    rc |= up(O.r, d->radius, 0.0);
-    rc |= up(O.m_s, d->m_s, 0.0);
-    rc |= up(O.kap, d->kappa_s, 0.0);
-    rc |= up(O.rc, d->rc, 0.0);
-    rc |= up(O.res, d->res, 0.0);
-    rc |= up(O.actres, d->actres, 0.0);
-    rc |= up(O.numact, d->numact, 0.0);
-    rc |= up(O.Tf, d->Tf, 0.0);
-    rc |= up(O.qinf, d->qinf, 0.0);
-    rc |= up(O.qstar, d->qstar, 0.0);
-    rc |= up(O.Tpold, d->Tp_old, 0.0);
-    rc |= up(O.rold, d->radius_old, 0.0);
-    if (rc) return rc;
-    CK(cudaMemcpyAsync(O.mult, d->mult, (size_t)n * 8, cudaMemcpyHostToDevice, c->stream));
-    k_iota<<<(n + 255) / 256 + 1, 256, 0, c->stream>>>(O.lid, n);
-    bool rk3_given = d->xrhs[0] || d->vrhs[0] || d->Tprhs_s || d->Tprhs_L || d->radrhs;
-    if (rk3_given || c->have_rk3) {
-        if (!c->have_rk3) {
-            CK(cudaStreamSynchronize(c->stream));
-            for (int b = 0; b < 2; ++b) {
-                DevState &s = c->box.st[b];
-                for (int a = 0; a < 3; ++a) { DA(s.xrhs[a], c->cap); DA(s.vrhs[a], c->cap); }
-                DA(s.Tprhs_s, c->cap); DA(s.Tprhs_L, c->cap); DA(s.radrhs, c->cap);
-            }
-            c->have_rk3 = true;
-        }
-        const DevState &R = c->box.st[1 - c->box.cur];
-        for (int a = 0; a < 3; ++a) {
-            if (up(R.xrhs[a], d->xrhs[a], 0.0) || up(R.vrhs[a], d->vrhs[a], 0.0)) return NTLP_ERR_CUDA;
-        }
-        if (up(R.Tprhs_s, d->Tprhs_s, 0.0) || up(R.Tprhs_L, d->Tprhs_L, 0.0) || up(R.radrhs, d->radrhs, 0.0))
-            return NTLP_ERR_CUDA;
-    }
-    CK(cudaMemcpyAsync(c->box.n_alive, &n, sizeof(int), cudaMemcpyHostToDevice, c->stream));
-    if (push_box(c)) return NTLP_ERR_CUDA;
-    launch_keys_initial(c->box_d, c->drop_tiles_d, (int)c->drop_tiles.size(), c->stream);
-    launch_sort(c->box_d, c->plan, c->stream);
-    launch_finish(c->box_d, 1, c->stream);
-    CK(cudaGetLastError());
-    if (pull_box(c)) return NTLP_ERR_CUDA;
-    c->n_uploaded = n;
-    c->have_droplets = true;
-    c->payload_valid = false;
-    return NTLP_OK;
-}
+int ntlp_droplets_upload(ntlp_ctx *c, const ntlp_droplets *d) { return ntlp_box_droplets_upload(c, 0, d); }
 
-int ntlp_droplets_download(ntlp_ctx *c, ntlp_droplets *d) {
-    if (!c || !d) return NTLP_ERR_ARG;
-    if (!c->have_droplets) return fail(c, NTLP_ERR_STATE, "no droplets uploaded");
-    if (pull_box(c)) return NTLP_ERR_CUDA;
-    int n = 0;
-    if (read_n_alive(c, &n)) return NTLP_ERR_CUDA;
-    d->n = n;
-    if (n == 0) return NTLP_OK;
-    const DevState &S = c->box.st[c->box.cur];
-    launch_rank_alive(c->box_d, 0, c->rank_d, c->n_uploaded, c->stream);
-    const int blocks = (n + 255) / 256;
-    auto get = [&](const double *src, double *host) -> int {
-        if (!host || !src) return NTLP_OK;
-        k_gather_d<<<blocks, 256, 0, c->stream>>>(src, c->box.perm, S.lid, c->rank_d, c->staging_d, n);
-        CK(cudaMemcpyAsync(host, c->staging_d, (size_t)n * 8, cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaStreamSynchronize(c->stream));
-        return NTLP_OK;
-    };
-    int rc = 0;
-    for (int a = 0; a < 3 && !rc; ++a) {
-        rc |= get(S.x[a], d->xp[a]);
-        rc |= get(S.v[a], d->vp[a]);
-        rc |= get(S.uf[a], d->uf[a]);
-        rc |= get(S.vold[a], d->vp_old[a]);
-        if (c->have_rk3) {
-            rc |= get(S.xrhs[a], d->xrhs[a]);
-            rc |= get(S.vrhs[a], d->vrhs[a]);
-        }
-    }
-    rc |= get(S.Tp, d->Tp);
-    rc |= get(S.r, d->radius);
-    rc |= get(S.m_s, d->m_s);
-    rc |= get(S.kap, d->kappa_s);
-    rc |= get(S.rc, d->rc);
-    rc |= get(S.res, d->res);
-    rc |= get(S.actres, d->actres);
-    rc |= get(S.numact, d->numact);
-    rc |= get(S.Tf, d->Tf);
-    rc |= get(S.qinf, d->qinf);
-    rc |= get(S.qstar, d->qstar);
-    rc |= get(S.Tpold, d->Tp_old);
-    rc |= get(S.rold, d->radius_old);
-    if (c->have_rk3) {
-        rc |= get(S.Tprhs_s, d->Tprhs_s);
-        rc |= get(S.Tprhs_L, d->Tprhs_L);
-        rc |= get(S.radrhs, d->radrhs);
-    }
-    if (rc) return rc;
-    if (d->mult) {
-        k_gather_i64<<<blocks, 256, 0, c->stream>>>(S.mult, c->box.perm, S.lid, c->rank_d,
-                                                    (long long *)c->staging_d, n);
-        CK(cudaMemcpyAsync(d->mult, c->staging_d, (size_t)n * 8, cudaMemcpyDeviceToHost, c->stream));
-    }
-    if (d->lid) {
-        k_gather_lid<<<blocks, 256, 0, c->stream>>>(c->box.perm, S.lid, c->rank_d, (int *)c->staging_d, n);
-        CK(cudaMemcpyAsync(d->lid, c->staging_d, (size_t)n * 4, cudaMemcpyDeviceToHost, c->stream));
-    }
-    CK(cudaStreamSynchronize(c->stream));
-    CK(cudaGetLastError());
-    return NTLP_OK;
-}
-
-static int finish_counters(ntlp_ctx *c, ntlp_counters *out) {
-    if (!out) return NTLP_OK;
-    CK(cudaMemcpyAsync(c->counters_h, c->box.counters, sizeof(long long) * kNumCounters, cudaMemcpyDeviceToHost,
-                       c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    out->numpart = c->counters_h[C_NUMPART];
-    out->num_destroy = c->counters_h[C_DESTROY];
-    out->denum = c->counters_h[C_DENUM];
-    out->actnum = c->counters_h[C_ACTNUM];
-    out->num100 = c->counters_h[C_NUM100];
-    out->numimpos = c->counters_h[C_NUMIMPOS];
-    out->neg_qinf = c->counters_h[C_NEGQ];
-    out->bad_index = c->counters_h[C_BAD];
-    return NTLP_OK;
-}
-
-static int do_step(ntlp_ctx *c, int kind, int istage, double dt, int32_t it, ntlp_counters *counters) {
+int ntlp_box_droplets_upload(ntlp_ctx *c, int32_t box, const ntlp_droplets *d) {
     if (!c) return NTLP_ERR_ARG;
-    if (!c->have_fields) return fail(c, NTLP_ERR_STATE, "fields not uploaded");
-    if (!c->have_droplets) return fail(c, NTLP_ERR_STATE, "droplets not uploaded");
-    if (!(dt > 0.0)) return fail(c, NTLP_ERR_ARG, "dt must be positive");
-    const int ntiles = (int)c->drop_tiles.size();
-    StepIn in;
-    in.dt = dt;
-    in.it = it;
-    in.istage = istage;
-    in.write_payload = (kind == 1 || istage == 3) ? 1 : 0;
-    cudaEvent_t e0 = phase_begin(c);
-    launch_reset_step(c->box_d, 1, c->stream);
-    phase_end(c, PH_OTHER, e0);
-    e0 = phase_begin(c);
-    if (kind == 1) {
-        if (c->params.precision == NTLP_PREC_MIXED)
-            launch_update_be_mixed(c->params.ilin, c->box_d, c->drop_tiles_d, ntiles, 1, c->dp_d, in, c->stream);
-        else
-            launch_update_be64(c->params.ilin, c->box_d, c->drop_tiles_d, ntiles, 1, c->dp_d, in, c->stream);
-        c->launches += kUpdateLaunches - 1;
-    } else {
-        launch_update_rk3_64(c->params.ilin, c->box_d, c->drop_tiles_d, ntiles, c->dp_d, in, c->stream);
-    }
-    phase_end(c, PH_UPDATE, e0);
-    e0 = phase_begin(c);
-    launch_sort(c->box_d, c->plan, c->stream);
-    launch_finish(c->box_d, 1, c->stream);
-    phase_end(c, PH_SORT, e0);
-    c->launches += 1 + 1 + kSortLaunches + 1;
-    CK(cudaGetLastError());
-    c->box.cur = 1 - c->box.cur;
-    std::swap(c->box.perm, c->box.sorted);
-    if (in.write_payload) {
-        c->payload_valid = true;
-        c->last_dt = dt;
-    } else {
-        c->payload_valid = false;
-    }
-    return finish_counters(c, counters);
+    return droplets_upload(c, box, d);
+}
+
+int ntlp_droplets_download(ntlp_ctx *c, ntlp_droplets *d) { return ntlp_box_droplets_download(c, 0, d); }
+
+int ntlp_box_droplets_download(ntlp_ctx *c, int32_t box, ntlp_droplets *d) {
+    if (!c) return NTLP_ERR_ARG;
+    return droplets_download(c, box, d);
 }
 
 int ntlp_step_be(ntlp_ctx *c, double dt, int32_t it, ntlp_counters *counters) {
@@ -683,79 +962,75 @@ int ntlp_step_rk3(ntlp_ctx *c, int32_t istage, double dt, int32_t it, ntlp_count
     if (istage < 1 || istage > 3) return fail(c, NTLP_ERR_ARG, "istage must be 1, 2 or 3");
     if (c->params.precision != NTLP_PREC_FP64)
         return fail(c, NTLP_ERR_ARG, "the RK3 path is FP64 only (create the context with NTLP_PREC_FP64)");
-    if (!c->have_rk3) {
-        CK(cudaStreamSynchronize(c->stream));
-        for (int b = 0; b < 2; ++b) {
-            DevState &s = c->box.st[b];
-            for (int a = 0; a < 3; ++a) { DA(s.xrhs[a], c->cap); DA(s.vrhs[a], c->cap); }
-            DA(s.Tprhs_s, c->cap); DA(s.Tprhs_L, c->cap); DA(s.radrhs, c->cap);
-            for (int a = 0; a < 3; ++a) {
-                CK(cudaMemset(s.xrhs[a], 0, c->cap * 8));
-                CK(cudaMemset(s.vrhs[a], 0, c->cap * 8));
-            }
-            CK(cudaMemset(s.Tprhs_s, 0, c->cap * 8));
-            CK(cudaMemset(s.Tprhs_L, 0, c->cap * 8));
-            CK(cudaMemset(s.radrhs, 0, c->cap * 8));
-        }
-        c->have_rk3 = true;
-        if (push_box(c)) return NTLP_ERR_CUDA;
-    }
     return do_step(c, 2, istage, dt, it, counters);
+}
+
+int ntlp_box_counters(ntlp_ctx *c, int32_t box, ntlp_counters *out) {
+    if (!box_ok(c, box) || !out) return NTLP_ERR_ARG;
+    int rc = read_counters(c);
+    if (rc) return rc;
+    counters_of(c->counters_h + (size_t)box * kNumCounters, out);
+    return NTLP_OK;
 }
 
 int ntlp_coupling(ntlp_ctx *c, double dt, int32_t layout, double *partsrc, double *partTsrc, double *partHsrc,
                   double *partTEsrc) {
     if (!c) return NTLP_ERR_ARG;
-    if (!c->have_droplets) return fail(c, NTLP_ERR_STATE, "droplets not uploaded");
+    bool any = false;
+    for (auto &h : c->bh) any = any || h.have_droplets;
+    if (!any) return fail(c, NTLP_ERR_STATE, "droplets not uploaded");
     if (layout != NTLP_LAYOUT_COLUMN && layout != NTLP_LAYOUT_FLOW)
         return fail(c, NTLP_ERR_ARG, "unknown layout %d", layout);
     if (!(dt > 0.0)) return fail(c, NTLP_ERR_ARG, "dt must be positive");
     if (!c->payload_valid || c->last_dt != dt) {
         cudaEvent_t ep = phase_begin(c);
         if (c->params.precision == NTLP_PREC_MIXED)
-            launch_payload_mixed(c->box_d, c->drop_tiles_d, (int)c->drop_tiles.size(), c->dp_d, dt, c->stream);
+            launch_payload_mixed(c->box_d, c->drop_tiles_d[0], c->n_drop_tiles[0], c->dp_d, dt, c->stream);
         else
-            launch_payload64(c->box_d, c->drop_tiles_d, (int)c->drop_tiles.size(), c->dp_d, dt, c->stream);
+            launch_payload64(c->box_d, c->drop_tiles_d[0], c->n_drop_tiles[0], c->dp_d, dt, c->stream);
         phase_end(c, PH_OTHER, ep);
         c->launches += 1;
         c->payload_valid = true;
         c->last_dt = dt;
     }
     cudaEvent_t e0 = phase_begin(c);
+    const int v = c->dep_variant;
     if (c->params.precision == NTLP_PREC_MIXED)
-        launch_deposit_mixed(c->box_d, c->node_tiles_d, (int)c->node_tiles.size(), c->dp_d, c->stream);
+        launch_deposit_mixed(v, c->box_d, c->dep_tiles_d[v], c->n_dep_tiles[v], c->dp_d, c->stream);
     else
-        launch_deposit64(c->box_d, c->node_tiles_d, (int)c->node_tiles.size(), c->dp_d, c->stream);
+        launch_deposit64(v, c->box_d, c->dep_tiles_d[v], c->n_dep_tiles[v], c->dp_d, c->stream);
     phase_end(c, PH_DEPOSIT, e0);
     c->launches += 1;
     CK(cudaGetLastError());
-    const DevGrid &g = c->box.g;
-    const size_t nn = (size_t)g.nnodes;
-    double *host[6] = {partsrc, partsrc ? partsrc + nn : nullptr, partsrc ? partsrc + 2 * nn : nullptr,
-                       partTsrc, partHsrc, partTEsrc};
-    for (int q = 0; q < 6; ++q) {
-        if (!host[q]) continue;
-        const double *src = c->box.src[q];
-        if (layout == NTLP_LAYOUT_FLOW) {
-            dim3 grid((g.nnx + 31) / 32, (g.nz2 + 31) / 32, g.nny);
-            k_col_to_flow<<<grid, dim3(32, 8), 0, c->stream>>>(src, c->staging_d, g.nnx, g.nny, g.nz2);
-            c->launches += 1;
-            src = c->staging_d;
-        }
-        CK(cudaMemcpyAsync(host[q], src, nn * 8, cudaMemcpyDeviceToHost, c->stream));
-        if (layout == NTLP_LAYOUT_FLOW) CK(cudaStreamSynchronize(c->stream));
+    double *host[6] = {partsrc, nullptr, nullptr, partTsrc, partHsrc, partTEsrc};
+    if (partsrc) {
+        const size_t nn = (size_t)c->box[0].g.nnodes;
+        host[1] = partsrc + nn;
+        host[2] = partsrc + 2 * nn;
     }
-    CK(cudaStreamSynchronize(c->stream));
-    CK(cudaGetLastError());
-    return NTLP_OK;
+    return sources_out(c, 0, layout, host);
+}
+
+int ntlp_box_sources(ntlp_ctx *c, int32_t box, int32_t layout, double *partsrc, double *partTsrc,
+                     double *partHsrc, double *partTEsrc) {
+    if (!box_ok(c, box)) return NTLP_ERR_ARG;
+    if (layout != NTLP_LAYOUT_COLUMN && layout != NTLP_LAYOUT_FLOW)
+        return fail(c, NTLP_ERR_ARG, "unknown layout %d", layout);
+    double *host[6] = {partsrc, nullptr, nullptr, partTsrc, partHsrc, partTEsrc};
+    if (partsrc) {
+        const size_t nn = (size_t)c->box[box].g.nnodes;
+        host[1] = partsrc + nn;
+        host[2] = partsrc + 2 * nn;
+    }
+    return sources_out(c, box, layout, host);
 }
 
 int ntlp_flux(ntlp_ctx *c, double *pflux, double *pmassflux, double *penegflux) {
     if (!c) return NTLP_ERR_ARG;
-    const int nz1 = c->box.g.nnz + 1;
+    const int nz1 = c->box[0].g.nnz + 1;
     std::vector<long long> fx((size_t)2 * nz1 * kFluxLimbs);
-    if (pflux) CK(cudaMemcpyAsync(pflux, c->box.pflux, nz1 * 8, cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaMemcpyAsync(fx.data(), c->box.flux_fx, fx.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+    if (pflux) CK(cudaMemcpyAsync(pflux, c->box[0].pflux, nz1 * 8, cudaMemcpyDefault, c->stream));
+    CK(cudaMemcpyAsync(fx.data(), c->box[0].flux_fx, fx.size() * 8, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     double *outs[2] = {pmassflux, penegflux};
     for (int qn = 0; qn < 2; ++qn) {
@@ -770,11 +1045,113 @@ int ntlp_flux(ntlp_ctx *c, double *pflux, double *pmassflux, double *penegflux) 
                 L[k + 1] += carry;
             }
             long double v = 0.0L;
-            for (int k = kFluxLimbs - 1; k >= 0; --k)
-                v += ldexpl((long double)L[k], 32 * k + kFluxLsbExp);
+            for (int k = kFluxLimbs - 1; k >= 0; --k) v += ldexpl((long double)L[k], 32 * k + kFluxLsbExp);
             outs[qn][iz] = (double)v;
         }
     }
+    return NTLP_OK;
+}
+
+int ntlp_advance_graph(ntlp_ctx *c, double dt, int32_t it, int32_t nsteps) {
+    if (!c) return NTLP_ERR_ARG;
+    if (it < 2) return fail(c, NTLP_ERR_ARG, "graph steps need it >= 2 (run the first step eagerly)");
+    if (nsteps < 1 || nsteps > 1000) return fail(c, NTLP_ERR_ARG, "nsteps must be in 1..1000");
+    int rc = check_ready(c, dt);
+    if (rc) return rc;
+    if (!c->gexec || c->g_dt != dt || c->g_nsteps != nsteps || c->g_dep != c->dep_variant ||
+        c->g_nt != c->nt_variant) {
+        if (c->gexec) {
+            cudaGraphExecDestroy(c->gexec);
+            c->gexec = nullptr;
+        }
+        const bool prof = c->prof;
+        c->prof = false;   // no events inside the capture
+        const int64_t launches = c->launches;
+        CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        int lrc = NTLP_OK;
+        for (int s = 0; s < nsteps && !lrc; ++s) lrc = launch_step(c, 1, 0, dt, it, true);
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+        c->prof = prof;
+        c->launches = launches;
+        if (lrc) {
+            if (graph) cudaGraphDestroy(graph);
+            return lrc;
+        }
+        if (e != cudaSuccess) return fail(c, NTLP_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&c->gexec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            c->gexec = nullptr;
+            return fail(c, NTLP_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(e));
+        }
+        c->g_dt = dt;
+        c->g_nsteps = nsteps;
+        c->g_dep = c->dep_variant;
+        c->g_nt = c->nt_variant;
+    }
+    cudaEvent_t e0 = phase_begin(c);
+    CK(cudaGraphLaunch(c->gexec, c->stream));
+    phase_end(c, PH_OTHER, e0);
+    c->launches += (int64_t)nsteps * (1 + kUpdateLaunches + 1 + kSortLaunches + 1);
+    mirror_flip(c, nsteps);
+    c->payload_valid = true;
+    c->last_dt = dt;
+    return NTLP_OK;
+}
+
+int ntlp_autotune(ntlp_ctx *c, double dt, int32_t it, int32_t steps, int32_t choice[2],
+                  double ms[NTLP_TUNE_VARIANTS]) {
+    if (!c) return NTLP_ERR_ARG;
+    int rc = check_ready(c, dt);
+    if (rc) return rc;
+    if (steps < 1) steps = 1;
+    if (it < 2) it = 2;
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    const bool prof = c->prof;
+    c->prof = false;
+    auto time_steps = [&](double *out_ms) -> int {
+        for (int s = 0; s < steps + 1; ++s) {     // one untimed step first
+            if (s == 1) CK(cudaEventRecord(a, c->stream));
+            int lrc = launch_step(c, 1, 0, dt, it++, true);
+            if (lrc) return lrc;
+            mirror_flip(c, 1);
+        }
+        CK(cudaEventRecord(b, c->stream));
+        CK(cudaEventSynchronize(b));
+        float t = 0.f;
+        CK(cudaEventElapsedTime(&t, a, b));
+        *out_ms = t / steps;
+        return NTLP_OK;
+    };
+    double local[NTLP_TUNE_VARIANTS] = {0, 0, 0, 0, 0};
+    int best_dep = 0, best_nt = 0;
+    for (int v = 0; v < kDepVariants && !rc; ++v) {
+        c->dep_variant = v;
+        rc = time_steps(&local[v]);
+        if (!rc && local[v] < local[best_dep]) best_dep = v;
+    }
+    c->dep_variant = best_dep;
+    for (int v = 0; v < kNtVariants && !rc; ++v) {
+        c->nt_variant = v;
+        rc = time_steps(&local[kDepVariants + v]);
+        if (!rc && local[kDepVariants + v] < local[kDepVariants + best_nt]) best_nt = v;
+    }
+    c->nt_variant = best_nt;
+    c->prof = prof;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (rc) return rc;
+    c->payload_valid = true;
+    c->last_dt = dt;
+    if (choice) {
+        choice[0] = best_dep;
+        choice[1] = best_nt;
+    }
+    if (ms)
+        for (int k = 0; k < NTLP_TUNE_VARIANTS; ++k) ms[k] = local[k];
     return NTLP_OK;
 }
 

@@ -29,8 +29,6 @@
 namespace ntlp {
 namespace {
 
-constexpr int kDepTX = 2, kDepTY = 4, kDepTZ = 32;                // 256 nodes per tile
-constexpr int kDepCols = (kDepTX + 1) * (kDepTY + 1);             // cell columns per tile
 constexpr int kDepCap64 = 640;                                    // droplets staged per tile (FP64)
 constexpr int kDepCapMixed = 1024;                                // droplets staged per tile (mixed)
 
@@ -176,14 +174,20 @@ __device__ __forceinline__ void node_global(const DevBox &B, const DevParams &p,
     }
 }
 
-constexpr int kDepCSW = kDepTZ + 2;                                // cell starts per column
-constexpr int kDepSmem64 = kDepCap64 * 4 + 14 * kDepCap64 * 8 + kDepCols * kDepCSW * 4 + kDepCols * 4 + 16;
-constexpr int kDepSmemMixed = kDepCapMixed * 4 + P32_N * kDepCapMixed * 4 + kDepCols * kDepCSW * 4 + kDepCols * 4 + 16;
+// shared memory of a tile shape (TX x TY x TZ nodes)
+__host__ __device__ constexpr int dep_smem_bytes(bool mixed, int TX, int TY, int TZ) {
+    return (mixed ? kDepCapMixed * 4 + P32_N * kDepCapMixed * 4 : kDepCap64 * 4 + 14 * kDepCap64 * 8) +
+           (TX + 1) * (TY + 1) * (TZ + 2) * 4 + (TX + 1) * (TY + 1) * 4 + 16;
+}
 
-// Tiled deposition: tiles enumerate (z fastest) the node tiles of each box.
-template <bool MIXED>
+// Tiled deposition: tiles enumerate (z fastest) the node tiles of each box;
+// tile shapes 2x4x32, 4x4x16 and 2x2x64 nodes are instantiated (autotuned).
+template <bool MIXED, int kDepTX, int kDepTY, int kDepTZ>
 __global__ void __launch_bounds__(kDepositThreads, MIXED ? 3 : 2)
 k_deposit_tiled(DevBox *boxes, const Tile *tiles, const DevParams *pp) {
+    static_assert(kDepTX * kDepTY * kDepTZ == kDepositThreads, "one thread per node of the tile");
+    constexpr int kDepCols = (kDepTX + 1) * (kDepTY + 1);
+    constexpr int kDepCSW = kDepTZ + 2;
     extern __shared__ __align__(16) unsigned char sm[];
     constexpr int CAP = MIXED ? kDepCapMixed : kDepCap64;
     // stage: values first (8-byte aligned), then lid, cell starts, column offsets

@@ -206,8 +206,8 @@ __device__ void interp6_64(const DevBox &B, double x1, double x2, double x3, Int
 // launches: interpolation, droplet body with Gauss-Newton, deferred
 // Levenberg-Marquardt droplets.
 // ---------------------------------------------------------------------------
-template <int ILIN>
-__global__ void __launch_bounds__(kUpdateThreads)
+template <int ILIN, int NT>
+__global__ void __launch_bounds__(NT)
 k_interp64(DevBox *boxes, const Tile *tiles) {
     const Tile tl = tiles[blockIdx.x];
     const DevBox &B = boxes[tl.box];
@@ -228,7 +228,8 @@ k_interp64(DevBox *boxes, const Tile *tiles) {
     B.key[t] = bad;
 }
 
-__global__ void __launch_bounds__(kUpdateThreads, 4)
+template <int NT>
+__global__ void __launch_bounds__(NT, 512 / NT)
 k_be64(DevBox *boxes, const Tile *tiles, const DevParams *pp, StepIn in) {
     const Tile tl = tiles[blockIdx.x];
     const DevBox &B = boxes[tl.box];
@@ -391,14 +392,18 @@ __global__ void k_payload64(DevBox *boxes, const Tile *tiles, const DevParams *p
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
-void launch_update_be64(int ilin, DevBox *boxes, const Tile *tiles, int ntiles, int nbox, const DevParams *pp,
-                        StepIn in, cudaStream_t st) {
+void launch_update_be64(int ilin, int nt, DevBox *boxes, const Tile *tiles, int ntiles, int nbox,
+                        const DevParams *pp, StepIn in, cudaStream_t st) {
     if (ntiles <= 0) return;
-    if (ilin == 1)
-        k_interp64<1><<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles);
-    else
-        k_interp64<0><<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles);
-    k_be64<<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles, pp, in);
+    if (nt == 256) {
+        if (ilin == 1) k_interp64<1, 256><<<ntiles, 256, 0, st>>>(boxes, tiles);
+        else k_interp64<0, 256><<<ntiles, 256, 0, st>>>(boxes, tiles);
+        k_be64<256><<<ntiles, 256, 0, st>>>(boxes, tiles, pp, in);
+    } else {
+        if (ilin == 1) k_interp64<1, 128><<<ntiles, 128, 0, st>>>(boxes, tiles);
+        else k_interp64<0, 128><<<ntiles, 128, 0, st>>>(boxes, tiles);
+        k_be64<128><<<ntiles, 128, 0, st>>>(boxes, tiles, pp, in);
+    }
     k_be_defer64<<<dim3(kDeferBlocks, nbox), kUpdateThreads, 0, st>>>(boxes, pp, in);
 }
 
@@ -417,14 +422,36 @@ void launch_payload64(DevBox *boxes, const Tile *tiles, int ntiles, const DevPar
     k_payload64<<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles, pp, dt);
 }
 
-void launch_deposit64(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp, cudaStream_t st) {
+template <int V>
+static void dep64(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp, cudaStream_t st) {
+    constexpr int TX = kDepShape[V][0], TY = kDepShape[V][1], TZ = kDepShape[V][2];
+    k_deposit_tiled<false, TX, TY, TZ>
+        <<<ntiles, kDepositThreads, dep_smem_bytes(false, TX, TY, TZ), st>>>(boxes, tiles, pp);
+}
+
+template <int V>
+static void dep64_attr() {
+    constexpr int TX = kDepShape[V][0], TY = kDepShape[V][1], TZ = kDepShape[V][2];
+    cudaFuncSetAttribute(k_deposit_tiled<false, TX, TY, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         dep_smem_bytes(false, TX, TY, TZ));
+}
+
+void prepare_kernels64() {
+    static bool done = false;
+    if (done) return;
+    dep64_attr<0>();
+    dep64_attr<1>();
+    dep64_attr<2>();
+    done = true;
+}
+
+void launch_deposit64(int variant, DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp,
+                      cudaStream_t st) {
     if (ntiles <= 0) return;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_deposit_tiled<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (false ? kDepSmemMixed : kDepSmem64));
-        attr = true;
-    }
-    k_deposit_tiled<false><<<ntiles, kDepositThreads, (false ? kDepSmemMixed : kDepSmem64), st>>>(boxes, tiles, pp);
+    prepare_kernels64();
+    if (variant == 1) dep64<1>(boxes, tiles, ntiles, pp, st);
+    else if (variant == 2) dep64<2>(boxes, tiles, ntiles, pp, st);
+    else dep64<0>(boxes, tiles, ntiles, pp, st);
 }
 
 }  // namespace ntlp

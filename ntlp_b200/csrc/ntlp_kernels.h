@@ -14,10 +14,18 @@ constexpr int kScanTile = 2048;       // cells per scan tile
 constexpr int kDeferBlocks = 148;     // blocks of the deferred-droplet pass
 constexpr int kUpdateLaunches = 3;    // interpolation, droplet body, deferred droplets
 
-// Node tiles of the deposition: 2 (x) x 4 (y) x 32 (z) nodes each.
-inline long long deposit_tile_count(int nnx, int nny, int nnz) {
-    return (long long)((nnx + 1) / 2) * ((nny + 3) / 4) * ((nnz + 2 + 31) / 32);
+// Deposition tile shapes (nodes per tile in x, y, z; 256 nodes each),
+// chosen per context by the autotuner.
+constexpr int kDepVariants = 3;
+constexpr int kDepShape[kDepVariants][3] = {{2, 4, 32}, {4, 4, 16}, {2, 2, 64}};
+inline long long deposit_tile_count(int variant, int nnx, int nny, int nnz) {
+    const int *s = kDepShape[variant];
+    return (long long)((nnx + s[0] - 1) / s[0]) * ((nny + s[1] - 1) / s[1]) * ((nnz + 2 + s[2] - 1) / s[2]);
 }
+inline long long deposit_tile_count(int nnx, int nny, int nnz) { return deposit_tile_count(0, nnx, nny, nnz); }
+// Droplets per block of the update kernels (autotuned).
+constexpr int kNtVariants = 2;
+constexpr int kNtValues[kNtVariants] = {128, 256};
 
 struct StepIn {
     double dt;
@@ -27,21 +35,26 @@ struct StepIn {
 };
 
 // FP64, reference operation order (ntlp_fp64.cu)
-void launch_update_be64(int ilin, DevBox *boxes, const Tile *tiles, int ntiles, int nbox, const DevParams *pp,
-                        StepIn in, cudaStream_t st);
+void launch_update_be64(int ilin, int nt, DevBox *boxes, const Tile *tiles, int ntiles, int nbox,
+                        const DevParams *pp, StepIn in, cudaStream_t st);
 void launch_update_rk3_64(int ilin, DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp,
                           StepIn in, cudaStream_t st);
 void launch_payload64(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp, double dt,
                       cudaStream_t st);
-void launch_deposit64(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp, cudaStream_t st);
+void launch_deposit64(int variant, DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp,
+                      cudaStream_t st);
 
 // mixed precision (ntlp_mixed.cu)
-void launch_update_be_mixed(int ilin, DevBox *boxes, const Tile *tiles, int ntiles, int nbox,
+void launch_update_be_mixed(int ilin, int nt, DevBox *boxes, const Tile *tiles, int ntiles, int nbox,
                             const DevParams *pp, StepIn in, cudaStream_t st);
 void launch_payload_mixed(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp, double dt,
                           cudaStream_t st);
-void launch_deposit_mixed(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp,
+void launch_deposit_mixed(int variant, DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp,
                           cudaStream_t st);
+// one-time kernel attributes (dynamic shared memory of the deposition);
+// call outside stream capture
+void prepare_kernels64();
+void prepare_kernels_mixed();
 
 // sort and bookkeeping (ntlp_sort.cu)
 struct SortPlan {

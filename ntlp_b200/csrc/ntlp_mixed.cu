@@ -203,8 +203,8 @@ __device__ void interp_lin_mixed(const DevBox &B, double x1, double x2, double x
     o.qinf = B.f[4][ridx] + (double)q;
 }
 
-template <int ILIN>
-__global__ void __launch_bounds__(kUpdateThreads, 4)
+template <int ILIN, int NT>
+__global__ void __launch_bounds__(NT, 512 / NT)
 k_interp_mixed(DevBox *boxes, const Tile *tiles) {
     const Tile tl = tiles[blockIdx.x];
     const DevBox &B = boxes[tl.box];
@@ -225,7 +225,8 @@ k_interp_mixed(DevBox *boxes, const Tile *tiles) {
     B.key[t] = bad;
 }
 
-__global__ void __launch_bounds__(kUpdateThreads, 4)
+template <int NT>
+__global__ void __launch_bounds__(NT, 512 / NT)
 k_be_mixed(DevBox *boxes, const Tile *tiles, const DevParams *pp, StepIn in) {
     const Tile tl = tiles[blockIdx.x];
     const DevBox &B = boxes[tl.box];
@@ -249,14 +250,18 @@ k_be_defer_mixed(DevBox *boxes, const DevParams *pp, StepIn in) {
     block_add_counters(B, cnt);
 }
 
-void launch_update_be_mixed(int ilin, DevBox *boxes, const Tile *tiles, int ntiles, int nbox,
+void launch_update_be_mixed(int ilin, int nt, DevBox *boxes, const Tile *tiles, int ntiles, int nbox,
                             const DevParams *pp, StepIn in, cudaStream_t st) {
     if (ntiles <= 0) return;
-    if (ilin == 1)
-        k_interp_mixed<1><<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles);
-    else
-        k_interp_mixed<0><<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles);
-    k_be_mixed<<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles, pp, in);
+    if (nt == 256) {
+        if (ilin == 1) k_interp_mixed<1, 256><<<ntiles, 256, 0, st>>>(boxes, tiles);
+        else k_interp_mixed<0, 256><<<ntiles, 256, 0, st>>>(boxes, tiles);
+        k_be_mixed<256><<<ntiles, 256, 0, st>>>(boxes, tiles, pp, in);
+    } else {
+        if (ilin == 1) k_interp_mixed<1, 128><<<ntiles, 128, 0, st>>>(boxes, tiles);
+        else k_interp_mixed<0, 128><<<ntiles, 128, 0, st>>>(boxes, tiles);
+        k_be_mixed<128><<<ntiles, 128, 0, st>>>(boxes, tiles, pp, in);
+    }
     k_be_defer_mixed<<<dim3(kDeferBlocks, nbox), kUpdateThreads, 0, st>>>(boxes, pp, in);
 }
 
@@ -282,14 +287,36 @@ void launch_payload_mixed(DevBox *boxes, const Tile *tiles, int ntiles, const De
     if (ntiles > 0) k_payload_mixed<<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles, pp, dt);
 }
 
-void launch_deposit_mixed(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp, cudaStream_t st) {
+template <int V>
+static void depm(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp, cudaStream_t st) {
+    constexpr int TX = kDepShape[V][0], TY = kDepShape[V][1], TZ = kDepShape[V][2];
+    k_deposit_tiled<true, TX, TY, TZ>
+        <<<ntiles, kDepositThreads, dep_smem_bytes(true, TX, TY, TZ), st>>>(boxes, tiles, pp);
+}
+
+template <int V>
+static void depm_attr() {
+    constexpr int TX = kDepShape[V][0], TY = kDepShape[V][1], TZ = kDepShape[V][2];
+    cudaFuncSetAttribute(k_deposit_tiled<true, TX, TY, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         dep_smem_bytes(true, TX, TY, TZ));
+}
+
+void prepare_kernels_mixed() {
+    static bool done = false;
+    if (done) return;
+    depm_attr<0>();
+    depm_attr<1>();
+    depm_attr<2>();
+    done = true;
+}
+
+void launch_deposit_mixed(int variant, DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp,
+                          cudaStream_t st) {
     if (ntiles <= 0) return;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_deposit_tiled<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (true ? kDepSmemMixed : kDepSmem64));
-        attr = true;
-    }
-    k_deposit_tiled<true><<<ntiles, kDepositThreads, (true ? kDepSmemMixed : kDepSmem64), st>>>(boxes, tiles, pp);
+    prepare_kernels_mixed();
+    if (variant == 1) depm<1>(boxes, tiles, ntiles, pp, st);
+    else if (variant == 2) depm<2>(boxes, tiles, ntiles, pp, st);
+    else depm<0>(boxes, tiles, ntiles, pp, st);
 }
 
 }  // namespace ntlp
