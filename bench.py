@@ -22,6 +22,13 @@ larger than L2, so no explicit flush is needed between steps.
   cpu_baseline  the CPU restatement of the reference step (oracle/) on the
           host cores, on a bounded sample of the same workload
 
+  batch   the batched ensemble: 48 boxes of uneven grid and droplet counts
+          in one context, autotuned, 50 steps as one CUDA-graph launch
+          (mixed and FP64)
+  serving the serving loop: a Poisson stream of per-box step jobs under a
+          150 GB HBM budget with continuous batching; throughput, p50/p99
+          step and job latency, FP64 spot checks
+
 --gpus N runs N independent replicas (weak scaling; the step has no data
 exchange on one domain), timed as the max over ranks.
 --impl reference times the reference's CPU implementation of the path (the
@@ -49,7 +56,7 @@ B_D = {"fp64": 248, "mixed": 224}       # algorithmic bytes per droplet
 # the measured traffic to the bench workload; see
 # profiles/k_update_mixed_1M_droplets_128cube.md
 NCU_BYTES_PER_DROPLET = {"mixed": 400.0}
-METRIC = "droplet-updates/s (mixed precision, 16M droplets, 6th-order BE step + coupling)"
+METRIC = "droplet-updates/s (mixed vs FP64 GPU) at 16M; p50/p99 serving step latency"
 
 
 def parse():
@@ -65,6 +72,17 @@ def parse():
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--skip-batch", action="store_true")
+    ap.add_argument("--skip-serving", action="store_true")
+    ap.add_argument("--batch-boxes", type=int, default=48)
+    ap.add_argument("--batch-steps", type=int, default=50)
+    ap.add_argument("--tune-steps", type=int, default=2)
+    ap.add_argument("--serve-jobs", type=int, default=120)
+    ap.add_argument("--serve-rate", type=float, default=200.0)
+    ap.add_argument("--serve-work-cap", type=float, default=2e7)
+    ap.add_argument("--hbm-budget", type=float, default=150e9)
+    ap.add_argument("--serve-depth", type=int, default=2)
+    ap.add_argument("--serve-priorities", type=int, default=1)
     ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
                     help="run one precision only (profiling)")
     return ap.parse_args()
@@ -249,6 +267,95 @@ def run_e2e(case, args, dist):
     return dict(seconds=dt, n0=n0, n1=n1, h2d=5 * npad * 8, d2h=6 * nsrc * 8)
 
 
+def run_batch(args, precision: str):
+    """Batched ensemble: 48 independent periodic boxes (edges log-uniform
+    32..128, droplets log-uniform 1e4..4e6, radius median 0.5..5 um, mean T
+    285..295 K, dt = 1e-3) in one context; autotuned deposition tile shape
+    and droplet block size; the timed steps are one CUDA-graph launch."""
+    import torch
+    import ntlp_b200
+    from ntlp_b200 import abi, devgen
+    from ntlp_b200 import generator as gen
+    dev = torch.device("cuda", torch.cuda.current_device())
+    specs = devgen.draw_ensemble(args.batch_boxes, seed=3)
+    p = gen.default_params(ilin=args.ilin,
+                           precision=abi.NTLP_PREC_MIXED if precision == "mixed" else abi.NTLP_PREC_FP64)
+    grids = [gen.make_grid(sp["edge"], sp["edge"], sp["edge"], 2.0, 2.0, 2.0, None) for sp in specs]
+    caps = [sp["n"] for sp in specs]
+    s = ntlp_b200.DropletBatch(grids, p, caps)
+    for b, sp in enumerate(specs):
+        box = devgen.make_box(sp["edge"], sp["n"], sp["seed"], p, dev, T0=sp["T0"], median=sp["median"])
+        torch.cuda.synchronize()
+        s.box_fill_ext(b, box["flow"], sync=True)
+        s.set_box_droplets(b, box["droplets"])
+        del box
+    torch.cuda.empty_cache()
+    dt = 1e-3
+    s.particle_update_BE(dt, 1, counters=False)
+    s.particle_coupling_update(dt, download=False)
+    tune = s.autotune(dt, 2, steps=args.tune_steps)
+    it = 2 + 5 * (args.tune_steps + 1)
+    s.advance_graph(dt, it, args.batch_steps)          # records the graph; also a warm-up
+    it += args.batch_steps
+    s.sync()
+    n0 = sum(s.box_numpart(b) for b in range(len(specs)))
+    stream = torch.cuda.ExternalStream(s.stream_handle)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    clk = ClockSampler()
+    clk.start()
+    e0.record(stream)
+    s.advance_graph(dt, it, args.batch_steps)
+    e1.record(stream)
+    e1.synchronize()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1)
+    n1 = sum(s.box_numpart(b) for b in range(len(specs)))
+    s.close()
+    upd = 0.5 * (n0 + n1) * args.batch_steps
+    return {"value": upd / (ms * 1e-3), "unit": "droplet-updates/s", "ms_per_step": ms / args.batch_steps,
+            "boxes": len(specs), "droplets": int(n0), "steps": args.batch_steps,
+            "edges": [sp["edge"] for sp in specs], "graph_launches_timed": 1,
+            "autotune": {"deposit_shape": ["2x4x32", "4x4x16", "2x2x64"][tune["deposit_variant"]],
+                         "block": [128, 256][tune["block_variant"]],
+                         "ms_per_step": [round(v, 4) for v in tune["ms"]]},
+            "clocks": clocks}
+
+
+def run_serving(args):
+    """Serving loop: Poisson job stream (edges 32..192, droplets 1e4..1e7,
+    radius median 1..10 um, 1..20 steps per job) under a 150 GB HBM budget,
+    mixed precision with an FP64 spot check on 1% of jobs."""
+    import torch
+    from ntlp_b200 import serving
+    eng = serving.CudaEngine(dt=1e-3, priorities=bool(args.serve_priorities))
+    calib = eng.calibrate()
+    jobs = serving.draw_jobs(args.serve_jobs, rate=args.serve_rate, seed=4)
+    eng.stage(jobs)
+    server = serving.Server(eng, hbm_budget=args.hbm_budget, max_active_droplets=args.serve_work_cap,
+                            depth=args.serve_depth)
+    clk = ClockSampler()
+    clk.start()
+    rep = server.run(jobs, realtime=True, time_limit=600)
+    clocks = clk.stop()
+    torch.cuda.empty_cache()
+    spots = [r["result"]["spot_check"] for r in rep["records"] if "spot_check" in r["result"]]
+    offered = sum(j.n * j.steps for j in jobs) / max(jobs[-1].arrival, 1e-9)
+    return {"jobs": rep["jobs"], "rejected": len(rep["rejected"]), "arrival_rate_jobs_per_s": args.serve_rate,
+            "offered_droplet_updates_per_s": offered,
+            "throughput": rep["throughput"], "unit": "droplet-updates/s", "jobs_per_s": rep["jobs_per_s"],
+            "wall_s": rep["wall_s"],
+            "step_ms_p50": rep["step_ms_p50"], "step_ms_p99": rep["step_ms_p99"],
+            "job_ms_p50": rep["job_ms_p50"], "job_ms_p99": rep["job_ms_p99"],
+            "admission_wait_ms_p50": rep["wait_ms_p50"], "admission_wait_ms_p99": rep["wait_ms_p99"],
+            "ingest_ms_p50": rep["ingest_ms_p50"], "ingest_ms_p99": rep["ingest_ms_p99"],
+            "step_slowdown_p50": rep["step_slowdown_p50"], "step_slowdown_p99": rep["step_slowdown_p99"],
+            "peak_admitted_bytes": rep["peak_bytes"], "hbm_budget": args.hbm_budget,
+            "peak_active_jobs": rep["peak_active"], "work_cap_droplets": args.serve_work_cap,
+            "alone_step_calibration_ms": [[e, n, round(t, 4)] for e, n, t in calib],
+            "spot_checks": spots, "clocks": clocks}
+
+
 def cpu_baseline(case, seconds: float, dist=None):
     """The oracle (CPU restatement of the reference step) on the host cores.
 
@@ -343,6 +450,12 @@ def main():
             continue
         res[prec] = run_device(case, prec, args, dist, rank)
     e2e = None if args.skip_e2e else run_e2e(case, args, dist)
+    batch, serve = {}, None
+    if ws == 1 and not args.skip_batch:
+        for prec in ("mixed", "fp64"):
+            batch[prec] = run_batch(args, prec)
+    if ws == 1 and not args.skip_serving:
+        serve = run_serving(args)
     cb = None
     if rank == 0 and ws == 1 and not args.skip_cpu:
         cb = cpu_baseline(case, args.cpu_seconds)
@@ -400,6 +513,12 @@ def main():
                        "note": "fields uploaded from pinned host memory and sources downloaded every step"}
     if cb:
         line["cpu_baseline"] = cb
+    if batch:
+        line["batch"] = batch
+        if "fp64" in batch:
+            batch["mixed_over_fp64"] = batch["mixed"]["value"] / batch["fp64"]["value"]
+    if serve:
+        line["serving"] = serve
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()

@@ -1,0 +1,410 @@
+"""Serving loop: per-box step jobs with continuous batching on one GPU.
+
+No counterpart in the reference (one LES run steps one domain).  A job is
+one periodic box (its grid, fields and droplets) and a number of
+particle_update_BE + particle_coupling_update steps.  Jobs arrive as a
+Poisson stream; the server
+
+* admits them in arrival order while the device bytes of the admitted
+  contexts (``ntlp_bytes_required``, exact) stay within an HBM budget and
+  the droplets in flight stay within a work cap, so that requests arriving
+  while others run join as memory and slots free up;
+* builds each admitted job's box on the device on an ingest thread and
+  keeps its fields and droplets resident in its own context for all of its
+  steps (no host round trip between steps);
+* keeps up to ``depth`` steps of every active job queued on that job's own
+  CUDA stream, so steps of different jobs overlap on the device; smaller
+  jobs get higher stream priority, so their short steps are not queued
+  behind the long ones of large jobs;
+* times every step on the device (events on the job's stream around the
+  step) and every job from arrival to completion on the host clock.
+
+An FP64 twin of a spot-check job (1% of jobs) runs beside it on the same
+inputs and the two final droplet states are compared.
+
+The scheduler logic (admission, ordering, accounting) is independent of the
+device: ``Server`` drives any engine with the methods of ``CudaEngine``
+(tests run it with a simulated engine on the CPU).
+"""
+from __future__ import annotations
+
+import math
+import threading
+import time
+from collections import deque
+from concurrent.futures import ThreadPoolExecutor
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import generator as gen
+
+
+@dataclass
+class JobSpec:
+    jid: int
+    arrival: float          # seconds after the start of the stream
+    edge: int               # grid edge (cube of edge^3 cells)
+    n: int                  # droplets
+    median: float           # lognormal radius median (m)
+    steps: int
+    seed: int
+    spot_check: bool = False
+
+
+def draw_jobs(n_jobs: int, rate: float = 200.0, edge=(32, 192), droplets=(1e4, 1e7),
+              median=(1e-6, 10e-6), steps=(1, 20), spot_frac: float = 0.01, seed: int = 0) -> list:
+    """Seeded job stream: exponential inter-arrival times (Poisson process of
+    the given rate, first arrival at 0), grid edge and droplet count
+    log-uniform over their ranges, radius median uniform, steps uniform;
+    round(spot_frac * n_jobs) jobs (at least one) carry the FP64 spot check."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    gaps = rng.exponential(1.0 / rate, n_jobs)
+    arrivals = np.concatenate([[0.0], np.cumsum(gaps[1:])])
+    edges = np.exp(rng.uniform(math.log(edge[0]), math.log(edge[1] + 1), n_jobs)).astype(np.int64)
+    edges = np.clip(edges, edge[0], edge[1])
+    ns = np.exp(rng.uniform(math.log(droplets[0]), math.log(droplets[1]), n_jobs)).round().astype(np.int64)
+    meds = rng.uniform(median[0], median[1], n_jobs)
+    st = rng.integers(steps[0], steps[1] + 1, n_jobs)
+    seeds = rng.integers(1, 2**31 - 1, n_jobs)
+    n_spot = max(1, int(round(spot_frac * n_jobs))) if spot_frac > 0 else 0
+    spot = set(rng.choice(n_jobs, n_spot, replace=False).tolist()) if n_spot else set()
+    return [JobSpec(jid=i, arrival=float(arrivals[i]), edge=int(edges[i]), n=int(ns[i]), median=float(meds[i]),
+                    steps=int(st[i]), seed=int(seeds[i]), spot_check=i in spot) for i in range(n_jobs)]
+
+
+def percentile(v, q) -> float | None:
+    return float(np.percentile(np.asarray(v, dtype=np.float64), q)) if len(v) else None
+
+
+@dataclass
+class _Active:
+    spec: JobSpec
+    state: object                 # engine's job state
+    nbytes: int
+    admitted: float
+    ready: float = 0.0
+    issued: int = 0
+    completed: int = 0
+    events: deque = field(default_factory=deque)
+    step_ms: list = field(default_factory=list)
+
+
+class Server:
+    """Continuous-batching scheduler over an engine (see module docstring)."""
+
+    def __init__(self, engine, hbm_budget: float = 150e9, max_active: int = 64,
+                 max_active_droplets: float = 2e7, depth: int = 2, ingest_workers: int = 3):
+        self.engine = engine
+        self.budget = float(hbm_budget)
+        self.max_active = int(max_active)
+        self.max_drops = float(max_active_droplets)
+        self.depth = int(depth)
+        self.workers = int(ingest_workers)
+
+    def run(self, jobs: list, realtime: bool = True, time_limit: float | None = None) -> dict:
+        eng = self.engine
+        pending = deque(sorted(jobs, key=lambda j: (j.arrival, j.jid)))
+        queue: deque = deque()
+        ingesting: dict = {}
+        active: list = []
+        records: list = []
+        rejected: list = []
+        used_bytes = 0
+        used_drops = 0
+        peak_bytes = 0
+        peak_active = 0
+        admit_order: list = []
+        pool = ThreadPoolExecutor(max_workers=self.workers, thread_name_prefix="ingest")
+        t0 = time.perf_counter()
+        first_arrival = pending[0].arrival if pending else 0.0
+        try:
+            while pending or queue or ingesting or active:
+                now = time.perf_counter() - t0
+                if time_limit is not None and now > time_limit:
+                    raise TimeoutError(f"serving loop exceeded {time_limit} s")
+                progressed = False
+                # arrivals
+                while pending and (not realtime or pending[0].arrival <= now):
+                    queue.append(pending.popleft())
+                    progressed = True
+                # admission in arrival order by memory budget and work cap
+                while queue and len(active) + len(ingesting) < self.max_active:
+                    job = queue[0]
+                    b = eng.job_bytes(job)
+                    fits_mem = used_bytes + b <= self.budget
+                    fits_work = used_drops + job.n <= self.max_drops or (used_drops == 0)
+                    if not (fits_mem and fits_work):
+                        if b > self.budget:
+                            queue.popleft()
+                            rejected.append(job.jid)
+                            continue
+                        break
+                    queue.popleft()
+                    used_bytes += b
+                    used_drops += job.n
+                    peak_bytes = max(peak_bytes, used_bytes)
+                    admit_order.append(job.jid)
+                    fut = pool.submit(eng.prepare, job)
+                    ingesting[fut] = (job, b, time.perf_counter() - t0)
+                    progressed = True
+                # jobs whose boxes are on the device
+                for fut in [f for f in ingesting if f.done()]:
+                    job, b, ta = ingesting.pop(fut)
+                    st = fut.result()          # re-raises ingest errors
+                    active.append(_Active(spec=job, state=st, nbytes=b, admitted=ta,
+                                          ready=time.perf_counter() - t0))
+                    progressed = True
+                peak_active = max(peak_active, len(active))
+                # keep `depth` steps of every active job queued on its stream
+                for a in active:
+                    while len(a.events) < self.depth and a.issued < a.spec.steps:
+                        a.events.append(eng.issue_step(a.state, a.issued))
+                        a.issued += 1
+                        progressed = True
+                # completions
+                still = []
+                for a in active:
+                    while a.events and eng.done(a.events[0]):
+                        a.step_ms.append(eng.step_ms(a.events.popleft()))
+                        a.completed += 1
+                        progressed = True
+                    if a.completed == a.spec.steps:
+                        result = eng.finish(a.state)
+                        t_done = time.perf_counter() - t0
+                        used_bytes -= a.nbytes
+                        used_drops -= a.spec.n
+                        records.append(dict(jid=a.spec.jid, n=a.spec.n, edge=a.spec.edge, steps=a.spec.steps,
+                                            arrival=a.spec.arrival, admitted=a.admitted, ready=a.ready,
+                                            done=t_done, step_ms=a.step_ms, result=result,
+                                            spot_check=a.spec.spot_check))
+                    else:
+                        still.append(a)
+                active = still
+                if not progressed:
+                    time.sleep(0.0002)
+        finally:
+            for a in active:
+                try:
+                    eng.abandon(a.state)
+                except Exception:
+                    pass
+            for fut in ingesting:
+                try:
+                    eng.abandon(fut.result())
+                except Exception:
+                    pass
+            pool.shutdown(wait=True)
+        t_end = time.perf_counter() - t0
+        return self._report(records, rejected, admit_order, first_arrival, t_end, peak_bytes, peak_active)
+
+    def _report(self, records, rejected, admit_order, first_arrival, t_end, peak_bytes, peak_active) -> dict:
+        steps = [ms for r in records for ms in r["step_ms"]]
+        job_ms = [1e3 * (r["done"] - r["arrival"]) for r in records]
+        wait_ms = [1e3 * (r["admitted"] - r["arrival"]) for r in records]
+        ingest_ms = [1e3 * (r["ready"] - r["admitted"]) for r in records]
+        updates = sum(r["n"] * r["steps"] for r in records)
+        span = max(t_end - first_arrival, 1e-9)
+        slow = []
+        model = getattr(self.engine, "alone_ms", None)
+        for r in records:
+            base = model(r["edge"], r["n"]) if model is not None else None
+            if base:
+                slow.extend(ms / base for ms in r["step_ms"])
+        return dict(
+            jobs=len(records), rejected=rejected, admit_order=admit_order,
+            droplet_updates=int(updates), wall_s=span, throughput=updates / span,
+            jobs_per_s=len(records) / span,
+            step_ms_p50=percentile(steps, 50), step_ms_p99=percentile(steps, 99),
+            job_ms_p50=percentile(job_ms, 50), job_ms_p99=percentile(job_ms, 99),
+            wait_ms_p50=percentile(wait_ms, 50), wait_ms_p99=percentile(wait_ms, 99),
+            ingest_ms_p50=percentile(ingest_ms, 50), ingest_ms_p99=percentile(ingest_ms, 99),
+            step_slowdown_p50=percentile(slow, 50), step_slowdown_p99=percentile(slow, 99),
+            peak_bytes=int(peak_bytes), peak_active=int(peak_active),
+            records=records,
+        )
+
+
+class CudaEngine:
+    """Runs jobs on the current CUDA device through the C ABI, one context
+    (one box) per job, mixed precision; spot-check jobs get an FP64 twin."""
+
+    def __init__(self, params: dict | None = None, dt: float = 1e-3, keep_state: bool = False,
+                 priorities: bool = True, spot_keys=("radius", "Tp", "vp", "xp")):
+        import torch
+        import ntlp_b200
+        self.torch = torch
+        self.ntlp = ntlp_b200
+        self.device = torch.device("cuda", torch.cuda.current_device())
+        base = dict(params or gen.default_params())
+        self.p_mixed = dict(base, precision=1)
+        self.p_fp64 = dict(base, precision=0)
+        self.dt = float(dt)
+        self.keep_state = keep_state
+        self.priorities = priorities
+        self.spot_keys = spot_keys
+        lo, hi = torch.cuda.Stream.priority_range()   # (lowest, highest); numerically hi <= lo
+        self._prio = (lo, hi)
+        self._local = threading.local()
+        self._coef = None
+        self._payload: dict = {}
+
+    # -- sizes --
+    def job_bytes(self, job: JobSpec) -> int:
+        grid = gen.make_grid(job.edge, job.edge, job.edge, 2.0, 2.0, 2.0, None)
+        b = self.ntlp.bytes_required([grid], self.p_mixed, [max(job.n, 1)])
+        if job.spot_check:
+            b += self.ntlp.bytes_required([grid], self.p_fp64, [max(job.n, 1)])
+        return b
+
+    def _priority(self, n: int) -> int:
+        lo, hi = self._prio
+        if not self.priorities or lo == hi:
+            return lo
+        if n < 200_000:
+            return hi
+        if n < 2_000_000:
+            return (lo + hi) // 2 if abs(lo - hi) > 1 else hi
+        return lo
+
+    # -- ingest (runs on an ingest thread) --
+    def _ingest_stream(self):
+        s = getattr(self._local, "stream", None)
+        if s is None:
+            self.torch.cuda.set_device(self.device)
+            s = self.torch.cuda.Stream(device=self.device, priority=self._prio[1])
+            self._local.stream = s
+        return s
+
+    def _context(self, box, params, prio):
+        # the upload runs on the ingest thread's high-priority stream, so a
+        # job's set-up is not queued behind the steps of running jobs; its
+        # steps then go to a stream of the job's own priority
+        ist = self._ingest_stream()
+        ctx = self.ntlp.DropletBatch([box["grid"]], params, [max(box["n"], 1)])
+        ctx.use_stream(ist.cuda_stream)
+        ctx.box_fill_ext(0, box["flow"], sync=False)
+        ctx.set_box_droplets(0, box["droplets"])
+        stream = self.torch.cuda.Stream(device=self.device, priority=prio)
+        ctx.use_stream(stream.cuda_stream)      # waits for the upload
+        return ctx, stream
+
+    def _generate(self, job: JobSpec) -> dict:
+        from . import devgen
+        box = devgen.make_box(job.edge, job.n, job.seed, self.p_mixed, self.device, median=job.median,
+                              sigma_g=1.5)
+        box["n"] = job.n
+        return box
+
+    def stage(self, jobs: list):
+        """Build the jobs' input boxes in device memory ahead of the stream
+        (the request payloads), so that a job's ingest is its context set-up
+        and upload only."""
+        for job in jobs:
+            self._payload[job.jid] = self._generate(job)
+        self.torch.cuda.synchronize()
+
+    def prepare(self, job: JobSpec):
+        torch = self.torch
+        box = self._payload.pop(job.jid, None)
+        if box is None:
+            ist = self._ingest_stream()
+            with torch.cuda.stream(ist):
+                box = self._generate(job)
+            ist.synchronize()
+        prio = self._priority(job.n)
+        ctx, stream = self._context(box, self.p_mixed, prio)
+        twin = None
+        if job.spot_check:
+            twin = self._context(box, self.p_fp64, prio)
+        del box
+        return dict(job=job, ctx=ctx, stream=stream, twin=twin)
+
+    # -- steps --
+    def issue_step(self, st: dict, k: int):
+        torch = self.torch
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st["stream"])
+        st["ctx"].particle_update_BE(self.dt, k + 1, counters=False)
+        st["ctx"].particle_coupling_update(self.dt, download=False)
+        e1.record(st["stream"])
+        if st["twin"] is not None:
+            tctx, tstream = st["twin"]
+            tctx.particle_update_BE(self.dt, k + 1, counters=False)
+            tctx.particle_coupling_update(self.dt, download=False)
+            t1 = torch.cuda.Event()
+            t1.record(tstream)
+            return (e0, e1, t1)
+        return (e0, e1, None)
+
+    def done(self, ev) -> bool:
+        return ev[1].query() and (ev[2] is None or ev[2].query())
+
+    def step_ms(self, ev) -> float:
+        return float(ev[0].elapsed_time(ev[1]))
+
+    def finish(self, st: dict) -> dict:
+        ctx = st["ctx"]
+        out = dict(counters=ctx.box_counters(0), numpart=ctx.box_numpart(0))
+        if self.keep_state or st["twin"] is not None:
+            state = ctx.get_box_droplets(0)
+            if self.keep_state:
+                out["state"] = state
+                out["sources"] = ctx.box_sources(0)
+            if st["twin"] is not None:
+                tctx = st["twin"][0]
+                ref = tctx.get_box_droplets(0)
+                err = {}
+                for k in self.spot_keys:
+                    a, b = np.asarray(state[k]), np.asarray(ref[k])
+                    if a.shape != b.shape:
+                        err[k] = math.inf
+                    elif not a.size:
+                        err[k] = 0.0
+                    elif k == "xp":     # position error as a fraction of the 2 m box
+                        err[k] = float(np.max(np.abs(a - b)) / 2.0)
+                    elif k in ("vp", "uf"):   # relative to the velocity scale
+                        err[k] = float(np.max(np.abs(a - b)) / max(float(np.max(np.abs(b))), 1e-300))
+                    else:
+                        err[k] = float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-300)))
+                out["spot_check"] = dict(max_rel=err, numpart_equal=(ctx.box_numpart(0) == tctx.box_numpart(0)),
+                                         counters_equal=(ctx.box_counters(0) == tctx.box_counters(0)))
+                tctx.close()
+        ctx.close()
+        return out
+
+    def abandon(self, st: dict):
+        if st is None:
+            return
+        if st.get("twin") is not None:
+            st["twin"][0].close()
+        st["ctx"].close()
+
+    # -- alone-step model for slowdown figures --
+    def calibrate(self, shapes=((32, 10_000), (64, 100_000), (128, 1_000_000), (192, 10_000_000),
+                                (192, 10_000), (48, 3_000_000)), steps: int = 4) -> list:
+        """Time steps of single jobs running alone and fit
+        ms = a + b * droplets + c * cells (least squares, non-negative)."""
+        rows = []
+        for i, (edge, n) in enumerate(shapes):
+            job = JobSpec(jid=-1 - i, arrival=0.0, edge=edge, n=n, median=3e-6, steps=steps, seed=1000 + i)
+            st = self.prepare(job)
+            ms = []
+            for k in range(steps):
+                ev = self.issue_step(st, k)
+                ev[1].synchronize()
+                ms.append(self.step_ms(ev))
+            self.finish(st)
+            rows.append((edge, n, float(np.median(ms[1:]))))
+        A = np.array([[1.0, n, (e + 1) ** 3] for e, n, _ in rows])
+        y = np.array([t for _, _, t in rows])
+        coef = np.linalg.lstsq(A, y, rcond=None)[0]
+        self._coef = np.maximum(coef, 0.0)
+        return rows
+
+    def alone_ms(self, edge: int, n: int) -> float | None:
+        if self._coef is None:
+            return None
+        a, b, c = self._coef
+        return float(max(a + b * n + c * (edge + 1) ** 3, 1e-3))
