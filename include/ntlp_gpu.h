@@ -218,6 +218,55 @@ int ntlp_advance_graph(ntlp_ctx *ctx, double dt, int32_t it, int32_t nsteps);
 int ntlp_autotune(ntlp_ctx *ctx, double dt, int32_t it, int32_t steps, int32_t choice[2],
                   double ms[NTLP_TUNE_VARIANTS]);
 
+/* ---- statistics and histograms ------------------------------------------
+ * particle_xy_stats (particles.f90:3370-3770; les.F:476 calls it after every
+ * step), radius_histogram (:5011-5021) and the histograms and surface
+ * precipitation map that the step itself accumulates at deactivation
+ * (:3162-3164) and at the bottom-wall kill (:2733-2753).  One box per call
+ * (box 0 of a single-box context).  Sums are fixed-order or exact integer
+ * reductions on the device (deterministic); the reference adds in list
+ * order.                                                                    */
+#define NTLP_HIST_BINS 514            /* histbins + 2 (particles.f90:45)    */
+#define NTLP_STATS_LEVEL_QTYS 24      /* statsvec1 columns (:3608-3633)     */
+typedef struct ntlp_stats0 {
+    int64_t numpart, numdrop, numaerosol;       /* radius > rc: droplet     */
+    /* sums before averaging: Rep, Volp*rhow, Volp*rhop, Volp, radius, radius^2 */
+    double Rep_sum, wmass, pmass, pvol, rad_sum, rad2_sum;
+    double radmax, tempmax, qmax, vpmax[3];     /* from 0, 0, 0, -1000      */
+    double radmin, tempmin, qmin, vpmin[3];     /* from 1000                */
+} ntlp_stats0;
+/* 0th-order statistics, the per-level sums statsvec1(1:maxnz, 1:24)
+ * (column-major, level iz = minloc(z > xp3) - 1 fastest; maxnz >= nnz,
+ * levels above nnz are zero) and LWP(1:nnx, 1:nny) (column-major).  Either
+ * array may be NULL.  The averages, variances and concentrations the
+ * reference derives from these sums after its allreduce are left to the
+ * caller.                                                                   */
+int ntlp_stats(ntlp_ctx *ctx, int32_t box, ntlp_stats0 *s0, int32_t maxnz, double *level_sums, double *lwp);
+/* radius_histogram: hist_rad(1:514), log10(radius) binned over 1e-8..1e-3 m
+ * and weighted by mult.                                                      */
+int ntlp_radius_histogram(ntlp_ctx *ctx, int32_t box, double hist_rad[NTLP_HIST_BINS]);
+/* The histograms the steps have accumulated since the last reset, as
+ * hist[k*514 + bin] for k = 0 hist_actres, 1 hist_res, 2 hist_acttodeath,
+ * 3 hist_numact, 4 hist_raddeath, and surf_precip(1:nnx, 1:nny) (either may
+ * be NULL).  reset != 0 zeroes them afterwards (write_histograms,
+ * netcdf_io.f90:1537-1541).                                                 */
+int ntlp_step_histograms(ntlp_ctx *ctx, int32_t box, double *hist, double *surf_precip, int32_t reset);
+
+/* ---- particle restart file (save_particles / read_part_res) ------------
+ * particles.f90:1988-2146 on one domain: a 4-byte tnumpart, then one
+ * 352-byte record per droplet in the layout of the MPI type particletype
+ * (4 int32, 39 real8, int64 mult, two 8-byte pointers; :1930-1950).  Host
+ * only (no context, no device).  write: the droplets of d in list order
+ * (pidx = lid + 1; fields this library does not keep -- procidx, the
+ * neighbour indices, dist, u_sub, sigm_s -- are written as 0).  read: the
+ * records strictly inside (0, xl) x (0, yl), as read_part_res keeps them,
+ * into d (at most `capacity`; NTLP_ERR_CAPACITY beyond), lid = position;
+ * *n_total receives the file's tnumpart.                                   */
+#define NTLP_CHECKPOINT_RECORD_BYTES 352
+int ntlp_checkpoint_write(const char *path, const ntlp_droplets *d);
+int ntlp_checkpoint_read(const char *path, double xl, double yl, ntlp_droplets *d, int64_t capacity,
+                         int64_t *n_total);
+
 /* ---- droplet creation helper ------------------------------------------- */
 /* Koehler critical radius rc of n droplets (crit_radius with the radval
  * table of setup_radval, particles.f90:5294-5327), computed on the host;

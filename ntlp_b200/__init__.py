@@ -62,6 +62,12 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.ntlp_stream.argtypes = [C.c_void_p]
     L.ntlp_stream.restype = C.c_void_p
     L.ntlp_use_stream.argtypes = [C.c_void_p, C.c_void_p]
+    L.ntlp_stats.argtypes = [C.c_void_p, C.c_int32, P(abi.NtlpStats0), C.c_int32, dp, dp]
+    L.ntlp_radius_histogram.argtypes = [C.c_void_p, C.c_int32, dp]
+    L.ntlp_step_histograms.argtypes = [C.c_void_p, C.c_int32, dp, dp, C.c_int32]
+    L.ntlp_checkpoint_write.argtypes = [C.c_char_p, P(abi.NtlpDroplets)]
+    L.ntlp_checkpoint_read.argtypes = [C.c_char_p, C.c_double, C.c_double, P(abi.NtlpDroplets), C.c_int64,
+                                       P(C.c_int64)]
     L.ntlp_profile_enable.argtypes = [C.c_void_p, C.c_int]
     L.ntlp_profile_read.argtypes = [C.c_void_p, dp, P(C.c_int64)]
     # many boxes in one context
@@ -95,6 +101,33 @@ def crit_radius(params: dict, m_s, kappa_s, T) -> np.ndarray:
     if rc != 0:
         raise NtlpError(f"ntlp_crit_radius failed ({rc})")
     return out
+
+
+def save_particles(path: str, d: dict) -> None:
+    """Write droplets (a host dict in list order) as the reference's particle
+    restart file (save_particles, particles.f90:1988)."""
+    L = load_library()
+    s = abi.make_droplets_struct(d)
+    if L.ntlp_checkpoint_write(os.fsencode(path), C.byref(s)) != 0:
+        raise NtlpError(f"writing {path} failed")
+
+
+def read_part_res(path: str, xl: float, yl: float, capacity: int | None = None) -> dict:
+    """Read a particle restart file (read_part_res, particles.f90:2049): the
+    records strictly inside (0, xl) x (0, yl), as a host droplet dict."""
+    L = load_library()
+    if capacity is None:
+        with open(path, "rb") as f:
+            capacity = max(int(np.frombuffer(f.read(4), dtype=np.int32)[0]), 0)
+    d = abi.empty_droplets(max(capacity, 1))
+    s = abi.make_droplets_struct(d, n=0)
+    total = C.c_int64()
+    rc = L.ntlp_checkpoint_read(os.fsencode(path), float(xl), float(yl), C.byref(s), int(capacity),
+                                C.byref(total))
+    if rc != 0:
+        raise NtlpError(f"reading {path} failed ({rc})")
+    n = int(s.n)
+    return {k: np.ascontiguousarray(v[..., :n] if v.ndim == 2 else v[:n]) for k, v in d.items()}
 
 
 def _field(a):
@@ -254,6 +287,33 @@ class DropletStep:
         self._check(self.L.ntlp_coupling(self.h, float(dt), int(layout), abi.as_dptr(mom.reshape(-1)),
                                          *(abi.as_dptr(a.reshape(-1)) for a in rest)), "ntlp_coupling")
         return [mom[0], mom[1], mom[2], rest[0], rest[1], rest[2]]
+
+    # -- statistics (particle_xy_stats, radius_histogram, step histograms) --
+    def particle_xy_stats(self, box: int = 0, maxnz: int | None = None):
+        """Sums of particle_xy_stats for one box: (stats0 dict, level sums
+        (24, maxnz) = statsvec1 transposed, LWP (nny, nnx))."""
+        g = self.grids[box]
+        maxnz = g["nnz"] if maxnz is None else maxnz
+        s0 = abi.NtlpStats0()
+        levels = np.zeros((abi.NTLP_STATS_LEVEL_QTYS, maxnz))
+        lwp = np.zeros((g["nny"], g["nnx"]))
+        self._check(self.L.ntlp_stats(self.h, int(box), C.byref(s0), int(maxnz), abi.as_dptr(levels),
+                                      abi.as_dptr(lwp)), "ntlp_stats")
+        return s0.as_dict(), levels, lwp
+
+    def radius_histogram(self, box: int = 0) -> np.ndarray:
+        h = np.zeros(abi.NTLP_HIST_BINS)
+        self._check(self.L.ntlp_radius_histogram(self.h, int(box), abi.as_dptr(h)), "ntlp_radius_histogram")
+        return h
+
+    def step_histograms(self, box: int = 0, reset: bool = False):
+        """(hist (5, 514): actres, res, acttodeath, numact, raddeath; surf_precip (nny, nnx))."""
+        g = self.grids[box]
+        h = np.zeros((5, abi.NTLP_HIST_BINS))
+        sp = np.zeros((g["nny"], g["nnx"]))
+        self._check(self.L.ntlp_step_histograms(self.h, int(box), abi.as_dptr(h), abi.as_dptr(sp),
+                                                1 if reset else 0), "ntlp_step_histograms")
+        return h, sp
 
     def flux(self):
         nz1 = self.grid["nnz"] + 1

@@ -78,6 +78,31 @@ class NtlpCounters(C.Structure):
         return {name: int(getattr(self, name)) for name, _ in self._fields_}
 
 
+NTLP_HIST_BINS = 514
+NTLP_STATS_LEVEL_QTYS = 24
+NTLP_CHECKPOINT_RECORD_BYTES = 352
+# names of the statsvec1 columns (particles.f90:3608-3633), in order
+STATS_LEVEL_NAMES = ("partcount", "vp1mean", "vp2mean", "vp3mean", "vp1msqr", "vp2msqr", "vp3msqr", "upwpm",
+                     "uf1mean", "uf2mean", "uf3mean", "uf1msqr", "uf2msqr", "uf3msqr", "Tpmean", "Tpmsqr",
+                     "Tfmean", "radmean", "rad2mean", "qfmean", "wpTpm", "multmean", "mwmean", "qstarm")
+STEP_HIST_NAMES = ("actres", "res", "acttodeath", "numact", "raddeath")
+
+
+class NtlpStats0(C.Structure):
+    _fields_ = [("numpart", C.c_int64), ("numdrop", C.c_int64), ("numaerosol", C.c_int64),
+                ("Rep_sum", C.c_double), ("wmass", C.c_double), ("pmass", C.c_double), ("pvol", C.c_double),
+                ("rad_sum", C.c_double), ("rad2_sum", C.c_double),
+                ("radmax", C.c_double), ("tempmax", C.c_double), ("qmax", C.c_double), ("vpmax", C.c_double * 3),
+                ("radmin", C.c_double), ("tempmin", C.c_double), ("qmin", C.c_double), ("vpmin", C.c_double * 3)]
+
+    def as_dict(self) -> dict:
+        out = {}
+        for name, _ in self._fields_:
+            v = getattr(self, name)
+            out[name] = list(v) if name in ("vpmax", "vpmin") else v
+        return out
+
+
 # Per-droplet double arrays of the structure, in declaration order.
 VEC3_FIELDS = ("xp", "vp", "uf", "xrhs", "vrhs", "vp_old")
 SCALAR_FIELDS = ("Tp", "Tprhs_s", "Tprhs_L", "Tf", "radius", "radrhs", "qinf", "qstar",

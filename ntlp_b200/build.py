@@ -31,8 +31,10 @@ UNITS = {
     "ntlp_sort.cu": [],
     "ntlp_api.cu": [],
     "ntlp_noalloc.cu": [],
+    "ntlp_stats.cu": ["--fmad=false"],
+    "ntlp_checkpoint.cpp": [],
 }
-HEADERS = ["ntlp_math.h", "ntlp_dev.cuh", "ntlp_kernels.h", "ntlp_physics.cuh", "ntlp_deposit.cuh"]
+HEADERS = ["ntlp_math.h", "ntlp_hist.h", "ntlp_dev.cuh", "ntlp_kernels.h", "ntlp_physics.cuh", "ntlp_deposit.cuh"]
 
 
 def nvcc() -> str:
@@ -63,7 +65,7 @@ def build(verbose: bool = False, force: bool = False, ptxas_v: bool = False) -> 
     objs = []
     for unit, extra in UNITS.items():
         src = os.path.join(CSRC, unit)
-        obj = os.path.join(BUILD, unit.replace(".cu", ".o"))
+        obj = os.path.join(BUILD, os.path.splitext(unit)[0] + ".o")
         objs.append(obj)
         if not force and _newer(obj, [src, *hdrs, __file__]):
             continue

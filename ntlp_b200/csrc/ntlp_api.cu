@@ -39,10 +39,13 @@ namespace {
 struct BoxHost {
     ntlp_grid grid{};
     std::vector<double> z, zz, dzw, dzu;
+    std::vector<int> lut;           // level-search bucket tables (zz, then z)
+    std::vector<float> rden;        // window denominators (zz, then z)
     int64_t cap = 0;
     int n_uploaded = 0;
     bool have_fields = false, have_droplets = false;
-    void *arena = nullptr, *arena_rk3 = nullptr;
+    void *arena = nullptr, *arena_rk3 = nullptr, *arena_stats = nullptr;
+    StatsScratch stats{};
     size_t arena_bytes = 0;
     double *staging = nullptr;      // flow-field / source transposes, upload tile tables
     int *rank = nullptr;            // download: list-order position by lid
@@ -116,6 +119,9 @@ int fail(ntlp_ctx *c, int code, const char *fmt, ...) {
                         __LINE__);                                                                 \
     } while (0)
 
+constexpr int kLutPerLevel = 4;    // search buckets per vertical level
+constexpr int kF32Guard = 8;       // guard elements around the FP32 field copies
+
 // Two-pass carving of one allocation: the first pass (base == nullptr) only
 // sums sizes, the second hands out 256-byte aligned pointers.
 struct Carver {
@@ -150,8 +156,14 @@ void carve_box(Carver &cv, BoxHost &h, DevBox &B, bool mixed) {
     const size_t n = (size_t)h.cap;
     double *zg;
     cv.take(&zg, 2 * (size_t)g.nz2 + 2 * ((size_t)g.nnz + 3));
+    int *lut;
+    cv.take(&lut, 2 * (size_t)kLutPerLevel * g.nz2);
+    float *rden;
+    cv.take(&rden, 2 * 6 * ((size_t)g.nnz + 3));
     if (cv.base) {
         B.g.z = zg; B.g.zz = zg + g.nz2; B.g.dzw = zg + 2 * g.nz2; B.g.dzu = zg + 2 * g.nz2 + (g.nnz + 3);
+        B.g.lut_zz = lut; B.g.lut_z = lut + kLutPerLevel * g.nz2;
+        B.g.rden_zz = rden; B.g.rden_z = rden + 6 * (g.nnz + 3);
     }
     for (int k = 0; k < 5; ++k) {
         double *f;
@@ -159,12 +171,17 @@ void carve_box(Carver &cv, BoxHost &h, DevBox &B, bool mixed) {
         B.f[k] = f;
     }
     if (mixed) {
+        // guard elements on both sides: the 6-level window loads of the
+        // mixed stencil may reach 4 levels before the first column and 2
+        // after the last (with zero weight); the guards keep them in bounds
         float4 *f4;
         float *fw;
-        cv.take(&f4, npad);
-        cv.take(&fw, npad);
-        B.f4 = f4;
-        B.fw = fw;
+        cv.take(&f4, npad + 2 * kF32Guard);
+        cv.take(&fw, npad + 2 * kF32Guard);
+        if (cv.base) {
+            B.f4 = f4 + kF32Guard;
+            B.fw = fw + kF32Guard;
+        }
     }
     carve_state(cv, B.st[0], n);
     carve_state(cv, B.st[1], n);
@@ -188,6 +205,8 @@ void carve_box(Carver &cv, BoxHost &h, DevBox &B, bool mixed) {
     cv.take(&B.err, 1);
     cv.take(&B.defer, n);
     cv.take(&B.ndefer, 1);
+    cv.take(&B.hist, (size_t)NTLP_H_STEP_KINDS * NTLP_HIST_N);
+    cv.take(&B.precip_fx, (size_t)g.nnx * g.nny * kFluxLimbs);
     // staging: the largest of a droplet array, a source array, a flow field
     // and the one-box tile tables of an upload
     size_t stage = n;
@@ -198,6 +217,65 @@ void carve_box(Carver &cv, BoxHost &h, DevBox &B, bool mixed) {
     if (tiles > stage) stage = tiles;
     cv.take(&h.staging, stage);
     cv.take(&h.rank, n);
+}
+
+// Host-side vertical tables of one box (see DevGrid): the bucket tables that
+// start the level searches and the reciprocal denominators of the 6-level
+// Lagrange windows, with the boundary rules of the 6th-order stencil
+// (particles.f90, interpolation of u,v,T,q on zz and of w on z).
+void level_tables(const BoxHost &h, int nnz, std::vector<int> &lut, double &scale, std::vector<float> &rden) {
+    const int nz2 = nnz + 2;
+    const int nlut = kLutPerLevel * nz2;
+    const double top = h.z[nz2 - 1];
+    scale = (double)nlut / top;
+    lut.assign(2 * (size_t)nlut, nz2);
+    const std::vector<double> *lev[2] = {&h.zz, &h.z};
+    for (int t = 0; t < 2; ++t) {
+        const std::vector<double> &a = *lev[t];
+        for (int b = 0; b < nlut; ++b) {
+            const double lo = b == 0 ? -INFINITY : (double)(b - 1) / scale;
+            int i = 0;
+            while (i < nz2 && !(a[i] > lo)) ++i;
+            lut[(size_t)t * nlut + b] = i;
+        }
+    }
+    rden.assign(2 * 6 * (size_t)(nnz + 3), 0.0f);
+    for (int t = 0; t < 2; ++t) {
+        const std::vector<double> &a = *lev[t];
+        for (int k2 = -2; k2 <= nnz; ++k2) {
+            int first, last;
+            if (t == 0) {          // u, v, T, q on zz
+                if (k2 == 1) { first = 3; last = 4; }
+                else if (k2 == 0) { first = 4; last = 5; }
+                else if (k2 < 0) { first = 0; last = 0; }
+                else if (k2 == 2) { first = 2; last = 5; }
+                else if (k2 == nnz) { first = 2; last = 3; }
+                else if (k2 > nnz) { first = 0; last = 0; }
+                else if (k2 == nnz - 1) { first = 3; last = 4; }
+                else if (k2 == nnz - 2) { first = 2; last = 5; }
+                else { first = 1; last = 6; }
+            } else {               // w on z
+                if (k2 == 0) { first = 3; last = 4; }
+                else if (k2 < 0) { first = 0; last = 0; }
+                else if (k2 == 1) { first = 2; last = 5; }
+                else if (k2 == nnz - 1) { first = 3; last = 4; }
+                else if (k2 >= nnz) { first = 0; last = 0; }
+                else if (k2 == nnz - 2) { first = 2; last = 5; }
+                else { first = 1; last = 6; }
+            }
+            float *out = &rden[(size_t)t * 6 * (nnz + 3) + (size_t)(k2 + 2) * 6];
+            for (int j = 0; j < 6; ++j) {
+                if (j + 1 < first || j + 1 > last) continue;
+                const int lj = k2 + j - 2;
+                double den = 1.0;
+                for (int k = 0; k < 6; ++k) {
+                    if (k == j || k + 1 < first || k + 1 > last) continue;
+                    den *= a[lj] - a[k2 + k - 2];
+                }
+                out[j] = (float)(1.0 / den);
+            }
+        }
+    }
 }
 
 int check_grid(ntlp_ctx *c, const ntlp_grid *g) {
@@ -248,6 +326,12 @@ void fill_devparams(const ntlp_params *p, DevParams &d) {
     d.CpaCpp = p->Cpa / p->Cpp;                       // les.F:10759
     d.Sc13 = ntlp_pow(p->Sc, 1.0 / 3.0);              // Sc**(1./3.)
     d.Pra13 = ntlp_pow(p->Pra, 1.0 / 3.0);            // Pra**(1./3.)
+    // set_binsdata calls of particles.f90:1909-1921
+    d.hb[NTLP_H_ACTRES] = ntlp_hist_log_bins(1.0e-1, 1.0e4);
+    d.hb[NTLP_H_RES] = ntlp_hist_log_bins(1.0e-1, 1.0e4);
+    d.hb[NTLP_H_ACTTODEATH] = ntlp_hist_log_bins(1.0e-1, 1.0e4);
+    d.hb[NTLP_H_NUMACT] = ntlp_hist_int_bins(0.0);
+    d.hb[NTLP_H_RADDEATH] = ntlp_hist_log_bins(1.0e-8, 1.0e-3);
 }
 
 int push_boxes(ntlp_ctx *c) {
@@ -358,6 +442,7 @@ extern "C" void ntlp_ctx_destroy(ntlp_ctx *c) {
     for (auto &h : c->bh) {
         if (h.arena) cudaFreeAsync(h.arena, c->stream);
         if (h.arena_rk3) cudaFreeAsync(h.arena_rk3, c->stream);
+        if (h.arena_stats) cudaFreeAsync(h.arena_stats, c->stream);
     }
     if (c->small_arena) cudaFreeAsync(c->small_arena, c->stream);
     if (c->stream) cudaStreamSynchronize(c->stream);
@@ -444,12 +529,26 @@ int create(int nbox, const ntlp_grid *grids, const ntlp_params *params, const in
         Carver cv2;
         cv2.base = (unsigned char *)h.arena;
         carve_box(cv2, h, B, mixed);
-        if (cudaMemcpyAsync((void *)B.g.z, h.z.data(), nz2 * 8, cudaMemcpyHostToDevice, c->stream) ||
+        level_tables(h, grid->nnz, h.lut, B.g.lut_scale, h.rden);
+        B.g.nlut = kLutPerLevel * nz2;
+        if (mixed) {
+            const size_t npad = (size_t)nz2 * B.g.ny5 * B.g.nx5 + 2 * kF32Guard;
+            if (cudaMemsetAsync((void *)(B.f4 - kF32Guard), 0, npad * sizeof(float4), c->stream) ||
+                cudaMemsetAsync((void *)(B.fw - kF32Guard), 0, npad * sizeof(float), c->stream))
+                return bail(fail(c, NTLP_ERR_CUDA, "initialising box %d failed", b));
+        }
+        if (cudaMemcpyAsync((void *)B.g.lut_zz, h.lut.data(), h.lut.size() * sizeof(int), cudaMemcpyHostToDevice,
+                            c->stream) ||
+            cudaMemcpyAsync((void *)B.g.rden_zz, h.rden.data(), h.rden.size() * sizeof(float),
+                            cudaMemcpyHostToDevice, c->stream) ||
+            cudaMemcpyAsync((void *)B.g.z, h.z.data(), nz2 * 8, cudaMemcpyHostToDevice, c->stream) ||
             cudaMemcpyAsync((void *)B.g.zz, h.zz.data(), nz2 * 8, cudaMemcpyHostToDevice, c->stream) ||
             cudaMemcpyAsync((void *)B.g.dzw, h.dzw.data(), nz3 * 8, cudaMemcpyHostToDevice, c->stream) ||
             cudaMemcpyAsync((void *)B.g.dzu, h.dzu.data(), nz3 * 8, cudaMemcpyHostToDevice, c->stream) ||
             cudaMemsetAsync(B.cell_cnt, 0, sizeof(int) * (size_t)(g.ncells + 2), c->stream) ||
             cudaMemsetAsync(B.n_alive, 0, sizeof(int), c->stream) ||
+            cudaMemsetAsync(B.hist, 0, sizeof(long long) * NTLP_H_STEP_KINDS * NTLP_HIST_N, c->stream) ||
+            cudaMemsetAsync(B.precip_fx, 0, sizeof(long long) * kFluxLimbs * g.nnx * g.nny, c->stream) ||
             cudaMemsetAsync(B.counters, 0, sizeof(long long) * kNumCounters, c->stream))
             return bail(fail(c, NTLP_ERR_CUDA, "initialising box %d failed", b));
     }
@@ -824,6 +923,51 @@ int sources_out(ntlp_ctx *c, int b, int32_t layout, double *const host[6]) {
     return NTLP_OK;
 }
 
+// exact fixed-point limbs (kFluxLimbs x 32 bits, LSB 2^kFluxLsbExp) -> double
+double limbs_to_double(const long long *in) {
+    long long L[kFluxLimbs];
+    for (int k = 0; k < kFluxLimbs; ++k) L[k] = in[k];
+    for (int k = 0; k < kFluxLimbs - 1; ++k) {     // carry-normalise (top limb signed)
+        long long carry = L[k] >> 32;              // arithmetic shift: floor division
+        L[k] -= carry * 4294967296LL;
+        L[k + 1] += carry;
+    }
+    long double v = 0.0L;
+    for (int k = kFluxLimbs - 1; k >= 0; --k) v += ldexpl((long double)L[k], 32 * k + kFluxLsbExp);
+    return (double)v;
+}
+
+// stats tiles + reduction for one box into its (lazily allocated) scratch
+int stats_run(ntlp_ctx *c, int b, bool radius_hist) {
+    BoxHost &h = c->bh[b];
+    const DevGrid &g = c->box[b].g;
+    if (!h.arena_stats) {
+        const int nt = stats_tile_count(g);
+        StatsScratch w{};
+        auto lay = [&](Carver &k) {
+            k.take(&w.colsum, (size_t)(g.nnx + 1) * (g.nny + 1));
+            k.take(&w.tile0, (size_t)nt * kS0N);
+            k.take(&w.tileL, (size_t)nt * NTLP_STATS_LEVEL_QTYS * g.nnz);
+            k.take(&w.out0, kS0N);
+            k.take(&w.outL, (size_t)NTLP_STATS_LEVEL_QTYS * g.nnz);
+            k.take(&w.hrad, NTLP_HIST_N);
+        };
+        Carver cv;
+        lay(cv);
+        if (pool_alloc(c, &h.arena_stats, cv.off) != cudaSuccess)
+            return fail(c, NTLP_ERR_NOMEM, "device allocation of the statistics scratch refused");
+        c->bytes += (int64_t)cv.off;
+        Carver cv2;
+        cv2.base = (unsigned char *)h.arena_stats;
+        lay(cv2);
+        h.stats = w;
+    }
+    launch_stats(c->box_d, b, g, c->dp_d, h.stats, radius_hist, c->stream);
+    c->launches += 2;
+    CK(cudaGetLastError());
+    return NTLP_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1152,6 +1296,99 @@ int ntlp_autotune(ntlp_ctx *c, double dt, int32_t it, int32_t steps, int32_t cho
     }
     if (ms)
         for (int k = 0; k < NTLP_TUNE_VARIANTS; ++k) ms[k] = local[k];
+    return NTLP_OK;
+}
+
+int ntlp_stats(ntlp_ctx *c, int32_t box, ntlp_stats0 *s0, int32_t maxnz, double *level_sums, double *lwp) {
+    if (!box_ok(c, box)) return NTLP_ERR_ARG;
+    BoxHost &h = c->bh[box];
+    if (!h.have_droplets) return fail(c, NTLP_ERR_STATE, "droplets not uploaded");
+    const DevGrid &g = c->box[box].g;
+    if (level_sums && maxnz < g.nnz) return fail(c, NTLP_ERR_ARG, "maxnz %d below nnz %d", maxnz, g.nnz);
+    int rc = stats_run(c, box, false);
+    if (rc) return rc;
+    std::vector<double> out0(kS0N);
+    CK(cudaMemcpyAsync(out0.data(), h.stats.out0, kS0N * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    std::vector<double> outL, col;
+    if (level_sums) {
+        outL.resize((size_t)NTLP_STATS_LEVEL_QTYS * g.nnz);
+        CK(cudaMemcpyAsync(outL.data(), h.stats.outL, outL.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                           c->stream));
+    }
+    if (lwp) {
+        col.resize((size_t)(g.nnx + 1) * (g.nny + 1));
+        CK(cudaMemcpyAsync(col.data(), h.stats.colsum, col.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                           c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    if (s0) {
+        // the reference's starting values of the extrema (particles.f90:3409-3421)
+        s0->numpart = (int64_t)out0[0];
+        s0->numdrop = (int64_t)out0[1];
+        s0->numaerosol = s0->numpart - s0->numdrop;
+        s0->Rep_sum = out0[2]; s0->wmass = out0[3]; s0->pmass = out0[4]; s0->pvol = out0[5];
+        s0->rad_sum = out0[6]; s0->rad2_sum = out0[7];
+        s0->radmax = fmax(0.0, out0[8]);
+        s0->tempmax = fmax(0.0, out0[9]);
+        s0->qmax = fmax(0.0, out0[10]);
+        for (int k = 0; k < 3; ++k) s0->vpmax[k] = fmax(-1000.0, out0[11 + k]);
+        s0->radmin = fmin(1000.0, out0[14]);
+        s0->tempmin = fmin(1000.0, out0[15]);
+        s0->qmin = fmin(1000.0, out0[16]);
+        for (int k = 0; k < 3; ++k) s0->vpmin[k] = fmin(1000.0, out0[17 + k]);
+    }
+    if (level_sums) {
+        for (int q = 0; q < NTLP_STATS_LEVEL_QTYS; ++q)
+            for (int iz = 0; iz < maxnz; ++iz)
+                level_sums[(size_t)q * maxnz + iz] = iz < g.nnz ? outL[(size_t)q * g.nnz + iz] : 0.0;
+    }
+    if (lwp) {
+        // columns ipt = nnx+1 / jpt = nny+1 hold droplets exactly at x = xl /
+        // y = yl; they are added to their periodic images, x first, then y
+        const int nx1 = g.nnx + 1, ny1 = g.nny + 1;
+        auto at = [&](int i, int j) -> double & { return col[(size_t)(j - 1) + (size_t)ny1 * (i - 1)]; };
+        for (int j = 1; j <= ny1; ++j) at(1, j) = at(1, j) + at(nx1, j);
+        for (int i = 1; i <= g.nnx; ++i) at(i, 1) = at(i, 1) + at(i, ny1);
+        for (int j = 1; j <= g.nny; ++j)
+            for (int i = 1; i <= g.nnx; ++i) lwp[(size_t)(i - 1) + (size_t)g.nnx * (j - 1)] = at(i, j);
+    }
+    return NTLP_OK;
+}
+
+int ntlp_radius_histogram(ntlp_ctx *c, int32_t box, double hist_rad[NTLP_HIST_BINS]) {
+    if (!box_ok(c, box) || !hist_rad) return NTLP_ERR_ARG;
+    BoxHost &h = c->bh[box];
+    if (!h.have_droplets) return fail(c, NTLP_ERR_STATE, "droplets not uploaded");
+    int rc = stats_run(c, box, true);
+    if (rc) return rc;
+    long long hb[NTLP_HIST_N];
+    CK(cudaMemcpyAsync(hb, h.stats.hrad, sizeof hb, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int b = 0; b < NTLP_HIST_N; ++b) hist_rad[b] = (double)hb[b];
+    return NTLP_OK;
+}
+
+int ntlp_step_histograms(ntlp_ctx *c, int32_t box, double *hist, double *surf_precip, int32_t reset) {
+    if (!box_ok(c, box)) return NTLP_ERR_ARG;
+    const DevBox &B = c->box[box];
+    const DevGrid &g = B.g;
+    std::vector<long long> hb((size_t)NTLP_H_STEP_KINDS * NTLP_HIST_N);
+    std::vector<long long> fx;
+    CK(cudaMemcpyAsync(hb.data(), B.hist, hb.size() * sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
+    if (surf_precip) {
+        fx.resize((size_t)g.nnx * g.nny * kFluxLimbs);
+        CK(cudaMemcpyAsync(fx.data(), B.precip_fx, fx.size() * sizeof(long long), cudaMemcpyDeviceToHost,
+                           c->stream));
+    }
+    if (reset) {
+        CK(cudaMemsetAsync(B.hist, 0, hb.size() * sizeof(long long), c->stream));
+        CK(cudaMemsetAsync(B.precip_fx, 0, sizeof(long long) * kFluxLimbs * g.nnx * g.nny, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    if (hist)
+        for (size_t k = 0; k < hb.size(); ++k) hist[k] = (double)hb[k];
+    if (surf_precip)
+        for (size_t e = 0; e < (size_t)g.nnx * g.nny; ++e) surf_precip[e] = limbs_to_double(&fx[e * kFluxLimbs]);
     return NTLP_OK;
 }
 

@@ -18,7 +18,8 @@
 // MIXED=false: each contribution is formed as the reference writes it,
 // ((P*wtt)/dV)*mult with wtt = wtx*wty*wtz, subtracted term by term.
 // MIXED=true: the FP32 payload (cell-relative fractions, momentum/heat/
-// vapour factors, mult/dV), FP32 weights, FP64 sums.
+// vapour factors, mult/dV), FP32 weights, FP64 sums, taken cell by cell in a
+// fixed order instead of merged (deterministic, not list order).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -133,10 +134,39 @@ __device__ __forceinline__ void merge_ranges(const DevBox &B, const DevParams &p
     }
 }
 
+// Mixed: the node's cells in the fixed order (i, j, k) = (0,0,0), (0,0,1),
+// ..., (1,1,1), each cell's droplets in its (lid-sorted) list order; the
+// staged and the global path below perform the same operations in the same
+// order, so every tile shape gives the same sums.
+__device__ __forceinline__ void image_global32(const DevBox &B, const DevParams &p, int px, int py, int pz,
+                                               double acc[6]) {
+    const DevGrid &g = B.g;
+    for (int q = 0; q < 6; ++q) acc[q] = 0.0;
+#pragma unroll
+    for (int o = 0; o < 8; ++o) {
+        const int i = o >> 2, j = (o >> 1) & 1, k = o & 1;
+        const int ci = px - i, cj = py - j, ckk = pz - k;
+        if (ci < 1 || ci > g.nnx + 1 || cj < 1 || cj > g.nny + 1 || ckk < 0 || ckk > g.nnz) continue;
+        const int key = ckk + (g.nnz + 1) * ((cj - 1) + (g.nny + 1) * (ci - 1));
+        const int a = B.cell_start[key], b = B.cell_start[key + 1];
+        for (int at = a; at < b; ++at) {
+            const int t = B.perm[at];
+            float v[P32_N];
+#pragma unroll
+            for (int q = 0; q < P32_N; ++q) v[q] = B.pay32.f[q][t];
+            contribute32(p, v, i, j, k, acc);
+        }
+    }
+}
+
 // one pre-fold node image from global memory
 template <bool MIXED>
 __device__ __forceinline__ void image_global(const DevBox &B, const DevParams &p, int px, int py, int pz,
                                              double acc[6]) {
+    if (MIXED) {
+        image_global32(B, p, px, py, pz, acc);
+        return;
+    }
     const DevGrid &g = B.g;
     int pos[8], end[8], ck[8], off[8];
     int n = 0;
@@ -240,7 +270,7 @@ k_deposit_tiled(DevBox *boxes, const Tile *tiles, const DevParams *pp) {
                 int cc = 0;
                 while (cc + 1 < kDepCols && s_off[cc + 1] <= k) ++cc;
                 const int t = B.perm[s_cs[cc * kDepCSW] + (k - s_off[cc])];
-                s_lid[k] = O.lid[t];
+                if (!MIXED) s_lid[k] = O.lid[t];
                 if (MIXED) {
                     for (int q = 0; q < P32_N; ++q) s_f[q * CAP + k] = B.pay32.f[q][t];
                 } else {
@@ -260,7 +290,26 @@ k_deposit_tiled(DevBox *boxes, const Tile *tiles, const DevParams *pp) {
                 }
             }
             __syncthreads();
-            if (valid) {
+            if (valid && MIXED) {
+                for (int q = 0; q < 6; ++q) out[q] = 0.0;
+#pragma unroll
+                for (int o = 0; o < 8; ++o) {
+                    const int i = o >> 2, j = (o >> 1) & 1, k = o & 1;
+                    const int ckk = iz - k;
+                    if (ckk < 0 || ckk > g.nnz) continue;
+                    const int cc = (lx + 1 - i) * (kDepTY + 1) + (ly + 1 - j);
+                    const int lzz = lz + 1 - k;
+                    const int base = s_off[cc] - s_cs[cc * kDepCSW];
+                    const int a = base + s_cs[cc * kDepCSW + lzz];
+                    const int b = base + s_cs[cc * kDepCSW + lzz + 1];
+                    for (int at = a; at < b; ++at) {
+                        float v[P32_N];
+#pragma unroll
+                        for (int q = 0; q < P32_N; ++q) v[q] = s_f[q * CAP + at];
+                        contribute32(p, v, i, j, k, out);
+                    }
+                }
+            } else if (valid) {
                 int pos[8], end[8], ck[8], off[8];
                 int n = 0;
                 for (int i = 0; i <= 1; ++i)

@@ -20,6 +20,7 @@
 #include <cstdint>
 
 #include "ntlp_math.h"
+#include "ntlp_hist.h"
 
 namespace ntlp {
 
@@ -39,6 +40,16 @@ struct DevGrid {
     const double *z, *zz, *dzw, *dzu;
     long long ncells;      // (nnx+1)(nny+1)(nnz+1)
     long long nnodes;      // (nnz+2)*nny*nnx
+    // Bucket tables that start the level searches (NULL: plain binary
+    // search).  Bucket b covers heights [b, b+1) / lut_scale; its entry is
+    // the first level above the lower edge of bucket b-1.
+    const int *lut_zz, *lut_z;
+    int nlut;
+    double lut_scale;
+    // Reciprocal Lagrange denominators of every 6-level window of the
+    // 6th-order stencil (mixed path), 6 floats per window base k2 in
+    // [-2, nnz] at (k2+2)*6; 0 marks a point the boundary rules leave out.
+    const float *rden_zz, *rden_z;
 };
 
 struct DevParams {
@@ -48,6 +59,8 @@ struct DevParams {
     double radius_init, surf_rho, surf_p, tsfcc1, pi2;
     // derived on the host once: Cpa/Cpp (les.F:10759), Sc**(1./3.), Pra**(1./3.)
     double CpaCpp, Sc13, Pra13;
+    // histogram binning (particles.f90:1909-1921), by NTLP_H_* kind
+    ntlp_hbins hb[NTLP_H_STEP_KINDS];
 };
 
 struct DevState {
@@ -97,6 +110,8 @@ struct DevBox {
     int *err;              // device error word (0 = fine)
     int *defer;            // [cap] droplets whose Gauss-Newton solve failed this step
     int *ndefer;           // their count
+    long long *hist;       // [NTLP_H_STEP_KINDS][NTLP_HIST_N] step histograms (weights are integers)
+    long long *precip_fx;  // [nny][nnx][kFluxLimbs] surface precipitation, exact fixed point
 };
 
 // ---- binning ---------------------------------------------------------------
@@ -115,6 +130,28 @@ __device__ __forceinline__ int minloc_gt(const double *a, int n, double x) {
     return lo < n ? lo + 1 : 0;
 }
 
+// minloc_gt over z(0:nnz+1) / zz(0:nnz+1), started from the bucket table:
+// the levels below the table entry are all <= x, and the forward scan stops
+// at the first level > x, so the result is the binary search's.
+__device__ __forceinline__ int minloc_lut(const double *a, int n, const int *lut, int nlut, double scale,
+                                          double x) {
+    if (lut != nullptr && x == x) {
+        const double q = x * scale;
+        if (q >= 0.0 && q < (double)nlut) {
+            int i = lut[(int)q];
+            while (i < n && !(a[i] > x)) ++i;
+            return i < n ? i + 1 : 0;
+        }
+    }
+    return minloc_gt(a, n, x);
+}
+__device__ __forceinline__ int minloc_zz(const DevGrid &g, double x) {
+    return minloc_lut(g.zz, g.nz2, g.lut_zz, g.nlut, g.lut_scale, x);
+}
+__device__ __forceinline__ int minloc_z(const DevGrid &g, double x) {
+    return minloc_lut(g.z, g.nz2, g.lut_z, g.nlut, g.lut_scale, x);
+}
+
 // floor(x/d)+1 with an IEEE divide (particles.f90:571-572).
 __device__ __forceinline__ int ijpt(double x, double d) {
     double q = floor(x / d);
@@ -128,7 +165,7 @@ __device__ __forceinline__ int cell_key(const DevGrid &g, double x1, double x2, 
                                         int *kpt_out = nullptr) {
     int ipt = ijpt(x1, g.dx);
     int jpt = ijpt(x2, g.dy);
-    int kpt = minloc_gt(g.zz, g.nz2, x3) - 2;
+    int kpt = minloc_zz(g, x3) - 2;
     if (ipt_out) { *ipt_out = ipt; *jpt_out = jpt; *kpt_out = kpt; }
     if (ipt < 1 || ipt > g.nnx + 1 || jpt < 1 || jpt > g.nny + 1 || kpt < 0 || kpt > g.nnz)
         return (int)g.ncells;

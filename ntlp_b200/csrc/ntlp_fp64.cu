@@ -27,8 +27,8 @@ __device__ void interp_lin64(const DevBox &B, double x1, double x2, double x3, I
     const double dx = g.dx, dy = g.dy;
     int ipt = ijpt(x1, dx);
     int jpt = ijpt(x2, dy);
-    int kpt = minloc_gt(g.zz, g.nz2, x3) - 2;
-    int kwpt = minloc_gt(g.z, g.nz2, x3) - 2;
+    int kpt = minloc_zz(g, x3) - 2;
+    int kwpt = minloc_z(g, x3) - 2;
     if (kpt + 1 < 0 || kpt + 1 > g.nnz + 2 || kwpt + 1 < 0 || kwpt + 1 > g.nnz + 2) {
         bad = 1;
         kpt = kpt < -1 ? -1 : (kpt > g.nnz + 1 ? g.nnz + 1 : kpt);
@@ -100,8 +100,8 @@ __device__ void interp6_64(const DevBox &B, double x1, double x2, double x3, Int
     const int nnz = g.nnz;
     int ip3 = ijpt(x1, g.dx), jp3 = ijpt(x2, g.dy);
     int ku[6], kw[6];
-    ku[2] = minloc_gt(g.zz, g.nz2, x3) - 2;
-    kw[2] = minloc_gt(g.z, g.nz2, x3) - 2;
+    ku[2] = minloc_zz(g, x3) - 2;
+    kw[2] = minloc_z(g, x3) - 2;
     for (int a = 0; a < 6; ++a) { ku[a] = ku[2] + (a - 2); kw[a] = kw[2] + (a - 2); }
     double wx[6], wy[6], wz[6], wzw[6];
     {
@@ -363,6 +363,7 @@ k_update_rk3_64(DevBox *boxes, const Tile *tiles, const DevParams *pp, StepIn in
         if (!alive) {
             key = (int)B.g.ncells + 1;
             cnt.v[C_DESTROY]++;
+            record_kill(B, p, x, radius, S.rc[s], res, S.actres[s], S.numact[s], multi);
         } else {
             key = cell_key(B.g, x[0], x[1], x[2]);
             if (in.write_payload)

@@ -79,4 +79,20 @@ void launch_pack_f32(const DevBox *host_box, float4 *f4, float *fw, cudaStream_t
 // download: position of each survivor in list order
 void launch_rank_alive(DevBox *boxes, int box, int *rank_by_lid, int nlid, cudaStream_t st);
 
+// particle_xy_stats and radius_histogram of one box (ntlp_stats.cu)
+constexpr int kStatCols = 128;      // columns per tile (one block)
+constexpr int kStatThreads = 256;
+constexpr int kS0N = 20;            // 0th-order values per partial
+struct StatsScratch {
+    double *colsum;                 // [(nnx+1)(nny+1)] LWP per column
+    double *tile0;                  // [tiles][kS0N]
+    double *tileL;                  // [tiles][24][nnz]
+    double *out0;                   // [kS0N]
+    double *outL;                   // [24][nnz]
+    long long *hrad;                // [NTLP_HIST_N]
+};
+int stats_tile_count(const DevGrid &g);
+void launch_stats(const DevBox *boxes, int box, const DevGrid &g, const DevParams *pp, const StatsScratch &w,
+                  bool radius_hist, cudaStream_t st);
+
 }  // namespace ntlp

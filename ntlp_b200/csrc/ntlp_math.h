@@ -180,6 +180,21 @@ NTLP_HD double ntlp_log(double x) {
     return hi;
 }
 
+/* log10(x) = log(x) / ln(10): the double-double log times 1/ln(10) split
+ * into two doubles (computed to 60 digits from the definition).           */
+#define NTLP_INV_LN10_HI 0x1.bcb7b1526e50ep-2
+#define NTLP_INV_LN10_LO 0x1.95355baaafad3p-57
+NTLP_HD double ntlp_log10(double x) {
+    double lo;
+    double hi = ntlp_log_dd(x, &lo);
+    if (!(hi == hi) || hi == ntlp_inf() || hi == -ntlp_inf()) return hi;
+    double p = hi * NTLP_INV_LN10_HI;
+    double e = fma(hi, NTLP_INV_LN10_HI, -p);
+    e = fma(hi, NTLP_INV_LN10_LO, e);
+    e = fma(lo, NTLP_INV_LN10_HI, e);
+    return p + e;
+}
+
 /* ---- pow -------------------------------------------------------------- */
 NTLP_HD int ntlp_is_int(double y) { return floor(y) == y && fabs(y) < 0x1p53; }
 

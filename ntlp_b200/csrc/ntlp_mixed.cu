@@ -23,82 +23,71 @@
 
 namespace ntlp {
 
-// Lagrange weights on six nodes from FP64 offsets d[k] = x - x_k and node
-// differences, in FP32; unrolled with predicated factors (registers only).
-__device__ __forceinline__ void lagrange6_f(const double x, const double xn[6], int first, int last, float w[6]) {
-    float d[6];
-#pragma unroll
-    for (int k = 0; k < 6; ++k) d[k] = (float)(x - xn[k]);
-#pragma unroll
-    for (int j = 0; j < 6; ++j) {
-        const bool jin = (j + 1 >= first) && (j + 1 <= last);
-        float num = 1.0f, den = 1.0f;
-#pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            const bool use = k != j && k + 1 >= first && k + 1 <= last;
-            num *= use ? d[k] : 1.0f;
-            den *= use ? (float)(xn[j] - xn[k]) : 1.0f;
-        }
-        w[j] = jin ? num / den : 0.0f;
-    }
+// Lagrange weights on the uniform nodes 0..5 at s (x = x0 + s*dx):
+// w_j = prod_{k!=j} (s-k) / prod_{k!=j} (j-k), numerators from prefix and
+// suffix products.
+__device__ __forceinline__ void lagrange6_unif(float s, float w[6]) {
+    const float d0 = s, d1 = s - 1.f, d2 = s - 2.f, d3 = s - 3.f, d4 = s - 4.f, d5 = s - 5.f;
+    const float p2 = d0 * d1, p3 = p2 * d2, p4 = p3 * d3;
+    const float q3 = d4 * d5, q2 = d3 * q3, q1 = d2 * q2;
+    w[0] = (d1 * q1) * (-1.f / 120.f);
+    w[1] = (d0 * q1) * (1.f / 24.f);
+    w[2] = (p2 * q2) * (-1.f / 12.f);
+    w[3] = (p3 * q3) * (1.f / 12.f);
+    w[4] = (p4 * d5) * (-1.f / 24.f);
+    w[5] = (p4 * d4) * (1.f / 120.f);
 }
 
+// Lagrange weights of one 6-level window (levels k2-2 .. k2+3 of lev),
+// with the window's reciprocal denominators rd (0: point not used).
+__device__ __forceinline__ void lagrange6_win(double x, const double *lev, int k2, int nz2, const float *rd,
+                                              float w[6]) {
+    float d[6], r[6];
+#pragma unroll
+    for (int a = 0; a < 6; ++a) {
+        r[a] = rd[a];
+        int kk = k2 + a - 2;
+        kk = kk < 0 ? 0 : (kk > nz2 - 1 ? nz2 - 1 : kk);
+        d[a] = r[a] != 0.f ? (float)(x - lev[kk]) : 1.f;
+    }
+    const float p2 = d[0] * d[1], p3 = p2 * d[2], p4 = p3 * d[3];
+    const float q3 = d[4] * d[5], q2 = d[3] * q3, q1 = d[2] * q2;
+    w[0] = r[0] * (d[1] * q1);
+    w[1] = r[1] * (d[0] * q1);
+    w[2] = r[2] * (p2 * q2);
+    w[3] = r[3] * (p3 * q3);
+    w[4] = r[4] * (p4 * d[5]);
+    w[5] = r[5] * (p4 * d[4]);
+}
+
+// 6th-order interpolation (particles.f90:700-800) on the FP32 deviation
+// copies.  The stencil's boundary rules only remove points (weight 0), so
+// every column is read as one contiguous 6-level window; the window may
+// reach outside the column (into the neighbour or the guard elements) only
+// where the weight is 0.
 __device__ void interp6_mixed(const DevBox &B, double x1, double x2, double x3, Interp &o, int &bad) {
     const DevGrid &g = B.g;
     const int nnz = g.nnz;
-    int ip3 = ijpt(x1, g.dx), jp3 = ijpt(x2, g.dy);
-    int ku[6], kw[6];
-    ku[2] = minloc_gt(g.zz, g.nz2, x3) - 2;
-    kw[2] = minloc_gt(g.z, g.nz2, x3) - 2;
-    for (int a = 0; a < 6; ++a) { ku[a] = ku[2] + (a - 2); kw[a] = kw[2] + (a - 2); }
+    const int ip3 = ijpt(x1, g.dx), jp3 = ijpt(x2, g.dy);
+    const int ku2 = minloc_zz(g, x3) - 2;
+    const int kw2 = minloc_z(g, x3) - 2;
+    if (ku2 < 0 || ku2 > nnz + 1 || kw2 < 0) bad = 1;
     float wx[6], wy[6], wz[6], wzw[6];
-    {
-        double xn[6], yn[6];
-        for (int a = 0; a < 6; ++a) {
-            xn[a] = g.dx * (double)(ip3 + (a - 2) - 1);
-            yn[a] = g.dy * (double)(jp3 + (a - 2) - 1);
-        }
-        lagrange6_f(x1, xn, 1, 6, wx);
-        lagrange6_f(x2, yn, 1, 6, wy);
+    // xn(a) = dx*(ip3-3+a): s = x/dx - (ip3-3) in [2, 3)
+    lagrange6_unif((float)(x1 / g.dx - (double)(ip3 - 3)), wx);
+    lagrange6_unif((float)(x2 / g.dy - (double)(jp3 - 3)), wy);
+    const int cu = ku2 < -2 ? -2 : (ku2 > nnz ? nnz : ku2);
+    const int cw = kw2 < -2 ? -2 : (kw2 > nnz ? nnz : kw2);
+    if (g.rden_zz != nullptr) {
+        lagrange6_win(x3, g.zz, cu, g.nz2, g.rden_zz + (cu + 2) * 6, wz);
+        lagrange6_win(x3, g.z, cw, g.nz2, g.rden_z + (cw + 2) * 6, wzw);
+    } else {
+#pragma unroll
+        for (int a = 0; a < 6; ++a) { wz[a] = 0.f; wzw[a] = 0.f; }
+        bad = 1;
     }
-    int first, last;
-    if (ku[2] == 1) { first = 3; last = 4; ku[0] = 1; ku[1] = 1; }
-    else if (ku[2] == 0) { first = 4; last = 5; ku[0] = 1; ku[1] = 1; ku[2] = 1; }
-    else if (ku[2] < 0) { first = 0; last = 0; }
-    else if (ku[2] == 2) { first = 2; last = 5; }
-    else if (ku[2] == nnz) { first = 2; last = 3; ku[3] = nnz; ku[4] = nnz; ku[5] = nnz; }
-    else if (ku[2] > nnz) { first = 0; last = 0; }
-    else if (ku[2] == nnz - 1) { first = 3; last = 4; ku[4] = nnz; ku[5] = nnz; }
-    else if (ku[2] == nnz - 2) { first = 2; last = 5; }
-    else { first = 1; last = 6; }
-    {
-        double zn[6];
-        for (int a = 0; a < 6; ++a) {
-            int kk = ku[a] < 0 ? 0 : (ku[a] > nnz + 1 ? nnz + 1 : ku[a]);
-            ku[a] = kk;
-            zn[a] = g.zz[kk];
-        }
-        lagrange6_f(x3, zn, first, last, wz);
-    }
-    if (kw[2] == 0) { first = 3; last = 4; kw[0] = 1; kw[1] = 1; }
-    else if (kw[2] < 0) { first = 0; last = 0; kw[0] = 1; kw[1] = 1; kw[2] = 1; }
-    else if (kw[2] == 1) { first = 2; last = 5; kw[0] = 1; }
-    else if (kw[2] == nnz - 1) { first = 3; last = 4; kw[4] = nnz; kw[5] = nnz; }
-    else if (kw[2] >= nnz) { first = 0; last = 0; kw[2] = nnz; kw[3] = nnz; kw[4] = nnz; kw[5] = nnz; }
-    else if (kw[2] == nnz - 2) { first = 2; last = 5; kw[5] = nnz; }
-    else { first = 1; last = 6; }
-    {
-        double zn[6];
-        for (int a = 0; a < 6; ++a) {
-            int kk = kw[a] < 0 ? 0 : (kw[a] > nnz + 1 ? nnz + 1 : kw[a]);
-            kw[a] = kk;
-            zn[a] = g.z[kk];
-        }
-        lagrange6_f(x3, zn, first, last, wzw);
-    }
-    if (ku[2] < 0 || ku[2] > nnz + 1 || kw[2] < 0) bad = 1;
-    const float4 *f4 = B.f4;
-    const float *fw = B.fw;
+    const float4 *f4 = B.f4 + (cu - 2);
+    const float *fw = B.fw + (cw - 2);
     float su = 0.f, sv = 0.f, sw = 0.f, sT = 0.f, sq = 0.f;
     // the x loop stays rolled (one column plane of loads in flight at a
     // time); its weight is rotated through wx[0] so no array is indexed
@@ -108,7 +97,7 @@ __device__ void interp6_mixed(const DevBox &B, double x1, double x2, double x3, 
         int ix = ip3 + (i - 2);
         if (ix > g.nnx + 3) ix -= g.nnx;
         if (ix < -1 || ix > g.nnx + 3) { bad = 1; ix = ix < -1 ? -1 : g.nnx + 3; }
-        float cu = 0.f, cv = 0.f, cw = 0.f, cT = 0.f, cq = 0.f;
+        float cu_ = 0.f, cv = 0.f, cw_ = 0.f, cT = 0.f, cq = 0.f;
 #pragma unroll
         for (int j = 0; j < 6; ++j) {
             int iy = jp3 + (j - 2);
@@ -118,22 +107,22 @@ __device__ void interp6_mixed(const DevBox &B, double x1, double x2, double x3, 
             float au = 0.f, av = 0.f, aT = 0.f, aq = 0.f, aw = 0.f;
 #pragma unroll
             for (int k = 0; k < 6; ++k) {
-                const float4 val = __ldg(f4 + base + ku[k]);
+                const float4 val = __ldg(f4 + base + k);
                 au = fmaf(val.x, wz[k], au);
                 av = fmaf(val.y, wz[k], av);
                 aT = fmaf(val.z, wz[k], aT);
                 aq = fmaf(val.w, wz[k], aq);
-                aw = fmaf(__ldg(fw + base + kw[k]), wzw[k], aw);
+                aw = fmaf(__ldg(fw + base + k), wzw[k], aw);
             }
-            cu = fmaf(au, wy[j], cu);
+            cu_ = fmaf(au, wy[j], cu_);
             cv = fmaf(av, wy[j], cv);
-            cw = fmaf(aw, wy[j], cw);
+            cw_ = fmaf(aw, wy[j], cw_);
             cT = fmaf(aT, wy[j], cT);
             cq = fmaf(aq, wy[j], cq);
         }
-        su = fmaf(cu, wx[0], su);
+        su = fmaf(cu_, wx[0], su);
         sv = fmaf(cv, wx[0], sv);
-        sw = fmaf(cw, wx[0], sw);
+        sw = fmaf(cw_, wx[0], sw);
         sT = fmaf(cT, wx[0], sT);
         sq = fmaf(cq, wx[0], sq);
 #pragma unroll
@@ -151,8 +140,8 @@ __device__ void interp_lin_mixed(const DevBox &B, double x1, double x2, double x
     const DevGrid &g = B.g;
     int ipt = ijpt(x1, g.dx);
     int jpt = ijpt(x2, g.dy);
-    int kpt = minloc_gt(g.zz, g.nz2, x3) - 2;
-    int kwpt = minloc_gt(g.z, g.nz2, x3) - 2;
+    int kpt = minloc_zz(g, x3) - 2;
+    int kwpt = minloc_z(g, x3) - 2;
     if (kpt + 1 < 0 || kpt + 1 > g.nnz + 2 || kwpt + 1 < 0 || kwpt + 1 > g.nnz + 2) {
         bad = 1;
         kpt = kpt < -1 ? -1 : (kpt > g.nnz + 1 ? g.nnz + 1 : kpt);

@@ -159,6 +159,116 @@ __device__ int gauss_newton64(const DevParams &p, const Drop &d, const double ve
     return flag;
 }
 
+// Mixed path: the same Gauss-Newton iteration (start, relaxation, stopping
+// and failure rules of gauss_newton_2d) with the exact Jacobian of the
+// residual (forward-mode derivatives) instead of one-sided differences of
+// step 1e-12, and the 2x2 system solved directly (J^T J has determinant
+// det(J)^2, so the singularity test |det(J^T J)| < 1e-10 becomes
+// |det J| < 1e-5).  The residual is ie_vrt_nd with rhop*rnext/taup and
+// rhop/taup reduced to c_taup/(4 rnext) and c_taup/(4 rnext^2), and
+// VolP*rhop - m_s to VolP*rhow (identities of the definitions).  Both
+// iterations stop at |correction| < 1e-8 on the same root.
+struct AdConst {
+    double k_rpre;   // c_taup / (36 Sc rhow)
+    double k_tpre;   // -CpaCpp c_taup / (12 Pra rhow)
+    double k_rep;    // 2 diffnorm / nuf
+    double k_vol;    // (2/3) pi2
+    double k_sol;    // c_sol / rhow
+    double k_clat;   // 3 Lv / Cpp
+    double k_g;      // 2 Mw Gam / (Ru rhow)
+    double k_e1;     // Lv Mw / Ru
+    double k_q;      // Mw esa / (Ru rhoa)
+};
+
+__device__ __forceinline__ void resid_jac_ad(const DevParams &p, const Drop &d, const AdConst &k, double a,
+                                             double b, double f[2], double J[4]) {
+    const double R = d.radius;
+    const double rn = a * R;
+    const double irn = 1.0 / rn;
+    // r-dependent part (derivatives with respect to a; drn/da = R)
+    const double Rep = k.k_rep * rn;
+    const double sRep = sqrt(Rep);
+    const double sRep_a = sRep > 0.0 ? 0.5 * k.k_rep * R / sRep : 0.0;
+    const double Shp = 2.0 + 0.6 * sRep * p.Sc13, Shp_a = 0.6 * p.Sc13 * sRep_a;
+    const double Nup = 2.0 + 0.6 * sRep * p.Pra13, Nup_a = 0.6 * p.Pra13 * sRep_a;
+    const double rpre = k.k_rpre * Shp * irn;
+    const double rpre_a = k.k_rpre * (Shp_a - Shp * R * irn) * irn;
+    const double irn2 = irn * irn;
+    const double tpre = k.k_tpre * Nup * irn2;
+    const double tpre_a = k.k_tpre * (Nup_a - 2.0 * Nup * R * irn) * irn2;
+    const double clat = k.k_clat * irn, clat_a = -clat * R * irn;
+    const double solterm = k.k_sol / (k.k_vol * rn * rn * rn);
+    const double solterm_a = -3.0 * solterm * R * irn;
+    const double g = k.k_g * irn, g_a = -g * R * irn;
+    // T-dependent part (dTn/db = Tp)
+    const double Tn = b * d.Tp;
+    const double iTn = 1.0 / Tn, iTn_b = -iTn * iTn * d.Tp;
+    const double E = k.k_e1 * (d.inv_Tf - iTn) + g * iTn - solterm;
+    const double E_a = g_a * iTn - solterm_a;
+    const double E_b = (g - k.k_e1) * iTn_b;
+    const double qstr = k.k_q * iTn * ntlp_exp(E);
+    const double qstr_a = qstr * E_a;
+    const double qstr_b = qstr * (E_b - d.Tp * iTn);
+    const double dq = d.qinf - qstr;
+    const double rprime = rpre * dq * d.t0r;
+    const double rprime_a = (rpre_a * dq - rpre * qstr_a) * d.t0r;
+    const double rprime_b = -rpre * qstr_b * d.t0r;
+    const double Tprime = (tpre * (Tn - d.Tf) + clat * rprime * d.rt0) * d.t0T;
+    const double Tprime_a = (tpre_a * (Tn - d.Tf) + (clat_a * rprime + clat * rprime_a) * d.rt0) * d.t0T;
+    const double Tprime_b = (tpre * d.Tp + clat * rprime_b * d.rt0) * d.t0T;
+    f[0] = (a - 1.0) - d.h * rprime;
+    f[1] = (b - 1.0) - d.h * Tprime;
+    J[0] = 1.0 - d.h * rprime_a;   // df1/da
+    J[1] = -d.h * Tprime_a;        // df2/da
+    J[2] = -d.h * rprime_b;        // df1/db
+    J[3] = 1.0 - d.h * Tprime_b;   // df2/db
+}
+
+__device__ int gauss_newton_ad(const DevParams &p, const Drop &d, const double vec1[2], double vec2[2]) {
+    AdConst k;
+    k.k_rpre = d.c_taup / (36.0 * p.Sc * p.rhow);
+    k.k_tpre = -p.CpaCpp * d.c_taup / (12.0 * p.Pra * p.rhow);
+    k.k_rep = 2.0 * d.diffnorm / p.nuf;
+    k.k_vol = (2.0 / 3.0) * p.pi2;
+    k.k_sol = d.c_sol / p.rhow;
+    k.k_clat = 3.0 * p.Lv / p.Cpp;
+    k.k_g = 2.0 * p.Mw * p.Gam / (p.Ru * p.rhow);
+    k.k_e1 = p.Lv * p.Mw / p.Ru;
+    k.k_q = p.Mw * d.esa / (p.Ru * d.rhoa);
+    int iterations = 0, flag = 0;
+    double v1a = vec1[0], v1b = vec1[1];
+    vec2[0] = 0.0;
+    vec2[1] = 0.0;
+    while (iterations < 50) {
+        iterations++;
+        double fv[2], J[4];
+        resid_jac_ad(p, d, k, v1a, v1b, fv, J);
+        const double det = J[0] * J[3] - J[2] * J[1];
+        if (fabs(det) < 1.0e-5) { flag = 1; break; }
+        const double rd = 1.0 / det;
+        const double c1 = (J[3] * fv[0] - J[2] * fv[1]) * rd;
+        const double c2 = (J[0] * fv[1] - J[1] * fv[0]) * rd;
+        vec2[0] = v1a - c1;
+        vec2[1] = v1b - c2;
+        int counts = 0;
+        double relax = 1.0;
+        while ((vec2[0] < 0) || (vec2[1] < 0) || ntlp_isnan(vec2[0])) {
+            counts++;
+            relax = relax * 0.5;
+            vec2[0] = v1a - c1 * relax;
+            vec2[1] = v1b - c2 * relax;
+            if (counts > 10) break;
+        }
+        if (vec2[0] < 0.01 || vec2[1] < 0.01 || ntlp_isnan(vec2[0]) || ntlp_isnan(vec2[1])) { flag = 1; break; }
+        if (sqrt(c1 * c1 + c2 * c2) < 1.0e-8) break;
+        v1a = vec2[0];
+        v1b = vec2[1];
+    }
+    if (iterations == 50) flag = 1;
+    if (ntlp_isnan(vec2[0]) || vec2[0] < 0 || ntlp_isnan(vec2[1]) || vec2[1] < 0) flag = 1;
+    return flag;
+}
+
 // LV_solver, particles.f90:4143-4223
 __device__ int lv_solver64(const DevParams &p, const Drop &d, const double vec1[2], double vec2[2]) {
     int iterations = 0, flag = 0;
@@ -283,6 +393,33 @@ __device__ __forceinline__ void fx_add(long long *limbs, double v) {
         long long add = neg ? -(long long)parts[k] : (long long)parts[k];
         atomicAdd((unsigned long long *)&limbs[L + k], (unsigned long long)add);
     }
+}
+
+// add_histogram / add_histogram_integer (particles.f90:4932-5009): the
+// weights are integers (mult, or 1), so the bins are exact int64 sums
+__device__ __forceinline__ void hist_add(const DevBox &B, const DevParams &p, int kind, double axis_value,
+                                        long long w) {
+    if (B.hist == nullptr) return;
+    const int b = ntlp_hist_bin(p.hb[kind], axis_value);
+    atomicAdd((unsigned long long *)&B.hist[kind * NTLP_HIST_N + b], (unsigned long long)w);
+}
+
+// what particle_bcs_nonperiodic records for a droplet it kills at the
+// bottom wall (particles.f90:2733-2753): residence time, activated
+// residence time (if activated), activation count, radius, and the
+// surface precipitation at its (unwrapped) column
+__device__ __forceinline__ void record_kill(const DevBox &B, const DevParams &p, const double x[3], double radius,
+                                            double rc, double res, double actres, double numact,
+                                            long long mult) {
+    hist_add(B, p, NTLP_H_RES, ntlp_log10(res), mult);
+    if (radius > rc) hist_add(B, p, NTLP_H_ACTTODEATH, ntlp_log10(actres), mult);
+    hist_add(B, p, NTLP_H_NUMACT, numact, 1);
+    hist_add(B, p, NTLP_H_RADDEATH, ntlp_log10(radius), mult);
+    const DevGrid &g = B.g;
+    const int ipt = ijpt(x[0], g.dx), jpt = ijpt(x[1], g.dy);
+    if (B.precip_fx != nullptr && ipt >= 1 && ipt <= g.nnx && jpt >= 1 && jpt <= g.nny)
+        fx_add(B.precip_fx + ((long long)(ipt - 1) + (long long)g.nnx * (jpt - 1)) * kFluxLimbs,
+               (double)mult * (p.rhow * 2.0 / 3.0 * p.pi2 * cube(radius)));
 }
 
 // particle_bcs_nonperiodic (reflect/kill) + particle_bcs_periodic for one
@@ -487,7 +624,7 @@ __device__ __forceinline__ int be_body(const DevBox &B, const DevParams &p, cons
         D.t0r = taup0 / radius;
         D.rt0 = radius / taup0;
         D.t0T = taup0 / Tp;
-        int flag = gauss_newton64(p, D, rt_start, rtz);
+        int flag = MIXED ? gauss_newton_ad(p, D, rt_start, rtz) : gauss_newton64(p, D, rt_start, rtz);
         if (flag == 1) {
             if (!ALLOW_LM) {
                 B.defer[atomicAdd(B.ndefer, 1)] = t;
@@ -537,6 +674,7 @@ __device__ __forceinline__ int be_body(const DevBox &B, const DevParams &p, cons
     if (solved) {
         if (radius > rc && radius * rtz[0] < rc) {
             dc.v[C_DENUM]++;
+            hist_add(B, p, NTLP_H_ACTRES, ntlp_log10(actres), multi);
         } else if (radius < rc && radius * rtz[0] > rc) {
             dc.v[C_ACTNUM]++;
             numact = numact + 1.0;
@@ -568,13 +706,13 @@ __device__ __forceinline__ int be_body(const DevBox &B, const DevParams &p, cons
         int fluxloc, fluxloci;
         if (x[2] > g.zl) {
             fluxloc = g.nnz + 1;
-            fluxloci = minloc_gt(g.z, g.nz2, xp3i) - 1;
+            fluxloci = minloc_z(g, xp3i) - 1;
         } else if (x[2] < 0.0) {
-            fluxloci = minloc_gt(g.z, g.nz2, xp3i) - 1;
+            fluxloci = minloc_z(g, xp3i) - 1;
             fluxloc = 0;
         } else {
-            fluxloc = minloc_gt(g.z, g.nz2, x[2]) - 1;
-            fluxloci = minloc_gt(g.z, g.nz2, xp3i) - 1;
+            fluxloc = minloc_z(g, x[2]) - 1;
+            fluxloci = minloc_z(g, xp3i) - 1;
         }
         int lo = 0, hi = -1;
         double sgn = 0.0;
@@ -607,6 +745,7 @@ __device__ __forceinline__ int be_body(const DevBox &B, const DevParams &p, cons
     if (!alive) {
         key = (int)B.g.ncells + 1;
         dc.v[C_DESTROY]++;
+        record_kill(B, p, x, radius, rc, res, actres, numact, multi);
     } else {
         int ipt, jpt, kpt;
         key = cell_key(B.g, x[0], x[1], x[2], &ipt, &jpt, &kpt);

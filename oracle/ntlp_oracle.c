@@ -19,6 +19,7 @@
 #endif
 
 #include "../ntlp_b200/csrc/ntlp_math.h"
+#include "../ntlp_b200/csrc/ntlp_hist.h"
 
 #ifdef ORACLE_LIBM
 #define M_EXP(x) exp(x)
@@ -36,6 +37,14 @@
 
 double oracle_m_exp(double x) { return M_EXP(x); }
 double oracle_m_log(double x) { return M_LOG(x); }
+double oracle_m_log10(double x) { return ntlp_log10(x); }
+int oracle_hist_bin(int kind, double axis_value) {
+    /* kinds NTLP_H_* of the step histograms, 5 = hist_rad (bins_rad) */
+    ntlp_hbins hb = kind == NTLP_H_NUMACT ? ntlp_hist_int_bins(0.0)
+                  : (kind == NTLP_H_RADDEATH || kind == 5) ? ntlp_hist_log_bins(1.0e-8, 1.0e-3)
+                  : ntlp_hist_log_bins(1.0e-1, 1.0e4);
+    return ntlp_hist_bin(hb, axis_value);
+}
 double oracle_m_pow(double x, double y) { return M_POW(x, y); }
 double oracle_m_acos(double x) { return M_ACOS(x); }
 double oracle_m_cos(double x) { return M_COS(x); }
@@ -694,9 +703,51 @@ static void droplet_arrays(ntlp_droplets *d, double *dp[NFIELDS_D]) {
     while (k < NFIELDS_D) dp[k++] = NULL;
 }
 
-/* particle_bcs_nonperiodic (reflect / kill; the dead-droplet histograms,
- * surface precipitation map and re-injection branches are not part of the
- * step) followed by particle_bcs_periodic.  Returns survivors; compacts.  */
+/* Histograms the step accumulates (hist_actres at deactivation, :3162-3164;
+ * hist_res, hist_acttodeath, hist_numact, hist_raddeath and surf_precip at
+ * the bottom-wall kill, :2733-2753), when a sink is set.  The sink is
+ * process-wide test state; the OpenMP step never writes it.               */
+static double *g_hist = NULL;        /* [5][514] */
+static double *g_precip = NULL;      /* (1:nnx, 1:nny) column-major */
+static ntlp_hbins g_hb[NTLP_H_STEP_KINDS];
+
+void oracle_set_step_hist(double *hist, double *surf_precip) {
+    g_hist = hist;
+    g_precip = surf_precip;
+    /* set_binsdata calls of particles.f90:1909-1921 */
+    g_hb[NTLP_H_ACTRES] = ntlp_hist_log_bins(1.0e-1, 1.0e4);
+    g_hb[NTLP_H_RES] = ntlp_hist_log_bins(1.0e-1, 1.0e4);
+    g_hb[NTLP_H_ACTTODEATH] = ntlp_hist_log_bins(1.0e-1, 1.0e4);
+    g_hb[NTLP_H_NUMACT] = ntlp_hist_int_bins(0.0);
+    g_hb[NTLP_H_RADDEATH] = ntlp_hist_log_bins(1.0e-8, 1.0e-3);
+}
+
+/* add_histogram (val1 given as log10(val1)) / add_histogram_integer */
+static void hist_add(int kind, double axis_value, double w) {
+    if (!g_hist) return;
+    int b = ntlp_hist_bin(g_hb[kind], axis_value);
+    g_hist[kind * NTLP_HIST_N + b] = g_hist[kind * NTLP_HIST_N + b] + w;
+}
+
+static void record_kill(const ntlp_grid *g, const ntlp_params *p, const ntlp_droplets *d, int64_t i) {
+    if (!g_hist) return;
+    double mult = (double)d->mult[i];
+    hist_add(NTLP_H_RES, ntlp_log10(d->res[i]), mult);
+    if (d->radius[i] > d->rc[i]) hist_add(NTLP_H_ACTTODEATH, ntlp_log10(d->actres[i]), mult);
+    hist_add(NTLP_H_NUMACT, d->numact[i], 1.0);
+    hist_add(NTLP_H_RADDEATH, ntlp_log10(d->radius[i]), mult);
+    double dx = g->xl / g->nnx, dy = g->yl / g->nny;
+    int ipt = (int)floor(d->xp[0][i] / dx) + 1;
+    int jpt = (int)floor(d->xp[1][i] / dy) + 1;
+    if (g_precip && ipt >= 1 && ipt <= g->nnx && jpt >= 1 && jpt <= g->nny) {
+        double *sp = &g_precip[(ipt - 1) + (int64_t)g->nnx * (jpt - 1)];
+        *sp = *sp + mult * (p->rhow * 2.0 / 3.0 * p->pi2 * cube(d->radius[i]));
+    }
+}
+
+/* particle_bcs_nonperiodic (reflect / kill, with what the kill records;
+ * the re-injection branches are not part of the step) followed by
+ * particle_bcs_periodic.  Returns survivors; compacts.                    */
 static int64_t apply_bcs(const ntlp_grid *g, const ntlp_params *p,
                          ntlp_droplets *d, int64_t *num_destroy) {
     double *dp[NFIELDS_D];
@@ -715,6 +766,7 @@ static int64_t apply_bcs(const ntlp_grid *g, const ntlp_params *p,
                 d->xp[2][i] = bot + (bot - d->xp[2][i]);
                 d->vp[2][i] = -d->vp[2][i];
             } else {
+                record_kill(g, p, d, i);
                 keep = 0;
                 killed++;
             }
@@ -833,6 +885,7 @@ static void be_one(gridc *c, const ntlp_params *p, const oracle_fields *f,
         }
         if (radius > rc && radius * rt_zeroes[0] < rc) {
             k->denum++;
+            hist_add(NTLP_H_ACTRES, ntlp_log10(d->actres[i]), (double)d->mult[i]);
         } else if (radius < rc && radius * rt_zeroes[0] > rc) {
             k->actnum++;
             d->numact[i] = d->numact[i] + 1.0;
@@ -1305,4 +1358,96 @@ int oracle_step_be_omp(const ntlp_grid *g, const ntlp_params *p,
     for (int t = 0; t < nthreads; ++t) free_prefold(S + 6 * t);
     free(S);
     return 0;
+}
+
+
+/* ------------------------------------------------------------------------ */
+/* particle_xy_stats (particles.f90:3370-3770) and radius_histogram          */
+/* (:5011-5021), list order, one domain                                      */
+/* ------------------------------------------------------------------------ */
+void oracle_stats(const ntlp_grid *g, const ntlp_params *p, const ntlp_droplets *d, ntlp_stats0 *s0,
+                  int maxnz, double *levels, double *lwp) {
+    const double pi2 = p->pi2;
+    int64_t numpart = 0, numdrop = 0, numaerosol = 0;
+    double myradavg = 0.0, myradmsqr = 0.0, myradmin = 1000.0, myradmax = 0.0;
+    double mytempmin = 1000.0, mytempmax = 0.0, myqmin = 1000.0, myqmax = 0.0;
+    double vpmin[3] = {1000.0, 1000.0, 1000.0}, vpmax[3] = {-1000.0, -1000.0, -1000.0};
+    double myRep_avg = 0.0, mywmass = 0.0, mypmass = 0.0, mypvol = 0.0;
+    for (int64_t i = 0; i < d->n; ++i) {
+        numpart = numpart + 1;
+        if (d->radius[i] > d->rc[i]) numdrop = numdrop + 1;
+        else numaerosol = numaerosol + 1;
+        double r = d->radius[i];
+        myradavg = myradavg + r;
+        myradmsqr = myradmsqr + r * r;
+        myradmax = fmax(myradmax, r);
+        myradmin = fmin(myradmin, r);
+        mytempmax = fmax(mytempmax, d->Tp[i]);
+        mytempmin = fmin(mytempmin, d->Tp[i]);
+        myqmax = fmax(myqmax, d->qinf[i]);
+        myqmin = fmin(myqmin, d->qinf[i]);
+        for (int a = 0; a < 3; ++a) {
+            vpmin[a] = fmin(vpmin[a], d->vp[a][i]);
+            vpmax[a] = fmax(vpmax[a], d->vp[a][i]);
+        }
+        double Volp = pi2 * 2.0 / 3.0 * cube(r);
+        double rhop = (d->m_s[i] + Volp * p->rhow) / Volp;
+        double d0 = d->vp[0][i] - d->uf[0][i], d1 = d->vp[1][i] - d->uf[1][i], d2 = d->vp[2][i] - d->uf[2][i];
+        double diffnorm = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+        double Rep = 2.0 * r * diffnorm / p->nuf;
+        myRep_avg = myRep_avg + Rep;
+        mywmass = mywmass + Volp * p->rhow;
+        mypmass = mypmass + Volp * rhop;
+        mypvol = mypvol + Volp;
+    }
+    if (s0) {
+        s0->numpart = numpart; s0->numdrop = numdrop; s0->numaerosol = numaerosol;
+        s0->Rep_sum = myRep_avg; s0->wmass = mywmass; s0->pmass = mypmass; s0->pvol = mypvol;
+        s0->rad_sum = myradavg; s0->rad2_sum = myradmsqr;
+        s0->radmax = myradmax; s0->tempmax = mytempmax; s0->qmax = myqmax;
+        s0->radmin = myradmin; s0->tempmin = mytempmin; s0->qmin = myqmin;
+        for (int a = 0; a < 3; ++a) { s0->vpmax[a] = vpmax[a]; s0->vpmin[a] = vpmin[a]; }
+    }
+    const double pi = p->pi2 * 0.5;   /* pi2 = 2*(4*atan(1)) (les.F), so this is 4*atan(1) */
+    const double dx = g->xl / g->nnx, dy = g->yl / g->nny;
+    const int nz2 = g->nnz + 2;
+    if (levels) memset(levels, 0, sizeof(double) * (size_t)maxnz * NTLP_STATS_LEVEL_QTYS);
+    if (lwp) memset(lwp, 0, sizeof(double) * (size_t)g->nnx * g->nny);
+    for (int64_t i = 0; i < d->n; ++i) {
+        int ipt = (int)floor(d->xp[0][i] / dx) + 1;
+        int jpt = (int)floor(d->xp[1][i] / dy) + 1;
+        int kpt = minloc_gt(g->z, nz2, d->xp[2][i]) - 1;
+        double r = d->radius[i], Tp = d->Tp[i], mult = (double)d->mult[i];
+        double v1 = d->vp[0][i], v2 = d->vp[1][i], v3 = d->vp[2][i];
+        double u1 = d->uf[0][i], u2 = d->uf[1][i], u3 = d->uf[2][i];
+        if (levels && kpt >= 1 && kpt <= maxnz) {
+            double val[NTLP_STATS_LEVEL_QTYS] = {
+                1.0, v1, v2, v3, v1 * v1, v2 * v2, v3 * v3, v1 * v3, u1, u2, u3, u1 * u1, u2 * u2, u3 * u3,
+                Tp, Tp * Tp, d->Tf[i], r, r * r, d->qinf[i], Tp * v3, mult,
+                mult * (p->rhow * 4.0 / 3.0 * pi * cube(r)), d->qstar[i]};
+            for (int q = 0; q < NTLP_STATS_LEVEL_QTYS; ++q) {
+                double *c = &levels[(size_t)q * maxnz + (kpt - 1)];
+                *c = *c + val[q];
+            }
+        }
+        if (lwp) {
+            /* ipt = nnx+1 / jpt = nny+1 (exactly at x = xl / y = yl) go to
+             * their periodic image (the reference indexes past LWP)       */
+            if (ipt == g->nnx + 1) ipt = 1;
+            if (jpt == g->nny + 1) jpt = 1;
+            if (ipt >= 1 && ipt <= g->nnx && jpt >= 1 && jpt <= g->nny) {
+                double *c = &lwp[(ipt - 1) + (size_t)g->nnx * (jpt - 1)];
+                *c = *c + mult * (p->rhow * 4.0 / 3.0 * pi * cube(r));
+            }
+        }
+    }
+}
+
+void oracle_radius_histogram(const ntlp_droplets *d, double *hist) {
+    ntlp_hbins hb = ntlp_hist_log_bins(1.0e-8, 1.0e-3);
+    for (int b = 0; b < NTLP_HIST_N; ++b) hist[b] = 0.0;
+    for (int64_t i = 0; i < d->n; ++i) {
+        int b = ntlp_hist_bin(hb, ntlp_log10(d->radius[i]));
+        hist[b] = hist[b] + (double)d->mult[i];
+    }
 }

@@ -106,6 +106,9 @@ void oracle_bin(const ntlp_grid *g, int64_t n, const double *x,
 /* Elementary functions, exported so tests can compare them with libm. */
 double oracle_m_exp(double x);
 double oracle_m_log(double x);
+double oracle_m_log10(double x);
+/* 0-based bin of a value on a histogram's axis (kinds NTLP_H_*, 5 = hist_rad) */
+int oracle_hist_bin(int kind, double axis_value);
 double oracle_m_pow(double x, double y);
 double oracle_m_acos(double x);
 double oracle_m_cos(double x);
@@ -117,6 +120,16 @@ int oracle_step_be_omp(const ntlp_grid *g, const ntlp_params *p,
                        const oracle_fields *f, ntlp_droplets *d, double dt,
                        int it, ntlp_counters *c, double *src[6], int nthreads);
 int oracle_max_threads(void);
+
+/* Step histograms sink (hist: [5][514], surf_precip: (1:nnx,1:nny)); NULL
+ * disables.  Serial steps only.                                            */
+void oracle_set_step_hist(double *hist, double *surf_precip);
+/* particle_xy_stats sums in list order: 0th order, statsvec1(1:maxnz,1:24)
+ * column-major, LWP(1:nnx,1:nny) column-major (any may be NULL).          */
+void oracle_stats(const ntlp_grid *g, const ntlp_params *p, const ntlp_droplets *d, ntlp_stats0 *s0,
+                  int maxnz, double *levels, double *lwp);
+/* radius_histogram: hist_rad(1:514) */
+void oracle_radius_histogram(const ntlp_droplets *d, double *hist);
 
 #ifdef __cplusplus
 }

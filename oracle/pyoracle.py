@@ -61,7 +61,7 @@ def lib(variant: str = "ntlp") -> C.CDLL:
     L.oracle_newton.restype = C.c_int
     L.oracle_mod_magnus.argtypes = [C.c_double]
     L.oracle_mod_magnus.restype = C.c_double
-    for fn in ("oracle_m_exp", "oracle_m_log", "oracle_m_acos", "oracle_m_cos"):
+    for fn in ("oracle_m_exp", "oracle_m_log", "oracle_m_log10", "oracle_m_acos", "oracle_m_cos"):
         getattr(L, fn).argtypes = [C.c_double]
         getattr(L, fn).restype = C.c_double
     L.oracle_m_pow.argtypes = [C.c_double, C.c_double]
@@ -69,6 +69,12 @@ def lib(variant: str = "ntlp") -> C.CDLL:
     L.oracle_step_be_omp.argtypes = [P(abi.NtlpGrid), P(abi.NtlpParams), C.c_void_p, P(abi.NtlpDroplets),
                                      C.c_double, C.c_int, P(abi.NtlpCounters), C.POINTER(_dp), C.c_int]
     L.oracle_max_threads.restype = C.c_int
+    L.oracle_set_step_hist.argtypes = [_dp, _dp]
+    L.oracle_stats.argtypes = [P(abi.NtlpGrid), P(abi.NtlpParams), P(abi.NtlpDroplets), P(abi.NtlpStats0),
+                               C.c_int, _dp, _dp]
+    L.oracle_radius_histogram.argtypes = [P(abi.NtlpDroplets), _dp]
+    L.oracle_hist_bin.argtypes = [C.c_int, C.c_double]
+    L.oracle_hist_bin.restype = C.c_int
     _libs[variant] = L
     return L
 
@@ -150,6 +156,38 @@ class Oracle:
         self.L.oracle_bin(C.byref(self.g), n, abi.as_dptr(x), abi.as_dptr(y), abi.as_dptr(z),
                           *(a.ctypes.data_as(C.POINTER(C.c_int32)) for a in o))
         return o
+
+    def step_histograms_on(self):
+        """Start collecting the step histograms (hist_actres, hist_res,
+        hist_acttodeath, hist_numact, hist_raddeath) and surf_precip of the
+        serial steps; returns the (hist (5, 514), surf_precip (nny, nnx))
+        arrays that the following steps add to."""
+        g = self.grid_d
+        self._hist = np.zeros((5, abi.NTLP_HIST_BINS))
+        self._precip = np.zeros((g["nny"], g["nnx"]))       # (1:nnx,1:nny) column-major
+        self.L.oracle_set_step_hist(abi.as_dptr(self._hist), abi.as_dptr(self._precip))
+        return self._hist, self._precip
+
+    def step_histograms_off(self):
+        self.L.oracle_set_step_hist(None, None)
+
+    def stats(self, d: dict, maxnz: int | None = None):
+        """particle_xy_stats sums: (stats0 dict, levels (24, maxnz), lwp (nny, nnx))."""
+        g = self.grid_d
+        maxnz = g["nnz"] if maxnz is None else maxnz
+        s = abi.make_droplets_struct(d)
+        s0 = abi.NtlpStats0()
+        levels = np.zeros((abi.NTLP_STATS_LEVEL_QTYS, maxnz))
+        lwp = np.zeros((g["nny"], g["nnx"]))
+        self.L.oracle_stats(C.byref(self.g), C.byref(self.p), C.byref(s), C.byref(s0), maxnz,
+                            abi.as_dptr(levels), abi.as_dptr(lwp))
+        return s0.as_dict(), levels, lwp
+
+    def radius_histogram(self, d: dict):
+        s = abi.make_droplets_struct(d)
+        h = np.zeros(abi.NTLP_HIST_BINS)
+        self.L.oracle_radius_histogram(C.byref(s), abi.as_dptr(h))
+        return h
 
     def crit_radius(self, m_s, kappa_s, T):
         return np.array([self.L.oracle_crit_radius(C.byref(self.p), a, b, c)

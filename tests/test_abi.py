@@ -45,6 +45,7 @@ def test_struct_sizes_match_header_layout():
     # the ABI structs are plain C: sizes follow from their fields
     assert C.sizeof(abi.NtlpGrid) == 4 * 4 + 3 * 8 + 4 * 8
     assert C.sizeof(abi.NtlpCounters) == 8 * 8
+    assert C.sizeof(abi.NtlpStats0) == 3 * 8 + 6 * 8 + 2 * 6 * 8
     assert C.sizeof(abi.NtlpDroplets) == 8 + 15 * 8 + 8 * 8 + 6 * 8 + 3 * 8 + 2 * 8 + 8 + 8
 
 
