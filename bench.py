@@ -329,7 +329,6 @@ def run_serving(args):
     import torch
     from ntlp_b200 import serving
     eng = serving.CudaEngine(dt=1e-3, priorities=bool(args.serve_priorities))
-    calib = eng.calibrate()
     jobs = serving.draw_jobs(args.serve_jobs, rate=args.serve_rate, seed=4)
     eng.stage(jobs)
     server = serving.Server(eng, hbm_budget=args.hbm_budget, max_active_droplets=args.serve_work_cap,
@@ -338,6 +337,10 @@ def run_serving(args):
     clk.start()
     rep = server.run(jobs, realtime=True, time_limit=600)
     clocks = clk.stop()
+    torch.cuda.empty_cache()
+    # the same jobs one at a time: per-step slowdowns and result equality
+    eng.stage(jobs)
+    cmp = serving.compare_alone(rep, eng.replay_alone(jobs))
     torch.cuda.empty_cache()
     spots = [r["result"]["spot_check"] for r in rep["records"] if "spot_check" in r["result"]]
     offered = sum(j.n * j.steps for j in jobs) / max(jobs[-1].arrival, 1e-9)
@@ -349,10 +352,12 @@ def run_serving(args):
             "job_ms_p50": rep["job_ms_p50"], "job_ms_p99": rep["job_ms_p99"],
             "admission_wait_ms_p50": rep["wait_ms_p50"], "admission_wait_ms_p99": rep["wait_ms_p99"],
             "ingest_ms_p50": rep["ingest_ms_p50"], "ingest_ms_p99": rep["ingest_ms_p99"],
-            "step_slowdown_p50": rep["step_slowdown_p50"], "step_slowdown_p99": rep["step_slowdown_p99"],
+            "step_slowdown_p50": cmp["step_slowdown_p50"], "step_slowdown_p99": cmp["step_slowdown_p99"],
+            "step_slowdown_p99_by_size": cmp["step_slowdown_p99_by_size"],
+            "alone_step_ms_p50": cmp["alone_step_ms_p50"], "alone_step_ms_p99": cmp["alone_step_ms_p99"],
+            "results_equal_alone_and_mix": cmp["results_equal_alone_and_mix"],
             "peak_admitted_bytes": rep["peak_bytes"], "hbm_budget": args.hbm_budget,
             "peak_active_jobs": rep["peak_active"], "work_cap_droplets": args.serve_work_cap,
-            "alone_step_calibration_ms": [[e, n, round(t, 4)] for e, n, t in calib],
             "spot_checks": spots, "clocks": clocks}
 
 

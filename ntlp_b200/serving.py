@@ -205,12 +205,6 @@ class Server:
         ingest_ms = [1e3 * (r["ready"] - r["admitted"]) for r in records]
         updates = sum(r["n"] * r["steps"] for r in records)
         span = max(t_end - first_arrival, 1e-9)
-        slow = []
-        model = getattr(self.engine, "alone_ms", None)
-        for r in records:
-            base = model(r["edge"], r["n"]) if model is not None else None
-            if base:
-                slow.extend(ms / base for ms in r["step_ms"])
         return dict(
             jobs=len(records), rejected=rejected, admit_order=admit_order,
             droplet_updates=int(updates), wall_s=span, throughput=updates / span,
@@ -219,10 +213,30 @@ class Server:
             job_ms_p50=percentile(job_ms, 50), job_ms_p99=percentile(job_ms, 99),
             wait_ms_p50=percentile(wait_ms, 50), wait_ms_p99=percentile(wait_ms, 99),
             ingest_ms_p50=percentile(ingest_ms, 50), ingest_ms_p99=percentile(ingest_ms, 99),
-            step_slowdown_p50=percentile(slow, 50), step_slowdown_p99=percentile(slow, 99),
             peak_bytes=int(peak_bytes), peak_active=int(peak_active),
             records=records,
         )
+
+
+def compare_alone(report: dict, alone: dict) -> dict:
+    """Per-step slowdown (a step's time in the mix over the same step of
+    the same job run alone) and whether every job's counters and droplet
+    count are the same alone and in the mix."""
+    slow, by_class = [], {"<2e5": [], "2e5-2e6": [], ">=2e6": []}
+    equal = True
+    for r in report["records"]:
+        ms_alone, res_alone = alone[r["jid"]]
+        cls = "<2e5" if r["n"] < 200_000 else ("2e5-2e6" if r["n"] < 2_000_000 else ">=2e6")
+        for a, b in zip(r["step_ms"], ms_alone):
+            slow.append(a / b)
+            by_class[cls].append(a / b)
+        equal = equal and res_alone["counters"] == r["result"]["counters"] and \
+            res_alone["numpart"] == r["result"]["numpart"]
+    return dict(step_slowdown_p50=percentile(slow, 50), step_slowdown_p99=percentile(slow, 99),
+                step_slowdown_p99_by_size={k: percentile(v, 99) for k, v in by_class.items()},
+                alone_step_ms_p50=percentile([m for ms, _ in alone.values() for m in ms], 50),
+                alone_step_ms_p99=percentile([m for ms, _ in alone.values() for m in ms], 99),
+                results_equal_alone_and_mix=bool(equal))
 
 
 class CudaEngine:
@@ -246,7 +260,6 @@ class CudaEngine:
         lo, hi = torch.cuda.Stream.priority_range()   # (lowest, highest); numerically hi <= lo
         self._prio = (lo, hi)
         self._local = threading.local()
-        self._coef = None
         self._payload: dict = {}
 
     # -- sizes --
@@ -381,30 +394,19 @@ class CudaEngine:
             st["twin"][0].close()
         st["ctx"].close()
 
-    # -- alone-step model for slowdown figures --
-    def calibrate(self, shapes=((32, 10_000), (64, 100_000), (128, 1_000_000), (192, 10_000_000),
-                                (192, 10_000), (48, 3_000_000)), steps: int = 4) -> list:
-        """Time steps of single jobs running alone and fit
-        ms = a + b * droplets + c * cells (least squares, non-negative)."""
-        rows = []
-        for i, (edge, n) in enumerate(shapes):
-            job = JobSpec(jid=-1 - i, arrival=0.0, edge=edge, n=n, median=3e-6, steps=steps, seed=1000 + i)
-            st = self.prepare(job)
+    # -- the same jobs alone, for slowdowns and the alone/mix equality --
+    def replay_alone(self, jobs: list) -> dict:
+        """Run every job by itself (one at a time, each step waited for) on
+        the same inputs: {jid: (step ms list, result)}.  Spot-check twins
+        are not run again."""
+        out = {}
+        for job in jobs:
+            solo = JobSpec(**{**job.__dict__, "spot_check": False})
+            st = self.prepare(solo)
             ms = []
-            for k in range(steps):
+            for k in range(solo.steps):
                 ev = self.issue_step(st, k)
                 ev[1].synchronize()
                 ms.append(self.step_ms(ev))
-            self.finish(st)
-            rows.append((edge, n, float(np.median(ms[1:]))))
-        A = np.array([[1.0, n, (e + 1) ** 3] for e, n, _ in rows])
-        y = np.array([t for _, _, t in rows])
-        coef = np.linalg.lstsq(A, y, rcond=None)[0]
-        self._coef = np.maximum(coef, 0.0)
-        return rows
-
-    def alone_ms(self, edge: int, n: int) -> float | None:
-        if self._coef is None:
-            return None
-        a, b, c = self._coef
-        return float(max(a + b * n + c * (edge + 1) ** 3, 1e-3))
+            out[job.jid] = (ms, self.finish(st))
+        return out
