@@ -47,6 +47,11 @@ import time
 
 import numpy as np
 
+# Many streams run concurrently in the serving loop; give each its own
+# hardware work queue (the default of 8 makes streams share queues and
+# wait on one another's kernels).  Must be set before CUDA starts.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -83,6 +88,8 @@ def parse():
     ap.add_argument("--hbm-budget", type=float, default=150e9)
     ap.add_argument("--serve-depth", type=int, default=2)
     ap.add_argument("--serve-priorities", type=int, default=1)
+    ap.add_argument("--serve-max-large", type=int, default=1)
+    ap.add_argument("--serve-ingest-priority", choices=["job", "high"], default="high")
     ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
                     help="run one precision only (profiling)")
     return ap.parse_args()
@@ -328,11 +335,13 @@ def run_serving(args):
     mixed precision with an FP64 spot check on 1% of jobs."""
     import torch
     from ntlp_b200 import serving
-    eng = serving.CudaEngine(dt=1e-3, priorities=bool(args.serve_priorities))
+    eng = serving.CudaEngine(dt=1e-3, priorities=bool(args.serve_priorities),
+                             ingest_priority=args.serve_ingest_priority)
     jobs = serving.draw_jobs(args.serve_jobs, rate=args.serve_rate, seed=4)
     eng.stage(jobs)
     server = serving.Server(eng, hbm_budget=args.hbm_budget, max_active_droplets=args.serve_work_cap,
-                            depth=args.serve_depth)
+                            depth=args.serve_depth,
+                            max_large=args.serve_max_large if args.serve_max_large > 0 else None)
     clk = ClockSampler()
     clk.start()
     rep = server.run(jobs, realtime=True, time_limit=600)

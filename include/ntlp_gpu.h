@@ -210,7 +210,7 @@ int ntlp_box_sources(ntlp_ctx *ctx, int32_t box, int32_t layout, double *partsrc
  * rule vp = uf belongs to an eagerly run first step).  Returns when queued. */
 int ntlp_advance_graph(ntlp_ctx *ctx, double dt, int32_t it, int32_t nsteps);
 /* Autotuner: times each deposition tile shape (NTLP_TUNE_VARIANTS of them:
- * 2x4x32, 4x4x16, 2x2x64 nodes) and each droplet block size (128, 256) on
+ * 2x4x32, 4x4x16, 2x2x64 nodes) and each interpolation block size (128, 256) on
  * this context's boxes over `steps` steps (state advances), keeps the
  * fastest, and reports the per-variant milliseconds per step (ms[i] for
  * deposition shape i, ms[3+j] for block size j).                          */

@@ -810,7 +810,8 @@ int launch_step(ntlp_ctx *c, int kind, int istage, double dt, int32_t it, bool w
     if (kind == 1) {
         if (c->params.precision == NTLP_PREC_MIXED)
             launch_update_be_mixed(c->params.ilin, nt, c->box_d, c->drop_tiles_d[c->nt_variant],
-                                   c->n_drop_tiles[c->nt_variant], c->nbox, c->dp_d, in, c->stream);
+                                   c->n_drop_tiles[c->nt_variant], c->drop_tiles_d[0], c->n_drop_tiles[0], c->nbox,
+                                   c->dp_d, in, c->stream);
         else
             launch_update_be64(c->params.ilin, nt, c->box_d, c->drop_tiles_d[c->nt_variant],
                                c->n_drop_tiles[c->nt_variant], c->nbox, c->dp_d, in, c->stream);

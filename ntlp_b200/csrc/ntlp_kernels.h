@@ -45,8 +45,8 @@ void launch_deposit64(int variant, DevBox *boxes, const Tile *tiles, int ntiles,
                       cudaStream_t st);
 
 // mixed precision (ntlp_mixed.cu)
-void launch_update_be_mixed(int ilin, int nt, DevBox *boxes, const Tile *tiles, int ntiles, int nbox,
-                            const DevParams *pp, StepIn in, cudaStream_t st);
+void launch_update_be_mixed(int ilin, int nt, DevBox *boxes, const Tile *tiles, int ntiles, const Tile *tiles128,
+                            int ntiles128, int nbox, const DevParams *pp, StepIn in, cudaStream_t st);
 void launch_payload_mixed(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp, double dt,
                           cudaStream_t st);
 void launch_deposit_mixed(int variant, DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp,

@@ -214,8 +214,8 @@ k_interp_mixed(DevBox *boxes, const Tile *tiles) {
     B.key[t] = bad;
 }
 
-template <int NT>
-__global__ void __launch_bounds__(NT, 512 / NT)
+// 5 resident blocks of 128: 94 registers, 20 warps per SM, no spills
+__global__ void __launch_bounds__(128, 5)
 k_be_mixed(DevBox *boxes, const Tile *tiles, const DevParams *pp, StepIn in) {
     const Tile tl = tiles[blockIdx.x];
     const DevBox &B = boxes[tl.box];
@@ -239,18 +239,21 @@ k_be_defer_mixed(DevBox *boxes, const DevParams *pp, StepIn in) {
     block_add_counters(B, cnt);
 }
 
-void launch_update_be_mixed(int ilin, int nt, DevBox *boxes, const Tile *tiles, int ntiles, int nbox,
-                            const DevParams *pp, StepIn in, cudaStream_t st) {
+// The interpolation runs with the tuned block size nt; the droplet body
+// always runs 128-thread blocks over the 128-droplet tiles.  Its FP64
+// arithmetic may be contracted by the code generator, and one register
+// budget for every tuning choice keeps the results identical across them.
+void launch_update_be_mixed(int ilin, int nt, DevBox *boxes, const Tile *tiles, int ntiles, const Tile *tiles128,
+                            int ntiles128, int nbox, const DevParams *pp, StepIn in, cudaStream_t st) {
     if (ntiles <= 0) return;
     if (nt == 256) {
         if (ilin == 1) k_interp_mixed<1, 256><<<ntiles, 256, 0, st>>>(boxes, tiles);
         else k_interp_mixed<0, 256><<<ntiles, 256, 0, st>>>(boxes, tiles);
-        k_be_mixed<256><<<ntiles, 256, 0, st>>>(boxes, tiles, pp, in);
     } else {
         if (ilin == 1) k_interp_mixed<1, 128><<<ntiles, 128, 0, st>>>(boxes, tiles);
         else k_interp_mixed<0, 128><<<ntiles, 128, 0, st>>>(boxes, tiles);
-        k_be_mixed<128><<<ntiles, 128, 0, st>>>(boxes, tiles, pp, in);
     }
+    k_be_mixed<<<ntiles128, 128, 0, st>>>(boxes, tiles128, pp, in);
     k_be_defer_mixed<<<dim3(kDeferBlocks, nbox), kUpdateThreads, 0, st>>>(boxes, pp, in);
 }
 

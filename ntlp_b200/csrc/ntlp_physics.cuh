@@ -174,6 +174,7 @@ struct AdConst {
     double k_rep;    // 2 diffnorm / nuf
     double k_vol;    // (2/3) pi2
     double k_sol;    // c_sol / rhow
+    double k_solv;   // k_sol / k_vol
     double k_clat;   // 3 Lv / Cpp
     double k_g;      // 2 Mw Gam / (Ru rhow)
     double k_e1;     // Lv Mw / Ru
@@ -187,8 +188,9 @@ __device__ __forceinline__ void resid_jac_ad(const DevParams &p, const Drop &d, 
     const double irn = 1.0 / rn;
     // r-dependent part (derivatives with respect to a; drn/da = R)
     const double Rep = k.k_rep * rn;
-    const double sRep = sqrt(Rep);
-    const double sRep_a = sRep > 0.0 ? 0.5 * k.k_rep * R / sRep : 0.0;
+    const double isRep = Rep > 0.0 ? rsqrt(Rep) : 0.0;
+    const double sRep = Rep * isRep;
+    const double sRep_a = 0.5 * k.k_rep * R * isRep;
     const double Shp = 2.0 + 0.6 * sRep * p.Sc13, Shp_a = 0.6 * p.Sc13 * sRep_a;
     const double Nup = 2.0 + 0.6 * sRep * p.Pra13, Nup_a = 0.6 * p.Pra13 * sRep_a;
     const double rpre = k.k_rpre * Shp * irn;
@@ -197,7 +199,7 @@ __device__ __forceinline__ void resid_jac_ad(const DevParams &p, const Drop &d, 
     const double tpre = k.k_tpre * Nup * irn2;
     const double tpre_a = k.k_tpre * (Nup_a - 2.0 * Nup * R * irn) * irn2;
     const double clat = k.k_clat * irn, clat_a = -clat * R * irn;
-    const double solterm = k.k_sol / (k.k_vol * rn * rn * rn);
+    const double solterm = k.k_solv * (irn2 * irn);
     const double solterm_a = -3.0 * solterm * R * irn;
     const double g = k.k_g * irn, g_a = -g * R * irn;
     // T-dependent part (dTn/db = Tp)
@@ -231,6 +233,7 @@ __device__ int gauss_newton_ad(const DevParams &p, const Drop &d, const double v
     k.k_rep = 2.0 * d.diffnorm / p.nuf;
     k.k_vol = (2.0 / 3.0) * p.pi2;
     k.k_sol = d.c_sol / p.rhow;
+    k.k_solv = k.k_sol / k.k_vol;
     k.k_clat = 3.0 * p.Lv / p.Cpp;
     k.k_g = 2.0 * p.Mw * p.Gam / (p.Ru * p.rhow);
     k.k_e1 = p.Lv * p.Mw / p.Ru;
@@ -337,6 +340,36 @@ __device__ double rad_solver2_64(const DevParams &p, double Tf, double qinf, dou
         }
     }
     return guess;
+}
+
+// Mixed path: the same equilibrium guess in FP32.  It only starts the
+// Newton iteration, which then converges to the same root under the same
+// stopping rule; a branch that flips near M = 0 changes the start, not the
+// root.
+__device__ double rad_solver2_32(const DevParams &p, double Tf, double qinf, double rhoa, double m_s,
+                                 double kap, double radius, double esa, int &mflag) {
+    mflag = 0;
+    const float pi2 = (float)p.pi2;
+    const float lg = logf((float)((p.Ru * Tf * rhoa * qinf) / (p.Mw * esa)));
+    const float a = -(float)((2.0 * p.Mw * p.Gam) / (p.Ru * p.rhow * Tf)) / lg;
+    const float c = (float)((kap * m_s) / ((2.0 / 3.0) * p.pi2 * p.rhos)) / lg;
+    const float Q = (a * a) / 9.0f;
+    const float R = (2.0f * a * a * a + 27.0f * c) / 54.0f;
+    const float M = R * R - Q * Q * Q;
+    float guess;
+    if (M < 0.0f) {
+        const float theta = acosf(fminf(fmaxf(R / sqrtf(Q * Q * Q), -1.0f), 1.0f));
+        guess = -(2.0f * sqrtf(Q) * cosf((theta - pi2) / 3.0f)) - a / 3.0f;
+        if (guess < 0.0f) guess = -(2.0f * sqrtf(Q) * cosf((theta + pi2) / 3.0f)) - a / 3.0f;
+    } else {
+        const float S = -copysignf(1.0f, R) * cbrtf(fabsf(R) + sqrtf(M));
+        guess = S + Q / S - a / 3.0f;
+        if (guess < 0.0f) {
+            mflag = 1;
+            return radius;
+        }
+    }
+    return (double)guess;
 }
 
 __device__ __forceinline__ double taup0_64(const DevParams &p, double m_s, double rhoa) {
@@ -605,7 +638,8 @@ __device__ __forceinline__ int be_body(const DevBox &B, const DevParams &p, cons
         const double taup0 = taup0_64(p, m_s, rhoa);
         const double esa = mod_magnus64(Tf);
         int mflag;
-        double guess = rad_solver2_64(p, Tf, qinf, rhoa, m_s, kap, radius, esa, mflag);
+        double guess = MIXED ? rad_solver2_32(p, Tf, qinf, rhoa, m_s, kap, radius, esa, mflag)
+                             : rad_solver2_64(p, Tf, qinf, rhoa, m_s, kap, radius, esa, mflag);
         double rt_start[2];
         if (mflag == 0) { rt_start[0] = guess / radius; rt_start[1] = Tf / Tp; }
         else { rt_start[0] = 1.0; rt_start[1] = 1.0; }

@@ -12,6 +12,8 @@ Poisson stream; the server
 * builds each admitted job's box on the device on an ingest thread and
   keeps its fields and droplets resident in its own context for all of its
   steps (no host round trip between steps);
+* lets at most `max_large` large jobs run at once, so that the long kernels
+  of large jobs do not fill the GPU while small jobs wait;
 * keeps up to ``depth`` steps of every active job queued on that job's own
   CUDA stream, so steps of different jobs overlap on the device; smaller
   jobs get higher stream priority, so their short steps are not queued
@@ -94,7 +96,10 @@ class Server:
     """Continuous-batching scheduler over an engine (see module docstring)."""
 
     def __init__(self, engine, hbm_budget: float = 150e9, max_active: int = 64,
-                 max_active_droplets: float = 2e7, depth: int = 2, ingest_workers: int = 3):
+                 max_active_droplets: float = 2e7, depth: int = 2, ingest_workers: int = 3,
+                 max_large: int | None = 1, large: int = 2_000_000):
+        self.max_large = max_large      # cap on concurrently admitted jobs of >= `large` droplets
+        self.large = int(large)
         self.engine = engine
         self.budget = float(hbm_budget)
         self.max_active = int(max_active)
@@ -112,6 +117,7 @@ class Server:
         rejected: list = []
         used_bytes = 0
         used_drops = 0
+        n_large = 0
         peak_bytes = 0
         peak_active = 0
         admit_order: list = []
@@ -134,6 +140,8 @@ class Server:
                     b = eng.job_bytes(job)
                     fits_mem = used_bytes + b <= self.budget
                     fits_work = used_drops + job.n <= self.max_drops or (used_drops == 0)
+                    if self.max_large is not None and job.n >= self.large and n_large >= self.max_large:
+                        fits_work = False
                     if not (fits_mem and fits_work):
                         if b > self.budget:
                             queue.popleft()
@@ -143,6 +151,7 @@ class Server:
                     queue.popleft()
                     used_bytes += b
                     used_drops += job.n
+                    n_large += job.n >= self.large
                     peak_bytes = max(peak_bytes, used_bytes)
                     admit_order.append(job.jid)
                     fut = pool.submit(eng.prepare, job)
@@ -174,6 +183,7 @@ class Server:
                         t_done = time.perf_counter() - t0
                         used_bytes -= a.nbytes
                         used_drops -= a.spec.n
+                        n_large -= a.spec.n >= self.large
                         records.append(dict(jid=a.spec.jid, n=a.spec.n, edge=a.spec.edge, steps=a.spec.steps,
                                             arrival=a.spec.arrival, admitted=a.admitted, ready=a.ready,
                                             done=t_done, step_ms=a.step_ms, result=result,
@@ -244,7 +254,7 @@ class CudaEngine:
     (one box) per job, mixed precision; spot-check jobs get an FP64 twin."""
 
     def __init__(self, params: dict | None = None, dt: float = 1e-3, keep_state: bool = False,
-                 priorities: bool = True, spot_keys=("radius", "Tp", "vp", "xp")):
+                 priorities: bool = True, spot_keys=("radius", "Tp", "vp", "xp"), ingest_priority: str = "high"):
         import torch
         import ntlp_b200
         self.torch = torch
@@ -257,6 +267,7 @@ class CudaEngine:
         self.keep_state = keep_state
         self.priorities = priorities
         self.spot_keys = spot_keys
+        self.ingest_priority = ingest_priority
         lo, hi = torch.cuda.Stream.priority_range()   # (lowest, highest); numerically hi <= lo
         self._prio = (lo, hi)
         self._local = threading.local()
@@ -290,15 +301,19 @@ class CudaEngine:
         return s
 
     def _context(self, box, params, prio):
-        # the upload runs on the ingest thread's high-priority stream, so a
-        # job's set-up is not queued behind the steps of running jobs; its
-        # steps then go to a stream of the job's own priority
-        ist = self._ingest_stream()
+        # with ingest_priority "high" the upload runs on the ingest thread's
+        # high-priority stream (set-up is not queued behind running steps);
+        # with "job" it runs at the job's own priority (a large job's set-up
+        # does not hold back the steps of small ones).  The steps go to a
+        # stream of the job's priority.
+        stream = self.torch.cuda.Stream(device=self.device, priority=prio)
         ctx = self.ntlp.DropletBatch([box["grid"]], params, [max(box["n"], 1)])
-        ctx.use_stream(ist.cuda_stream)
+        if self.ingest_priority == "high":
+            ctx.use_stream(self._ingest_stream().cuda_stream)
+        else:
+            ctx.use_stream(stream.cuda_stream)
         ctx.box_fill_ext(0, box["flow"], sync=False)
         ctx.set_box_droplets(0, box["droplets"])
-        stream = self.torch.cuda.Stream(device=self.device, priority=prio)
         ctx.use_stream(stream.cuda_stream)      # waits for the upload
         return ctx, stream
 
