@@ -218,6 +218,46 @@ int ntlp_advance_graph(ntlp_ctx *ctx, double dt, int32_t it, int32_t nsteps);
 int ntlp_autotune(ntlp_ctx *ctx, double dt, int32_t it, int32_t steps, int32_t choice[2],
                   double ms[NTLP_TUNE_VARIANTS]);
 
+/* ---- x-y column subdomains -------------------------------------------------
+ * The reference decomposes the periodic domain into x-y columns, one per MPI
+ * rank (set_bounds, particles.f90:1766-1781).  A subdomain context holds one
+ * such column: its grid gives the local nnx, nny (columns mxs..mxe, rows
+ * iys..iye), the global nnz, z arrays and the GLOBAL xl, yl; `sd` places it
+ * in the global grid.  Fields come with their halos filled by the caller
+ * (ntlp_fields_upload_ext; uext(0:nnz+1, iys-2:iye+3, mxs-2:mxe+3)).  After
+ * a step, the droplets that left the subdomain are out of its list and are
+ * read with ntlp_sub_emigrants, as particle_exchange (:1435-1764) sends
+ * them; the neighbours' arrivals are prepended with ntlp_sub_immigrants.
+ * The deposition keeps the sources of the +1 column and row, which
+ * particle_coupling_exchange (:1066-1113) hands to the neighbours:
+ * ntlp_sub_halo_get / ntlp_sub_halo_add, x (axis 0) before y (axis 1).
+ * Sources read back (ntlp_coupling, ntlp_box_sources) are the local
+ * columns and rows, column layout.                                          */
+typedef struct ntlp_subdomain {
+    int32_t nnx_g, nny_g;   /* columns and rows of the whole periodic domain    */
+    int32_t i0, j0;         /* first local column / row minus one: mxs-1, iys-1 */
+} ntlp_subdomain;
+int ntlp_sub_create(const ntlp_grid *local_grid, const ntlp_subdomain *sd, const ntlp_params *params,
+                    int64_t capacity, ntlp_ctx **out);
+/* droplets that left in the last step */
+int64_t ntlp_sub_emigrant_count(ntlp_ctx *ctx);
+/* They are written to *out (arrays of at least ntlp_sub_emigrant_count
+ * entries; NULL arrays are skipped) grouped by direction[i] (1 right =
+ * y above ymax, 2 top right, 3 top = x above xmax, 4 top left, 5 left,
+ * 6 bottom left, 7 bottom, 8 bottom right: particle_exchange's buffers),
+ * each group in list order; positions are already periodic.               */
+int ntlp_sub_emigrants(ntlp_ctx *ctx, ntlp_droplets *out, int32_t *direction);
+/* in->n droplets put at the head of the list in the given order (the first
+ * becomes the first of the list, as particle_exchange's prepending of its
+ * receive buffers produces when the caller reverses them)                  */
+int ntlp_sub_immigrants(ntlp_ctx *ctx, const ntlp_droplets *in);
+/* axis 0: sources of column nnx+1, rows 1..nny+1 (6 x (nnz+2)(nny+1));
+ * axis 1: row nny+1, columns 1..nnx (6 x (nnz+2) nnx); z fastest.           */
+int ntlp_sub_halo_get(ntlp_ctx *ctx, int32_t axis, double *out);
+/* add a neighbour's axis-0 halo to column 1 (rows 1..nny+1) or its axis-1
+ * halo to row 1 (columns 1..nnx)                                            */
+int ntlp_sub_halo_add(ntlp_ctx *ctx, int32_t axis, const double *in);
+
 /* ---- statistics and histograms ------------------------------------------
  * particle_xy_stats (particles.f90:3370-3770; les.F:476 calls it after every
  * step), radius_histogram (:5011-5021) and the histograms and surface

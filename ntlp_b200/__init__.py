@@ -63,6 +63,14 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.ntlp_stream.restype = C.c_void_p
     L.ntlp_use_stream.argtypes = [C.c_void_p, C.c_void_p]
     L.ntlp_stats.argtypes = [C.c_void_p, C.c_int32, P(abi.NtlpStats0), C.c_int32, dp, dp]
+    L.ntlp_sub_create.argtypes = [P(abi.NtlpGrid), P(abi.NtlpSubdomain), P(abi.NtlpParams), C.c_int64,
+                                  P(C.c_void_p)]
+    L.ntlp_sub_emigrant_count.argtypes = [C.c_void_p]
+    L.ntlp_sub_emigrant_count.restype = C.c_int64
+    L.ntlp_sub_emigrants.argtypes = [C.c_void_p, P(abi.NtlpDroplets), P(C.c_int32)]
+    L.ntlp_sub_immigrants.argtypes = [C.c_void_p, P(abi.NtlpDroplets)]
+    L.ntlp_sub_halo_get.argtypes = [C.c_void_p, C.c_int32, dp]
+    L.ntlp_sub_halo_add.argtypes = [C.c_void_p, C.c_int32, dp]
     L.ntlp_radius_histogram.argtypes = [C.c_void_p, C.c_int32, dp]
     L.ntlp_step_histograms.argtypes = [C.c_void_p, C.c_int32, dp, dp, C.c_int32]
     L.ntlp_checkpoint_write.argtypes = [C.c_char_p, P(abi.NtlpDroplets)]
@@ -417,3 +425,73 @@ class DropletBatch(DropletStep):
         ms = (C.c_double * 5)()
         self._check(self.L.ntlp_autotune(self.h, float(dt), int(it), int(steps), choice, ms), "ntlp_autotune")
         return dict(deposit_variant=int(choice[0]), block_variant=int(choice[1]), ms=list(ms))
+
+
+class SubdomainStep(DropletStep):
+    """One x-y column subdomain of a periodic domain (one MPI rank of the
+    reference, set_bounds particles.f90:1766-1781).  `local_grid` has the
+    local nnx, nny and the global xl, yl; fields come with halos
+    (set_fields_ext).  The exchanges with the neighbours are the caller's
+    (ntlp_b200.decomp)."""
+
+    def __init__(self, local_grid: dict, params: dict, capacity: int, nnx_g: int, nny_g: int, i0: int, j0: int):
+        self.L = load_library()
+        self.grid = local_grid
+        self.grids = [local_grid]
+        self.params = dict(params)
+        self._g, self._gkeep = abi.make_grid_struct(local_grid)
+        self._p = abi.make_params_struct(params)
+        self._sd = abi.NtlpSubdomain(nnx_g=nnx_g, nny_g=nny_g, i0=i0, j0=j0)
+        h = C.c_void_p()
+        rc = self.L.ntlp_sub_create(C.byref(self._g), C.byref(self._sd), C.byref(self._p), int(capacity),
+                                    C.byref(h))
+        if rc != 0 or not h.value:
+            raise NtlpError(f"ntlp_sub_create failed ({rc})")
+        self.h = h
+        self.capacity = int(capacity)
+        self.last_counters = {}
+
+    def emigrants(self):
+        """(droplet dict, direction array) of the droplets that left in the
+        last step, grouped by direction 1..8, list order within a group."""
+        m = int(self.L.ntlp_sub_emigrant_count(self.h))
+        if m < 0:
+            raise NtlpError("ntlp_sub_emigrant_count failed")
+        d = abi.empty_droplets(max(m, 1))
+        dirs = np.zeros(max(m, 1), dtype=np.int32)
+        s = abi.make_droplets_struct(d, n=m)
+        self._check(self.L.ntlp_sub_emigrants(self.h, C.byref(s), dirs.ctypes.data_as(C.POINTER(C.c_int32))),
+                    "ntlp_sub_emigrants")
+        return {k: np.ascontiguousarray(v[..., :m] if v.ndim == 2 else v[:m]) for k, v in d.items()}, dirs[:m]
+
+    def immigrants(self, d: dict):
+        """Put droplets at the head of the list, in the given order."""
+        if d["radius"].shape[0] == 0:
+            return
+        s = abi.make_droplets_struct(d)
+        self._check(self.L.ntlp_sub_immigrants(self.h, C.byref(s)), "ntlp_sub_immigrants")
+
+    def sources(self) -> list:
+        """The six source arrays of the last deposition on the local columns,
+        (nnx, nny, nnz+2) in C order (z fastest), halos already added."""
+        g = self.grid
+        shape = (g["nnx"], g["nny"], g["nnz"] + 2)
+        mom = np.empty((3,) + shape)
+        rest = [np.empty(shape) for _ in range(3)]
+        self._check(self.L.ntlp_box_sources(self.h, 0, abi.NTLP_LAYOUT_COLUMN, abi.as_dptr(mom.reshape(-1)),
+                                            *(abi.as_dptr(a.reshape(-1)) for a in rest)), "ntlp_box_sources")
+        return [mom[0], mom[1], mom[2], rest[0], rest[1], rest[2]]
+
+    def halo_size(self, axis: int) -> int:
+        g = self.grid
+        return 6 * (g["nnz"] + 2) * (g["nny"] + 1 if axis == 0 else g["nnx"])
+
+    def halo_get(self, axis: int) -> np.ndarray:
+        out = np.zeros(self.halo_size(axis))
+        self._check(self.L.ntlp_sub_halo_get(self.h, int(axis), abi.as_dptr(out)), "ntlp_sub_halo_get")
+        return out
+
+    def halo_add(self, axis: int, arr):
+        arr = np.ascontiguousarray(arr, dtype=np.float64)
+        assert arr.size == self.halo_size(axis)
+        self._check(self.L.ntlp_sub_halo_add(self.h, int(axis), abi.as_dptr(arr)), "ntlp_sub_halo_add")

@@ -88,6 +88,10 @@ STATS_LEVEL_NAMES = ("partcount", "vp1mean", "vp2mean", "vp3mean", "vp1msqr", "v
 STEP_HIST_NAMES = ("actres", "res", "acttodeath", "numact", "raddeath")
 
 
+class NtlpSubdomain(C.Structure):
+    _fields_ = [("nnx_g", C.c_int32), ("nny_g", C.c_int32), ("i0", C.c_int32), ("j0", C.c_int32)]
+
+
 class NtlpStats0(C.Structure):
     _fields_ = [("numpart", C.c_int64), ("numdrop", C.c_int64), ("numaerosol", C.c_int64),
                 ("Rep_sum", C.c_double), ("wmass", C.c_double), ("pmass", C.c_double), ("pvol", C.c_double),

@@ -39,6 +39,7 @@ UNITS = {
     "ntlp_noalloc.cu": [],
     "ntlp_stats.cu": ["--fmad=false"],
     "ntlp_checkpoint.cpp": [],
+    "ntlp_subdomain.cu": [],
 }
 HEADERS = ["ntlp_math.h", "ntlp_hist.h", "ntlp_dev.cuh", "ntlp_kernels.h", "ntlp_physics.cuh", "ntlp_deposit.cuh"]
 

@@ -45,6 +45,7 @@ struct BoxHost {
     int n_uploaded = 0;
     bool have_fields = false, have_droplets = false;
     void *arena = nullptr, *arena_rk3 = nullptr, *arena_stats = nullptr;
+    int *emig_order_slot = nullptr, *emig_order_dir = nullptr;   // subdomain: emigrants in send order
     StatsScratch stats{};
     size_t arena_bytes = 0;
     double *staging = nullptr;      // flow-field / source transposes, upload tile tables
@@ -201,10 +202,18 @@ void carve_box(Carver &cv, BoxHost &h, DevBox &B, bool mixed) {
     cv.take(&B.counters, kNumCounters);
     cv.take(&B.pflux, (size_t)g.nnz + 1);
     cv.take(&B.flux_fx, (size_t)2 * (g.nnz + 1) * kFluxLimbs);
-    for (int q = 0; q < 6; ++q) cv.take(&B.src[q], (size_t)g.nnodes);
+    const size_t nsrc = (size_t)g.nz2 * g.sny * g.snx;   // nnodes, or with the +1 column/row of a subdomain
+    for (int q = 0; q < 6; ++q) cv.take(&B.src[q], nsrc);
     cv.take(&B.err, 1);
     cv.take(&B.defer, n);
     cv.take(&B.ndefer, 1);
+    if (!g.periodic) {
+        cv.take(&B.emig_slot, n);
+        cv.take(&B.emig_dir, n);
+        cv.take(&B.nemig, 1);
+        cv.take(&h.emig_order_slot, n);
+        cv.take(&h.emig_order_dir, n);
+    }
     cv.take(&B.hist, (size_t)NTLP_H_STEP_KINDS * NTLP_HIST_N);
     cv.take(&B.precip_fx, (size_t)g.nnx * g.nny * kFluxLimbs);
     // staging: the largest of a droplet array, a source array, a flow field
@@ -212,7 +221,9 @@ void carve_box(Carver &cv, BoxHost &h, DevBox &B, bool mixed) {
     size_t stage = n;
     const size_t flow_n = (size_t)g.nnx * g.nny * g.nz2;
     const size_t tiles = (n / kUpdateThreads + 2 + (size_t)(g.ncells + 2) / kScanTile + 2) * 4 + 8;
-    if ((size_t)g.nnodes > stage) stage = (size_t)g.nnodes;
+    if (nsrc > stage) stage = nsrc;
+    const size_t halo = 6 * (size_t)g.nz2 * (size_t)(g.snx > g.sny ? g.snx : g.sny);
+    if (halo > stage) stage = halo;
     if (flow_n > stage) stage = flow_n;
     if (tiles > stage) stage = tiles;
     cv.take(&h.staging, stage);
@@ -462,11 +473,33 @@ void box_geometry(const ntlp_grid &grid, int64_t cap, DevBox &B) {
     g.xl = grid.xl; g.yl = grid.yl; g.zl = grid.zl;
     g.ncells = (long long)(grid.nnx + 1) * (grid.nny + 1) * (grid.nnz + 1);
     g.nnodes = (long long)g.nz2 * grid.nny * grid.nnx;
+    g.periodic = 1;
+    g.ioff = 0; g.joff = 0;
+    g.snx = grid.nnx; g.sny = grid.nny;
+    g.xmin = 0.0; g.xmax = grid.xl; g.ymin = 0.0; g.ymax = grid.yl;
     B.cap = (int)cap;
     B.cur = 0;
 }
 
-int create(int nbox, const ntlp_grid *grids, const ntlp_params *params, const int64_t *caps, ntlp_ctx **out) {
+// an x-y column subdomain of the periodic domain (set_bounds,
+// particles.f90:1766-1781): the grid spacing is the global domain's
+void subdomain_geometry(const ntlp_grid &grid, const ntlp_subdomain &sd, DevBox &B) {
+    DevGrid &g = B.g;
+    g.dx = grid.xl / sd.nnx_g;
+    g.dy = grid.yl / sd.nny_g;
+    g.periodic = 0;
+    g.ioff = sd.i0;
+    g.joff = sd.j0;
+    g.snx = grid.nnx + 1;
+    g.sny = grid.nny + 1;
+    g.xmin = g.dx * (double)sd.i0;
+    g.xmax = g.dx * (double)(sd.i0 + grid.nnx);
+    g.ymin = g.dy * (double)sd.j0;
+    g.ymax = g.dy * (double)(sd.j0 + grid.nny);
+}
+
+int create(int nbox, const ntlp_grid *grids, const ntlp_params *params, const int64_t *caps, ntlp_ctx **out,
+           const ntlp_subdomain *sd = nullptr) {
     if (!out) return NTLP_ERR_ARG;
     *out = nullptr;
     ntlp_ctx *c = new ntlp_ctx();
@@ -480,6 +513,10 @@ int create(int nbox, const ntlp_grid *grids, const ntlp_params *params, const in
     if (!rc && !params) rc = fail(c, NTLP_ERR_ARG, "params must not be NULL");
     if (!rc && params->precision != NTLP_PREC_FP64 && params->precision != NTLP_PREC_MIXED)
         rc = fail(c, NTLP_ERR_ARG, "unknown precision %d", params->precision);
+    if (!rc && sd && (nbox != 1 || sd->nnx_g < grids[0].nnx || sd->nny_g < grids[0].nny || sd->i0 < 0 ||
+                      sd->j0 < 0 || sd->i0 + grids[0].nnx > sd->nnx_g || sd->j0 + grids[0].nny > sd->nny_g))
+        rc = fail(c, NTLP_ERR_ARG, "subdomain (%d..%d, %d..%d) does not fit the %d x %d grid", sd->i0 + 1,
+                  sd->i0 + grids[0].nnx, sd->j0 + 1, sd->j0 + grids[0].nny, sd->nnx_g, sd->nny_g);
     for (int b = 0; !rc && b < nbox; ++b) {
         rc = check_grid(c, &grids[b]);
         if (!rc && (caps[b] < 1 || caps[b] > 0x7fffffffLL))
@@ -519,6 +556,7 @@ int create(int nbox, const ntlp_grid *grids, const ntlp_params *params, const in
         DevBox &B = c->box[b];
         const DevGrid &g = B.g;
         box_geometry(*grid, h.cap, B);
+        if (sd) subdomain_geometry(*grid, *sd, B);
         Carver cv;
         carve_box(cv, h, B, mixed);
         h.arena_bytes = cv.off;
@@ -562,7 +600,7 @@ int create(int nbox, const ntlp_grid *grids, const ntlp_params *params, const in
         bft.push_back((int)ct.size());
         for (long long s = 0; s < g.ncells + 2; s += kScanTile) ct.push_back(Tile{b, (int)s});
         for (int v = 0; v < kDepVariants; ++v) {
-            long long nt = deposit_tile_count(v, g.nnx, g.nny, g.nnz);
+            long long nt = deposit_tile_count(v, g.snx, g.sny, g.nnz);
             for (long long s = 0; s < nt; ++s) dpt[v].push_back(Tile{b, (int)s});
         }
     }
@@ -663,6 +701,8 @@ int fields_ext(ntlp_ctx *c, int b, const double *const h[5]) {
 
 int fields_flow(ntlp_ctx *c, int b, const double *const h[5]) {
     if (!box_ok(c, b)) return fail(c, NTLP_ERR_ARG, "box %d out of range", b);
+    if (!c->box[b].g.periodic)
+        return fail(c, NTLP_ERR_STATE, "a subdomain takes its fields with halos (ntlp_fields_upload_ext)");
     for (int k = 0; k < 5; ++k)
         if (!h[k]) return fail(c, NTLP_ERR_ARG, "field %d is NULL", k);
     const DevBox &B = c->box[b];
@@ -906,6 +946,18 @@ int sources_out(ntlp_ctx *c, int b, int32_t layout, double *const host[6]) {
     const DevGrid &g = B.g;
     const size_t nn = (size_t)g.nnodes;
     bool any = false;
+    if (!g.periodic) {
+        // local columns 1..nnx, rows 1..nny of the (nnx+1) x (nny+1) array
+        if (layout != NTLP_LAYOUT_COLUMN) return fail(c, NTLP_ERR_ARG, "a subdomain returns the column layout");
+        for (int q = 0; q < 6; ++q) {
+            if (!host[q]) continue;
+            any = true;
+            CK(cudaMemcpy2DAsync(host[q], (size_t)g.nz2 * g.nny * 8, B.src[q], (size_t)g.nz2 * g.sny * 8,
+                                 (size_t)g.nz2 * g.nny * 8, (size_t)g.nnx, cudaMemcpyDefault, c->stream));
+        }
+        if (any) CK(cudaStreamSynchronize(c->stream));
+        return NTLP_OK;
+    }
     for (int q = 0; q < 6; ++q) {
         if (!host[q]) continue;
         any = true;
@@ -1003,7 +1055,7 @@ int64_t ntlp_bytes_required(int32_t nbox, const ntlp_grid *grids, const ntlp_par
         size_t tiles = 0;
         for (int v = 0; v < kNtVariants; ++v) tiles += (size_t)(h.cap + kNtValues[v] - 1) / kNtValues[v];
         tiles += 2 * (size_t)((g.ncells + 2 + kScanTile - 1) / kScanTile);
-        for (int v = 0; v < kDepVariants; ++v) tiles += (size_t)deposit_tile_count(v, g.nnx, g.nny, g.nnz);
+        for (int v = 0; v < kDepVariants; ++v) tiles += (size_t)deposit_tile_count(v, g.snx, g.sny, g.nnz);
         total += tiles * sizeof(Tile) + sizeof(DevBox) + 64;
     }
     return (int64_t)(total + 16 * 256 + sizeof(DevParams));
@@ -1300,6 +1352,151 @@ int ntlp_autotune(ntlp_ctx *c, double dt, int32_t it, int32_t steps, int32_t cho
     return NTLP_OK;
 }
 
+int ntlp_sub_create(const ntlp_grid *local_grid, const ntlp_subdomain *sd, const ntlp_params *params,
+                    int64_t capacity, ntlp_ctx **out) {
+    if (!sd) return NTLP_ERR_ARG;
+    return create(1, local_grid, params, &capacity, out, sd);
+}
+
+int64_t ntlp_sub_emigrant_count(ntlp_ctx *c) {
+    if (!c || c->box[0].g.periodic) return 0;
+    int m = 0;
+    if (cudaMemcpyAsync(&m, c->box[0].nemig, sizeof(int), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+        cudaStreamSynchronize(c->stream) != cudaSuccess)
+        return -1;
+    return m;
+}
+
+int ntlp_sub_emigrants(ntlp_ctx *c, ntlp_droplets *d, int32_t *direction) {
+    if (!c || !d) return NTLP_ERR_ARG;
+    if (c->box[0].g.periodic) return fail(c, NTLP_ERR_STATE, "not a subdomain context");
+    const int64_t m64 = ntlp_sub_emigrant_count(c);
+    if (m64 < 0) return fail(c, NTLP_ERR_CUDA, "reading the emigrant count failed");
+    const int m = (int)m64;
+    d->n = m;
+    if (m == 0) return NTLP_OK;
+    if (pull_boxes(c)) return NTLP_ERR_CUDA;
+    BoxHost &h = c->bh[0];
+    const DevBox &B = c->box[0];
+    const DevState &S = B.st[B.cur];
+    launch_emig_order(c->box_d, 0, m, h.emig_order_slot, h.emig_order_dir, c->stream);
+    auto get = [&](const void *src, void *dst, int eb) -> int {
+        if (!src || !dst) return NTLP_OK;
+        launch_gather_slots(src, eb, h.emig_order_slot, h.staging, m, c->stream);
+        CK(cudaMemcpyAsync(dst, h.staging, (size_t)m * eb, cudaMemcpyDefault, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        return NTLP_OK;
+    };
+    int rc = 0;
+    for (int a = 0; a < 3; ++a) {
+        rc |= get(S.x[a], d->xp[a], 8); rc |= get(S.v[a], d->vp[a], 8); rc |= get(S.uf[a], d->uf[a], 8);
+        rc |= get(S.vold[a], d->vp_old[a], 8); rc |= get(S.xrhs[a], d->xrhs[a], 8);
+        rc |= get(S.vrhs[a], d->vrhs[a], 8);
+    }
+    rc |= get(S.Tp, d->Tp, 8); rc |= get(S.r, d->radius, 8); rc |= get(S.m_s, d->m_s, 8);
+    rc |= get(S.kap, d->kappa_s, 8); rc |= get(S.rc, d->rc, 8); rc |= get(S.res, d->res, 8);
+    rc |= get(S.actres, d->actres, 8); rc |= get(S.numact, d->numact, 8); rc |= get(S.Tf, d->Tf, 8);
+    rc |= get(S.qinf, d->qinf, 8); rc |= get(S.qstar, d->qstar, 8); rc |= get(S.Tpold, d->Tp_old, 8);
+    rc |= get(S.rold, d->radius_old, 8); rc |= get(S.Tprhs_s, d->Tprhs_s, 8);
+    rc |= get(S.Tprhs_L, d->Tprhs_L, 8); rc |= get(S.radrhs, d->radrhs, 8);
+    rc |= get(S.lid, d->lid, 4);
+    if (rc) return rc;
+    if (d->mult) {
+        launch_gather_slots_i64(S.mult, h.emig_order_slot, (long long *)h.staging, m, c->stream);
+        CK(cudaMemcpyAsync(d->mult, h.staging, (size_t)m * 8, cudaMemcpyDefault, c->stream));
+    }
+    if (direction) CK(cudaMemcpyAsync(direction, h.emig_order_dir, (size_t)m * 4, cudaMemcpyDefault, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaGetLastError());
+    return NTLP_OK;
+}
+
+int ntlp_sub_immigrants(ntlp_ctx *c, const ntlp_droplets *d) {
+    if (!c || !d) return NTLP_ERR_ARG;
+    if (c->box[0].g.periodic) return fail(c, NTLP_ERR_STATE, "not a subdomain context");
+    BoxHost &h = c->bh[0];
+    if (!h.have_droplets) return fail(c, NTLP_ERR_STATE, "droplets not uploaded");
+    const int m = (int)d->n;
+    if (m < 0) return fail(c, NTLP_ERR_ARG, "negative count");
+    if (m == 0) return NTLP_OK;
+    if (!d->xp[0] || !d->xp[1] || !d->xp[2] || !d->vp[0] || !d->vp[1] || !d->vp[2] || !d->Tp || !d->radius ||
+        !d->m_s || !d->kappa_s || !d->mult)
+        return fail(c, NTLP_ERR_ARG, "xp, vp, Tp, radius, m_s, kappa_s and mult are required");
+    int n = 0;
+    if (pull_boxes(c) || read_n_alive(c, 0, &n)) return NTLP_ERR_CUDA;
+    if ((int64_t)n + m > h.cap)
+        return fail(c, NTLP_ERR_CAPACITY, "%d + %d droplets exceed capacity %lld", n, m, (long long)h.cap);
+    // existing droplets to slots m.. in list order, then the arrivals to 0..m-1
+    launch_rank_alive(c->box_d, 0, h.rank, h.n_uploaded, c->stream);
+    launch_shift_existing(c->box_d, 0, n, m, h.rank, c->stream);
+    const DevState &O = c->box[0].st[1 - c->box[0].cur];
+    auto up = [&](void *dst, const void *src, size_t esz) -> int {
+        if (!dst) return NTLP_OK;
+        if (src) {
+            CK(cudaMemcpyAsync(dst, src, (size_t)m * esz, cudaMemcpyDefault, c->stream));
+        } else {
+            CK(cudaMemsetAsync(dst, 0, (size_t)m * esz, c->stream));
+        }
+        return NTLP_OK;
+    };
+    int rc = 0;
+    for (int a = 0; a < 3; ++a) {
+        rc |= up(O.x[a], d->xp[a], 8); rc |= up(O.v[a], d->vp[a], 8); rc |= up(O.uf[a], d->uf[a], 8);
+        rc |= up(O.vold[a], d->vp_old[a], 8); rc |= up(O.xrhs[a], d->xrhs[a], 8); rc |= up(O.vrhs[a], d->vrhs[a], 8);
+    }
+    rc |= up(O.Tp, d->Tp, 8); rc |= up(O.r, d->radius, 8); rc |= up(O.m_s, d->m_s, 8);
+    rc |= up(O.kap, d->kappa_s, 8); rc |= up(O.rc, d->rc, 8); rc |= up(O.res, d->res, 8);
+    rc |= up(O.actres, d->actres, 8); rc |= up(O.numact, d->numact, 8); rc |= up(O.Tf, d->Tf, 8);
+    rc |= up(O.qinf, d->qinf, 8); rc |= up(O.qstar, d->qstar, 8); rc |= up(O.Tpold, d->Tp_old, 8);
+    rc |= up(O.rold, d->radius_old, 8); rc |= up(O.Tprhs_s, d->Tprhs_s, 8);
+    rc |= up(O.Tprhs_L, d->Tprhs_L, 8); rc |= up(O.radrhs, d->radrhs, 8); rc |= up(O.mult, d->mult, 8);
+    if (rc) return rc;
+    k_iota<<<(m + 255) / 256, 256, 0, c->stream>>>(O.lid, m);
+    const int total = n + m;
+    CK(cudaMemcpyAsync(c->box[0].n_alive, &total, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    launch_keys_initial(c->box_d, c->drop_tiles_d[0], c->n_drop_tiles[0], c->stream);
+    launch_sort(c->box_d, c->plan, c->stream);
+    launch_finish(c->box_d, 1, c->stream);
+    CK(cudaGetLastError());
+    if (pull_boxes(c)) return NTLP_ERR_CUDA;     // also waits for the host copy of `total`
+    h.n_uploaded = total;
+    c->payload_valid = false;
+    return NTLP_OK;
+}
+
+int ntlp_sub_halo_get(ntlp_ctx *c, int32_t axis, double *out) {
+    if (!c || !out || (axis != 0 && axis != 1)) return NTLP_ERR_ARG;
+    const DevBox &B = c->box[0];
+    const DevGrid &g = B.g;
+    if (g.periodic) return fail(c, NTLP_ERR_STATE, "not a subdomain context");
+    if (axis == 0) {
+        const size_t n = (size_t)g.nz2 * g.sny;                    // column nnx+1, rows 1..nny+1
+        for (int q = 0; q < 6; ++q)
+            CK(cudaMemcpyAsync(out + q * n, B.src[q] + (size_t)g.nnx * n, n * 8, cudaMemcpyDefault, c->stream));
+    } else {
+        const size_t n = (size_t)g.nz2 * g.nnx;                    // row nny+1, columns 1..nnx
+        for (int q = 0; q < 6; ++q)
+            CK(cudaMemcpy2DAsync(out + q * n, (size_t)g.nz2 * 8, B.src[q] + (size_t)g.nz2 * g.nny,
+                                 (size_t)g.nz2 * g.sny * 8, (size_t)g.nz2 * 8, (size_t)g.nnx, cudaMemcpyDefault,
+                                 c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return NTLP_OK;
+}
+
+int ntlp_sub_halo_add(ntlp_ctx *c, int32_t axis, const double *in) {
+    if (!c || !in || (axis != 0 && axis != 1)) return NTLP_ERR_ARG;
+    const DevBox &B = c->box[0];
+    const DevGrid &g = B.g;
+    if (g.periodic) return fail(c, NTLP_ERR_STATE, "not a subdomain context");
+    const long long nq = (long long)g.nz2 * (axis == 0 ? g.sny : g.nnx);
+    CK(cudaMemcpyAsync(c->bh[0].staging, in, (size_t)(6 * nq) * 8, cudaMemcpyDefault, c->stream));
+    launch_halo_add(c->box_d, 0, axis, c->bh[0].staging, nq, c->stream);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->stream));
+    return NTLP_OK;
+}
+
 int ntlp_stats(ntlp_ctx *c, int32_t box, ntlp_stats0 *s0, int32_t maxnz, double *level_sums, double *lwp) {
     if (!box_ok(c, box)) return NTLP_ERR_ARG;
     BoxHost &h = c->bh[box];
@@ -1345,11 +1542,15 @@ int ntlp_stats(ntlp_ctx *c, int32_t box, ntlp_stats0 *s0, int32_t maxnz, double 
     }
     if (lwp) {
         // columns ipt = nnx+1 / jpt = nny+1 hold droplets exactly at x = xl /
-        // y = yl; they are added to their periodic images, x first, then y
+        // y = yl; on the periodic domain they are added to their images, x
+        // first, then y (a subdomain's edge column belongs to its neighbour
+        // and is left out, as LWP(mxs:mxe, iys:iye) has no room for it)
         const int nx1 = g.nnx + 1, ny1 = g.nny + 1;
         auto at = [&](int i, int j) -> double & { return col[(size_t)(j - 1) + (size_t)ny1 * (i - 1)]; };
-        for (int j = 1; j <= ny1; ++j) at(1, j) = at(1, j) + at(nx1, j);
-        for (int i = 1; i <= g.nnx; ++i) at(i, 1) = at(i, 1) + at(i, ny1);
+        if (g.periodic) {
+            for (int j = 1; j <= ny1; ++j) at(1, j) = at(1, j) + at(nx1, j);
+            for (int i = 1; i <= g.nnx; ++i) at(i, 1) = at(i, 1) + at(i, ny1);
+        }
         for (int j = 1; j <= g.nny; ++j)
             for (int i = 1; i <= g.nnx; ++i) lwp[(size_t)(i - 1) + (size_t)g.nnx * (j - 1)] = at(i, j);
     }

@@ -89,8 +89,8 @@ __device__ __forceinline__ void merge_ranges(const DevBox &B, const DevParams &p
     const DevState &O = B.st[B.cur];
     int head[8];
     for (int c = 0; c < n; ++c) head[c] = STAGED ? s_lid[pos[c]] : O.lid[B.perm[pos[c]]];
-    const double xv = g.dx * (double)(px - 1);
-    const double yv = g.dy * (double)(py - 1);
+    const double xv = g.dx * (double)(px + g.ioff - 1);
+    const double yv = g.dy * (double)(py + g.joff - 1);
     const double zv = g.zz[pz];
     while (true) {
         int best = -1, bl = 0x7fffffff;
@@ -189,14 +189,14 @@ __device__ __forceinline__ void node_global(const DevBox &B, const DevParams &p,
     const DevGrid &g = B.g;
     double a1[6];
     image_global<MIXED>(B, p, ix, iy, iz, out);
-    if (ix <= 2) {
+    if (g.periodic && ix <= 2) {
         image_global<MIXED>(B, p, ix + g.nnx, iy, iz, a1);
         for (int q = 0; q < 6; ++q) out[q] = out[q] + a1[q];
     }
-    if (iy <= 2) {
+    if (g.periodic && iy <= 2) {
         double b0[6];
         image_global<MIXED>(B, p, ix, iy + g.nny, iz, b0);
-        if (ix <= 2) {
+        if (g.periodic && ix <= 2) {
             image_global<MIXED>(B, p, ix + g.nnx, iy + g.nny, iz, a1);
             for (int q = 0; q < 6; ++q) b0[q] = b0[q] + a1[q];
         }
@@ -231,13 +231,13 @@ k_deposit_tiled(DevBox *boxes, const Tile *tiles, const DevParams *pp) {
     const DevBox &B = boxes[tl.box];
     const DevParams &p = pp[0];
     const DevGrid &g = B.g;
-    const int ntz = (g.nz2 + kDepTZ - 1) / kDepTZ, nty = (g.nny + kDepTY - 1) / kDepTY;
+    const int ntz = (g.nz2 + kDepTZ - 1) / kDepTZ, nty = (g.sny + kDepTY - 1) / kDepTY;
     const int tzi = tl.start % ntz, tyi = (tl.start / ntz) % nty, txi = tl.start / (ntz * nty);
     const int x0 = 1 + txi * kDepTX, y0 = 1 + tyi * kDepTY, z0 = tzi * kDepTZ;
     const int lz = threadIdx.x % kDepTZ, ly = (threadIdx.x / kDepTZ) % kDepTY, lx = threadIdx.x / (kDepTZ * kDepTY);
     const int ix = x0 + lx, iy = y0 + ly, iz = z0 + lz;
-    const bool valid = ix <= g.nnx && iy <= g.nny && iz <= g.nnz + 1;
-    const long long node = (long long)iz + (long long)g.nz2 * ((long long)(iy - 1) + (long long)g.nny * (ix - 1));
+    const bool valid = ix <= g.snx && iy <= g.sny && iz <= g.nnz + 1;
+    const long long node = (long long)iz + (long long)g.nz2 * ((long long)(iy - 1) + (long long)g.sny * (ix - 1));
     double out[6];
     bool staged = (x0 > 2) && (y0 > 2);
     if (staged) {

@@ -50,6 +50,16 @@ struct DevGrid {
     // 6th-order stencil (mixed path), 6 floats per window base k2 in
     // [-2, nnz] at (k2+2)*6; 0 marks a point the boundary rules leave out.
     const float *rden_zz, *rden_z;
+    // A box is either the whole periodic domain (periodic = 1: stencil
+    // columns and deposition nodes past the edge wrap to their images) or
+    // one x-y column subdomain of it (periodic = 0).  ioff/joff: global
+    // column/row index of local column/row 0 (mxs-1, iys-1); xl, yl and
+    // dx, dy are the global domain's.  A subdomain keeps the sources of
+    // its +1 column and row (snx = nnx+1, sny = nny+1) for the neighbours.
+    int periodic;
+    int ioff, joff;
+    int snx, sny;
+    double xmin, xmax, ymin, ymax;   // set_bounds (particles.f90:1766-1781)
 };
 
 struct DevParams {
@@ -112,6 +122,10 @@ struct DevBox {
     int *ndefer;           // their count
     long long *hist;       // [NTLP_H_STEP_KINDS][NTLP_HIST_N] step histograms (weights are integers)
     long long *precip_fx;  // [nny][nnx][kFluxLimbs] surface precipitation, exact fixed point
+    // subdomain boxes: droplets that left the subdomain in the last step
+    // (output slot in st[1-cur] before the finish, st[cur] after it) and
+    // the direction they left in (1..8, particle_exchange's send buffers)
+    int *emig_slot, *emig_dir, *nemig;
 };
 
 // ---- binning ---------------------------------------------------------------
@@ -163,8 +177,8 @@ __device__ __forceinline__ int ijpt(double x, double d) {
 __device__ __forceinline__ int cell_key(const DevGrid &g, double x1, double x2, double x3,
                                         int *ipt_out = nullptr, int *jpt_out = nullptr,
                                         int *kpt_out = nullptr) {
-    int ipt = ijpt(x1, g.dx);
-    int jpt = ijpt(x2, g.dy);
+    int ipt = ijpt(x1, g.dx) - g.ioff;     // local column (subdomain: mxs -> 1)
+    int jpt = ijpt(x2, g.dy) - g.joff;
     int kpt = minloc_zz(g, x3) - 2;
     if (ipt_out) { *ipt_out = ipt; *jpt_out = jpt; *kpt_out = kpt; }
     if (ipt < 1 || ipt > g.nnx + 1 || jpt < 1 || jpt > g.nny + 1 || kpt < 0 || kpt > g.nnz)
@@ -176,8 +190,10 @@ __device__ __forceinline__ int cell_key(const DevGrid &g, double x1, double x2, 
 // stencil of a droplet exactly at x == xl) is the periodic image i - nnx;
 // anything else outside the padded array is clamped and flagged.
 __device__ __forceinline__ long long ext_index(const DevGrid &g, int k, int j, int i, int &bad) {
-    if (i > g.nnx + 3) i -= g.nnx;
-    if (j > g.nny + 3) j -= g.nny;
+    if (g.periodic) {
+        if (i > g.nnx + 3) i -= g.nnx;
+        if (j > g.nny + 3) j -= g.nny;
+    }
     if (k < 0 || k > g.nnz + 1 || j < -1 || j > g.nny + 3 || i < -1 || i > g.nnx + 3) {
         bad = 1;
         k = k < 0 ? 0 : (k > g.nnz + 1 ? g.nnz + 1 : k);

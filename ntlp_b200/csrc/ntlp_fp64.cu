@@ -25,8 +25,9 @@ namespace ntlp {
 __device__ void interp_lin64(const DevBox &B, double x1, double x2, double x3, Interp &o, int &bad) {
     const DevGrid &g = B.g;
     const double dx = g.dx, dy = g.dy;
-    int ipt = ijpt(x1, dx);
-    int jpt = ijpt(x2, dy);
+    const int iptg = ijpt(x1, dx), jptg = ijpt(x2, dy);     // global (node positions)
+    int ipt = iptg - g.ioff;                                // local (array indices)
+    int jpt = jptg - g.joff;
     int kpt = minloc_zz(g, x3) - 2;
     int kwpt = minloc_z(g, x3) - 2;
     if (kpt + 1 < 0 || kpt + 1 > g.nnz + 2 || kwpt + 1 < 0 || kwpt + 1 > g.nnz + 2) {
@@ -38,9 +39,9 @@ __device__ void interp_lin64(const DevBox &B, double x1, double x2, double x3, I
     // innermost loop with the same operands
     double wx[2], wy[2], wz[2], wzw[2];
     for (int i = 0; i < 2; ++i) {
-        double xv = dx * (double)(i + ipt - 1);
+        double xv = dx * (double)(i + iptg - 1);
         wx[i] = (1.0 - fabs(x1 - xv) / dx);
-        double yv = dy * (double)(i + jpt - 1);
+        double yv = dy * (double)(i + jptg - 1);
         wy[i] = (1.0 - fabs(x2 - yv) / dy);
         int kz = i + kpt, kzw = i + kwpt;
         double zv = g.zz[kz < 0 ? 0 : (kz > g.nnz + 1 ? g.nnz + 1 : kz)];
@@ -98,7 +99,8 @@ __device__ __forceinline__ void lagrange6(double x, const double xn[6], int firs
 __device__ void interp6_64(const DevBox &B, double x1, double x2, double x3, Interp &o, int &bad) {
     const DevGrid &g = B.g;
     const int nnz = g.nnz;
-    int ip3 = ijpt(x1, g.dx), jp3 = ijpt(x2, g.dy);
+    const int ip3g = ijpt(x1, g.dx), jp3g = ijpt(x2, g.dy);   // global (node positions)
+    const int ip3 = ip3g - g.ioff, jp3 = jp3g - g.joff;     // local (array indices)
     int ku[6], kw[6];
     ku[2] = minloc_zz(g, x3) - 2;
     kw[2] = minloc_z(g, x3) - 2;
@@ -107,8 +109,8 @@ __device__ void interp6_64(const DevBox &B, double x1, double x2, double x3, Int
     {
         double xn[6], yn[6];
         for (int a = 0; a < 6; ++a) {
-            xn[a] = g.dx * (double)(ip3 + (a - 2) - 1);
-            yn[a] = g.dy * (double)(jp3 + (a - 2) - 1);
+            xn[a] = g.dx * (double)(ip3g + (a - 2) - 1);
+            yn[a] = g.dy * (double)(jp3g + (a - 2) - 1);
         }
         lagrange6(x1, xn, 1, 6, wx);
         lagrange6(x2, yn, 1, 6, wy);
@@ -155,8 +157,8 @@ __device__ void interp6_64(const DevBox &B, double x1, double x2, double x3, Int
 #pragma unroll
     for (int a = 0; a < 6; ++a) {
         int ix = ip3 + (a - 2), iy = jp3 + (a - 2);
-        if (ix > g.nnx + 3) ix -= g.nnx;
-        if (iy > g.nny + 3) iy -= g.nny;
+        if (g.periodic && ix > g.nnx + 3) ix -= g.nnx;
+        if (g.periodic && iy > g.nny + 3) iy -= g.nny;
         if (ix < -1 || ix > g.nnx + 3) { bad = 1; ix = ix < -1 ? -1 : g.nnx + 3; }
         if (iy < -1 || iy > g.nny + 3) { bad = 1; iy = iy < -1 ? -1 : g.nny + 3; }
         xo[a] = (long long)g.nz2 * g.ny5 * (ix + 1);
@@ -360,7 +362,12 @@ k_update_rk3_64(DevBox *boxes, const Tile *tiles, const DevParams *pp, StepIn in
         O.Tf[t] = Tf; O.qinf[t] = qinf; O.qstar[t] = qstar; O.Tpold[t] = Tpold; O.rold[t] = rold;
         O.Tprhs_s[t] = Tprhs_s; O.Tprhs_L[t] = Tprhs_L; O.radrhs[t] = radrhs;
         int key;
-        if (!alive) {
+        if (alive >= 10) {
+            key = (int)B.g.ncells + 1;
+            const int e = atomicAdd(B.nemig, 1);
+            B.emig_slot[e] = t;
+            B.emig_dir[e] = alive - 10;
+        } else if (!alive) {
             key = (int)B.g.ncells + 1;
             cnt.v[C_DESTROY]++;
             record_kill(B, p, x, radius, S.rc[s], res, S.actres[s], S.numact[s], multi);

@@ -79,6 +79,13 @@ void launch_pack_f32(const DevBox *host_box, float4 *f4, float *fw, cudaStream_t
 // download: position of each survivor in list order
 void launch_rank_alive(DevBox *boxes, int box, int *rank_by_lid, int nlid, cudaStream_t st);
 
+// x-y column subdomains (ntlp_subdomain.cu)
+void launch_emig_order(const DevBox *boxes, int box, int m, int *slot_out, int *dir_out, cudaStream_t st);
+void launch_gather_slots(const void *src, int elem_bytes, const int *slot, void *out, int m, cudaStream_t st);
+void launch_gather_slots_i64(const long long *src, const int *slot, long long *out, int m, cudaStream_t st);
+void launch_shift_existing(DevBox *boxes, int box, int n, int m, const int *rank_by_lid, cudaStream_t st);
+void launch_halo_add(DevBox *boxes, int box, int axis, const double *in, long long n_per_q, cudaStream_t st);
+
 // particle_xy_stats and radius_histogram of one box (ntlp_stats.cu)
 constexpr int kStatCols = 128;      // columns per tile (one block)
 constexpr int kStatThreads = 256;

@@ -68,14 +68,15 @@ __device__ __forceinline__ void lagrange6_win(double x, const double *lev, int k
 __device__ void interp6_mixed(const DevBox &B, double x1, double x2, double x3, Interp &o, int &bad) {
     const DevGrid &g = B.g;
     const int nnz = g.nnz;
-    const int ip3 = ijpt(x1, g.dx), jp3 = ijpt(x2, g.dy);
+    const int ip3g = ijpt(x1, g.dx), jp3g = ijpt(x2, g.dy);   // global (node positions)
+    const int ip3 = ip3g - g.ioff, jp3 = jp3g - g.joff;     // local (array indices)
     const int ku2 = minloc_zz(g, x3) - 2;
     const int kw2 = minloc_z(g, x3) - 2;
     if (ku2 < 0 || ku2 > nnz + 1 || kw2 < 0) bad = 1;
     float wx[6], wy[6], wz[6], wzw[6];
     // xn(a) = dx*(ip3-3+a): s = x/dx - (ip3-3) in [2, 3)
-    lagrange6_unif((float)(x1 / g.dx - (double)(ip3 - 3)), wx);
-    lagrange6_unif((float)(x2 / g.dy - (double)(jp3 - 3)), wy);
+    lagrange6_unif((float)(x1 / g.dx - (double)(ip3g - 3)), wx);
+    lagrange6_unif((float)(x2 / g.dy - (double)(jp3g - 3)), wy);
     const int cu = ku2 < -2 ? -2 : (ku2 > nnz ? nnz : ku2);
     const int cw = kw2 < -2 ? -2 : (kw2 > nnz ? nnz : kw2);
     if (g.rden_zz != nullptr) {
@@ -95,13 +96,13 @@ __device__ void interp6_mixed(const DevBox &B, double x1, double x2, double x3, 
 #pragma unroll 1
     for (int i = 0; i < 6; ++i) {
         int ix = ip3 + (i - 2);
-        if (ix > g.nnx + 3) ix -= g.nnx;
+        if (g.periodic && ix > g.nnx + 3) ix -= g.nnx;
         if (ix < -1 || ix > g.nnx + 3) { bad = 1; ix = ix < -1 ? -1 : g.nnx + 3; }
         float cu_ = 0.f, cv = 0.f, cw_ = 0.f, cT = 0.f, cq = 0.f;
 #pragma unroll
         for (int j = 0; j < 6; ++j) {
             int iy = jp3 + (j - 2);
-            if (iy > g.nny + 3) iy -= g.nny;
+            if (g.periodic && iy > g.nny + 3) iy -= g.nny;
             if (iy < -1 || iy > g.nny + 3) { bad = 1; iy = iy < -1 ? -1 : g.nny + 3; }
             const long long base = (long long)g.nz2 * ((long long)(iy + 1) + (long long)g.ny5 * (ix + 1));
             float au = 0.f, av = 0.f, aT = 0.f, aq = 0.f, aw = 0.f;
@@ -138,8 +139,9 @@ __device__ void interp6_mixed(const DevBox &B, double x1, double x2, double x3, 
 
 __device__ void interp_lin_mixed(const DevBox &B, double x1, double x2, double x3, Interp &o, int &bad) {
     const DevGrid &g = B.g;
-    int ipt = ijpt(x1, g.dx);
-    int jpt = ijpt(x2, g.dy);
+    const int iptg = ijpt(x1, g.dx), jptg = ijpt(x2, g.dy);
+    int ipt = iptg - g.ioff;
+    int jpt = jptg - g.joff;
     int kpt = minloc_zz(g, x3) - 2;
     int kwpt = minloc_z(g, x3) - 2;
     if (kpt + 1 < 0 || kpt + 1 > g.nnz + 2 || kwpt + 1 < 0 || kwpt + 1 > g.nnz + 2) {
@@ -149,8 +151,8 @@ __device__ void interp_lin_mixed(const DevBox &B, double x1, double x2, double x
     }
     float wx[2], wy[2], wz[2], wzw[2];
     for (int i = 0; i < 2; ++i) {
-        wx[i] = 1.0f - fabsf((float)(x1 - g.dx * (double)(i + ipt - 1))) / (float)g.dx;
-        wy[i] = 1.0f - fabsf((float)(x2 - g.dy * (double)(i + jpt - 1))) / (float)g.dy;
+        wx[i] = 1.0f - fabsf((float)(x1 - g.dx * (double)(i + iptg - 1))) / (float)g.dx;
+        wy[i] = 1.0f - fabsf((float)(x2 - g.dy * (double)(i + jptg - 1))) / (float)g.dy;
         int kz = i + kpt, kzw = i + kwpt;
         double zv = g.zz[kz < 0 ? 0 : (kz > g.nnz + 1 ? g.nnz + 1 : kz)];
         double zwv = g.z[kzw < 0 ? 0 : (kzw > g.nnz + 1 ? g.nnz + 1 : kzw)];

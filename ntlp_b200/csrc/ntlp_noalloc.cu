@@ -157,6 +157,9 @@ extern "C" int ntlp_coupling_noalloc(const ntlp_grid *grid, const ntlp_params *p
     g.dx = grid->xl / grid->nnx; g.dy = grid->yl / grid->nny;
     g.xl = grid->xl; g.yl = grid->yl; g.zl = grid->zl;
     g.ncells = ncells; g.nnodes = nnodes;
+    g.periodic = 1;
+    g.snx = grid->nnx; g.sny = grid->nny;
+    g.xmax = grid->xl; g.ymax = grid->yl;
     g.z = zg; g.zz = zg + (kMaxNz + 3); g.dzw = zg + 2 * (kMaxNz + 3); g.dzu = zg + 3 * (kMaxNz + 3);
     int *ints = (int *)(S + kOffInts);
     int *lid = ints, *key = ints + kMaxN, *sorted = ints + 2 * kMaxN, *perm = ints + 3 * kMaxN;

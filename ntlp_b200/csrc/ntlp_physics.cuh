@@ -449,14 +449,38 @@ __device__ __forceinline__ void record_kill(const DevBox &B, const DevParams &p,
     hist_add(B, p, NTLP_H_NUMACT, numact, 1);
     hist_add(B, p, NTLP_H_RADDEATH, ntlp_log10(radius), mult);
     const DevGrid &g = B.g;
-    const int ipt = ijpt(x[0], g.dx), jpt = ijpt(x[1], g.dy);
+    const int ipt = ijpt(x[0], g.dx) - g.ioff, jpt = ijpt(x[1], g.dy) - g.joff;
     if (B.precip_fx != nullptr && ipt >= 1 && ipt <= g.nnx && jpt >= 1 && jpt <= g.nny)
         fx_add(B.precip_fx + ((long long)(ipt - 1) + (long long)g.nnx * (jpt - 1)) * kFluxLimbs,
                (double)mult * (p.rhow * 2.0 / 3.0 * p.pi2 * cube(radius)));
 }
 
+// Where particle_exchange (particles.f90:1435-1495) sends a droplet that is
+// outside its subdomain after the non-periodic boundaries: 1 right (y above
+// ymax), 2 top right, 3 top (x above xmax), 4 top left, 5 left, 6 bottom
+// left, 7 bottom, 8 bottom right; 0 stays.  The tests are the reference's,
+// strict inequalities included (a droplet exactly on xmax or ymax stays).
+__device__ __forceinline__ int exchange_direction(const DevGrid &g, const double x[3]) {
+    if (x[1] > g.ymax) {
+        if (x[0] > g.xmax) return 2;
+        if (x[0] < g.xmin) return 8;
+        return 1;
+    }
+    if (x[1] < g.ymin) {
+        if (x[0] > g.xmax) return 4;
+        if (x[0] < g.xmin) return 6;
+        return 5;
+    }
+    if (x[0] > g.xmax && x[1] < g.ymax && x[1] > g.ymin) return 3;
+    if (x[0] < g.xmin && x[1] < g.ymax && x[1] > g.ymin) return 7;
+    return 0;
+}
+
 // particle_bcs_nonperiodic (reflect/kill) + particle_bcs_periodic for one
-// droplet (particles.f90:2683-2843); returns 0 if the droplet is killed.
+// droplet (particles.f90:2683-2843); returns 0 if the droplet is killed, 1
+// if it stays, 10 + direction if it leaves a subdomain (the direction is
+// taken before the periodic wrap, as particle_exchange runs before
+// particle_bcs_periodic, particles.f90:3248-3260).
 __device__ __forceinline__ int apply_bcs(const DevBox &B, const DevParams &p, double x[3], double v[3], double r) {
     const DevGrid &g = B.g;
     double top = (p.icase == 4) ? g.z[g.nnz - 1] - r : g.z[g.nnz] - r;
@@ -472,11 +496,12 @@ __device__ __forceinline__ int apply_bcs(const DevBox &B, const DevParams &p, do
             return 0;
         }
     }
+    const int dir = g.periodic ? 0 : exchange_direction(g, x);
     if (x[0] > g.xl) x[0] = x[0] - g.xl;
     else if (x[0] < 0) x[0] = g.xl + x[0];
     if (x[1] > g.yl) x[1] = x[1] - g.yl;
     else if (x[1] < 0) x[1] = g.yl + x[1];
-    return 1;
+    return dir ? 10 + dir : 1;
 }
 
 // Deposition payload (the droplet factors of particle_coupling_update,
@@ -547,8 +572,8 @@ __device__ __forceinline__ void write_payload_mixed(const DevBox &B, const DevPa
     const double taup_i = 18.0 * rhoa * p.nuf / rhop / ((2.0 * r) * (2.0 * r));
     const double H0 = p.rhow / rhoa * pi2 * 2.0 * (r * r) * radrhs;
     float *const *f = B.pay32.f;
-    f[P32_FX][t] = (float)((x[0] - g.dx * (double)(ipt - 1)) / g.dx);
-    f[P32_FY][t] = (float)((x[1] - g.dy * (double)(jpt - 1)) / g.dy);
+    f[P32_FX][t] = (float)((x[0] - g.dx * (double)(ipt + g.ioff - 1)) / g.dx);
+    f[P32_FY][t] = (float)((x[1] - g.dy * (double)(jpt + g.joff - 1)) / g.dy);
     f[P32_FZ][t] = (float)((x[2] - g.zz[kpt]) / g.dzu[kpt + 1]);
     for (int a = 0; a < 3; ++a) f[P32_DV0 + a][t] = (float)(partmass / rhoa * (vrhs[a] - p.g[a]) + H0 * v[a]);
     f[P32_T0][t] = (float)(Tprhs_s * 6.0 * p.rhow / rhop / p.CpaCpp / taup_i * (pi2 / 2.0) * r * p.nuf);
@@ -776,7 +801,14 @@ __device__ __forceinline__ int be_body(const DevBox &B, const DevParams &p, cons
     O.res[t] = res; O.actres[t] = actres; O.numact[t] = numact; O.mult[t] = multi; O.lid[t] = S.lid[s];
     O.Tf[t] = Tf; O.qstar[t] = qstar; O.Tpold[t] = Tpold; O.rold[t] = rold;
     int key;
-    if (!alive) {
+    if (alive >= 10) {
+        // leaves the subdomain: out of this box's list (with the killed),
+        // kept at its output slot for the exchange
+        key = (int)B.g.ncells + 1;
+        const int e = atomicAdd(B.nemig, 1);
+        B.emig_slot[e] = t;
+        B.emig_dir[e] = alive - 10;
+    } else if (!alive) {
         key = (int)B.g.ncells + 1;
         dc.v[C_DESTROY]++;
         record_kill(B, p, x, radius, rc, res, actres, numact, multi);

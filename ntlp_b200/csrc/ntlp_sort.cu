@@ -203,6 +203,7 @@ __global__ void k_reset_step(DevBox *boxes, int nbox) {
     if (threadIdx.x == 0) {
         *B.err = 0;
         *B.ndefer = 0;
+        if (B.nemig) *B.nemig = 0;
     }
 }
 
