@@ -89,6 +89,7 @@ def parse():
     ap.add_argument("--serve-depth", type=int, default=2)
     ap.add_argument("--serve-priorities", type=int, default=1)
     ap.add_argument("--serve-max-large", type=int, default=1)
+    ap.add_argument("--serve-max-active", type=int, default=4)
     ap.add_argument("--serve-ingest-priority", choices=["job", "high"], default="high")
     ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
                     help="run one precision only (profiling)")
@@ -340,7 +341,7 @@ def run_serving(args):
     jobs = serving.draw_jobs(args.serve_jobs, rate=args.serve_rate, seed=4)
     eng.stage(jobs)
     server = serving.Server(eng, hbm_budget=args.hbm_budget, max_active_droplets=args.serve_work_cap,
-                            depth=args.serve_depth,
+                            depth=args.serve_depth, max_active=args.serve_max_active,
                             max_large=args.serve_max_large if args.serve_max_large > 0 else None)
     clk = ClockSampler()
     clk.start()

@@ -167,7 +167,8 @@ __device__ int gauss_newton64(const DevParams &p, const Drop &d, const double ve
 // |det J| < 1e-5).  The residual is ie_vrt_nd with rhop*rnext/taup and
 // rhop/taup reduced to c_taup/(4 rnext) and c_taup/(4 rnext^2), and
 // VolP*rhop - m_s to VolP*rhow (identities of the definitions).  Both
-// iterations stop at |correction| < 1e-8 on the same root.
+// iterations converge to the same root; this one stops at |correction| < tol
+// (the reference's 1e-8, or 1e-6 after a converged FP32 phase).
 struct AdConst {
     double k_rpre;   // c_taup / (36 Sc rhow)
     double k_tpre;   // -CpaCpp c_taup / (12 Pra rhow)
@@ -226,7 +227,106 @@ __device__ __forceinline__ void resid_jac_ad(const DevParams &p, const Drop &d, 
     J[3] = 1.0 - d.h * Tprime_b;   // df2/db
 }
 
-__device__ int gauss_newton_ad(const DevParams &p, const Drop &d, const double vec1[2], double vec2[2]) {
+// FP32 copy of the residual's constants and of the droplet's state.
+struct AdConst32 {
+    float R, Tp, Tf, inv_Tf, qinf, h, t0r, rt0, t0T;
+    float k_rpre, k_tpre, k_rep, k_solv, k_clat, k_g, k_e1, k_q, sc6, pr6;
+};
+
+// resid_jac_ad in FP32 (same expressions; reciprocals by __frcp_rn).
+__device__ __forceinline__ void resid_jac_ad32(const AdConst32 &k, float a, float b, float f[2], float J[4]) {
+    const float R = k.R;
+    const float rn = a * R;
+    const float irn = __frcp_rn(rn);
+    const float Rep = k.k_rep * rn;
+    const float isRep = Rep > 0.f ? rsqrtf(Rep) : 0.f;
+    const float sRep = Rep * isRep;
+    const float sRep_a = 0.5f * k.k_rep * R * isRep;
+    const float Shp = 2.f + k.sc6 * sRep, Shp_a = k.sc6 * sRep_a;
+    const float Nup = 2.f + k.pr6 * sRep, Nup_a = k.pr6 * sRep_a;
+    const float rpre = k.k_rpre * Shp * irn;
+    const float rpre_a = k.k_rpre * (Shp_a - Shp * R * irn) * irn;
+    const float irn2 = irn * irn;
+    const float tpre = k.k_tpre * Nup * irn2;
+    const float tpre_a = k.k_tpre * (Nup_a - 2.f * Nup * R * irn) * irn2;
+    const float clat = k.k_clat * irn, clat_a = -clat * R * irn;
+    const float solterm = k.k_solv * (irn2 * irn);
+    const float solterm_a = -3.f * solterm * R * irn;
+    const float g = k.k_g * irn, g_a = -g * R * irn;
+    const float Tn = b * k.Tp;
+    const float iTn = __frcp_rn(Tn), iTn_b = -iTn * iTn * k.Tp;
+    const float E = k.k_e1 * (k.inv_Tf - iTn) + g * iTn - solterm;
+    const float E_a = g_a * iTn - solterm_a;
+    const float E_b = (g - k.k_e1) * iTn_b;
+    const float qstr = k.k_q * iTn * expf(E);
+    const float qstr_a = qstr * E_a;
+    const float qstr_b = qstr * (E_b - k.Tp * iTn);
+    const float dq = k.qinf - qstr;
+    const float rprime = rpre * dq * k.t0r;
+    const float rprime_a = (rpre_a * dq - rpre * qstr_a) * k.t0r;
+    const float rprime_b = -rpre * qstr_b * k.t0r;
+    const float Tprime = (tpre * (Tn - k.Tf) + clat * rprime * k.rt0) * k.t0T;
+    const float Tprime_a = (tpre_a * (Tn - k.Tf) + (clat_a * rprime + clat * rprime_a) * k.rt0) * k.t0T;
+    const float Tprime_b = (tpre * k.Tp + clat * rprime_b * k.rt0) * k.t0T;
+    f[0] = (a - 1.f) - k.h * rprime;
+    f[1] = (b - 1.f) - k.h * Tprime;
+    J[0] = 1.f - k.h * rprime_a;
+    J[1] = -k.h * Tprime_a;
+    J[2] = -k.h * rprime_b;
+    J[3] = 1.f - k.h * Tprime_b;
+}
+
+// First phase of the mixed solve: Gauss-Newton in FP32 from (a, b) until
+// the FP32 correction is below 1e-5 (at most 10 iterations).  Returns 1 and
+// the point in (a, b) when it converged to a point with both components
+// >= 0.01; 0 (a, b unchanged) when it did not, when the Jacobian is singular
+// or when a step leaves that range -- the FP64 phase then starts from the
+// original point with the reference's own rules.
+__device__ __forceinline__ int gauss_newton32(const DevParams &p, const Drop &d, double &a, double &b) {
+    AdConst32 k;
+    k.R = (float)d.radius;
+    k.Tp = (float)d.Tp;
+    k.Tf = (float)d.Tf;
+    k.inv_Tf = (float)d.inv_Tf;
+    k.qinf = (float)d.qinf;
+    k.h = (float)d.h;
+    k.t0r = (float)d.t0r;
+    k.rt0 = (float)d.rt0;
+    k.t0T = (float)d.t0T;
+    k.k_rpre = (float)(d.c_taup / (36.0 * p.Sc * p.rhow));
+    k.k_tpre = (float)(-p.CpaCpp * d.c_taup / (12.0 * p.Pra * p.rhow));
+    k.k_rep = (float)(2.0 * d.diffnorm / p.nuf);
+    k.k_solv = (float)(d.c_sol / p.rhow / ((2.0 / 3.0) * p.pi2));
+    k.k_clat = (float)(3.0 * p.Lv / p.Cpp);
+    k.k_g = (float)(2.0 * p.Mw * p.Gam / (p.Ru * p.rhow));
+    k.k_e1 = (float)(p.Lv * p.Mw / p.Ru);
+    k.k_q = (float)(p.Mw * d.esa / (p.Ru * d.rhoa));
+    k.sc6 = (float)(0.6 * p.Sc13);
+    k.pr6 = (float)(0.6 * p.Pra13);
+    float va = (float)a, vb = (float)b;
+    for (int it = 0; it < 10; ++it) {
+        float f[2], J[4];
+        resid_jac_ad32(k, va, vb, f, J);
+        const float det = J[0] * J[3] - J[2] * J[1];
+        if (!(fabsf(det) >= 1.0e-5f)) return 0;   // singular, or NaN
+        const float rd = __frcp_rn(det);
+        const float c1 = (J[3] * f[0] - J[2] * f[1]) * rd;
+        const float c2 = (J[0] * f[1] - J[1] * f[0]) * rd;
+        va -= c1;
+        vb -= c2;
+        if (!(va >= 0.01f && vb >= 0.01f)) return 0;   // out of range, or NaN
+        if (c1 * c1 + c2 * c2 < 1.0e-10f) {
+            a = (double)va;
+            b = (double)vb;
+            return 1;
+        }
+    }
+    return 0;
+}
+
+// tol: the stopping tolerance on |correction| (1e-8 in gauss_newton_2d).
+__device__ int gauss_newton_ad(const DevParams &p, const Drop &d, const double vec1[2], double vec2[2],
+                               double tol) {
     AdConst k;
     k.k_rpre = d.c_taup / (36.0 * p.Sc * p.rhow);
     k.k_tpre = -p.CpaCpp * d.c_taup / (12.0 * p.Pra * p.rhow);
@@ -263,7 +363,7 @@ __device__ int gauss_newton_ad(const DevParams &p, const Drop &d, const double v
             if (counts > 10) break;
         }
         if (vec2[0] < 0.01 || vec2[1] < 0.01 || ntlp_isnan(vec2[0]) || ntlp_isnan(vec2[1])) { flag = 1; break; }
-        if (sqrt(c1 * c1 + c2 * c2) < 1.0e-8) break;
+        if (sqrt(c1 * c1 + c2 * c2) < tol) break;
         v1a = vec2[0];
         v1b = vec2[1];
     }
@@ -683,7 +783,19 @@ __device__ __forceinline__ int be_body(const DevBox &B, const DevParams &p, cons
         D.t0r = taup0 / radius;
         D.rt0 = radius / taup0;
         D.t0T = taup0 / Tp;
-        int flag = MIXED ? gauss_newton_ad(p, D, rt_start, rtz) : gauss_newton64(p, D, rt_start, rtz);
+        int flag;
+        if (MIXED) {
+            // FP32 Gauss-Newton to within ~1e-6 of the root, then FP64
+            // iterations from there until the FP64 correction is below 1e-6
+            // (normally one: the point it returns is within ~|c|^2 of the
+            // root); without a converged FP32 phase, the FP64 iteration from
+            // the reference's start under its 1e-8 rule.
+            double gn0[2] = {rt_start[0], rt_start[1]};
+            const int ok32 = gauss_newton32(p, D, gn0[0], gn0[1]);
+            flag = gauss_newton_ad(p, D, gn0, rtz, ok32 ? 1.0e-6 : 1.0e-8);
+        } else {
+            flag = gauss_newton64(p, D, rt_start, rtz);
+        }
         if (flag == 1) {
             if (!ALLOW_LM) {
                 B.defer[atomicAdd(B.ndefer, 1)] = t;
