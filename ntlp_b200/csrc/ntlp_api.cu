@@ -337,6 +337,14 @@ void fill_devparams(const ntlp_params *p, DevParams &d) {
     d.CpaCpp = p->Cpa / p->Cpp;                       // les.F:10759
     d.Sc13 = ntlp_pow(p->Sc, 1.0 / 3.0);              // Sc**(1./3.)
     d.Pra13 = ntlp_pow(p->Pra, 1.0 / 3.0);            // Pra**(1./3.)
+    d.m_rpre = 1.0 / (36.0 * p->Sc * p->rhow);
+    d.m_tpre = -d.CpaCpp / (12.0 * p->Pra * p->rhow);
+    d.m_rep = 2.0 / p->nuf;
+    d.m_solv = 1.0 / (p->rhow * ((2.0 / 3.0) * p->pi2));
+    d.m_clat = 3.0 * p->Lv / p->Cpp;
+    d.m_g = 2.0 * p->Mw * p->Gam / (p->Ru * p->rhow);
+    d.m_e1 = p->Lv * p->Mw / p->Ru;
+    d.m_q = p->Mw / p->Ru;
     // set_binsdata calls of particles.f90:1909-1921
     d.hb[NTLP_H_ACTRES] = ntlp_hist_log_bins(1.0e-1, 1.0e4);
     d.hb[NTLP_H_RES] = ntlp_hist_log_bins(1.0e-1, 1.0e4);
@@ -851,13 +859,13 @@ int launch_step(ntlp_ctx *c, int kind, int istage, double dt, int32_t it, bool w
         if (c->params.precision == NTLP_PREC_MIXED)
             launch_update_be_mixed(c->params.ilin, nt, c->box_d, c->drop_tiles_d[c->nt_variant],
                                    c->n_drop_tiles[c->nt_variant], c->drop_tiles_d[0], c->n_drop_tiles[0], c->nbox,
-                                   c->dp_d, in, c->stream);
+                                   c->dp, in, c->stream);
         else
             launch_update_be64(c->params.ilin, nt, c->box_d, c->drop_tiles_d[c->nt_variant],
-                               c->n_drop_tiles[c->nt_variant], c->nbox, c->dp_d, in, c->stream);
+                               c->n_drop_tiles[c->nt_variant], c->nbox, c->dp, in, c->stream);
         c->launches += kUpdateLaunches;
     } else {
-        launch_update_rk3_64(c->params.ilin, c->box_d, c->drop_tiles_d[0], c->n_drop_tiles[0], c->dp_d, in,
+        launch_update_rk3_64(c->params.ilin, c->box_d, c->drop_tiles_d[0], c->n_drop_tiles[0], c->dp, in,
                              c->stream);
         c->launches += 1;
     }
@@ -871,9 +879,9 @@ int launch_step(ntlp_ctx *c, int kind, int istage, double dt, int32_t it, bool w
         e0 = phase_begin(c);
         const int v = c->dep_variant;
         if (c->params.precision == NTLP_PREC_MIXED)
-            launch_deposit_mixed(v, c->box_d, c->dep_tiles_d[v], c->n_dep_tiles[v], c->dp_d, c->stream);
+            launch_deposit_mixed(v, c->box_d, c->dep_tiles_d[v], c->n_dep_tiles[v], c->dp, c->stream);
         else
-            launch_deposit64(v, c->box_d, c->dep_tiles_d[v], c->n_dep_tiles[v], c->dp_d, c->stream);
+            launch_deposit64(v, c->box_d, c->dep_tiles_d[v], c->n_dep_tiles[v], c->dp, c->stream);
         phase_end(c, PH_DEPOSIT, e0);
         c->launches += 1;
     }
@@ -1182,9 +1190,9 @@ int ntlp_coupling(ntlp_ctx *c, double dt, int32_t layout, double *partsrc, doubl
     if (!c->payload_valid || c->last_dt != dt) {
         cudaEvent_t ep = phase_begin(c);
         if (c->params.precision == NTLP_PREC_MIXED)
-            launch_payload_mixed(c->box_d, c->drop_tiles_d[0], c->n_drop_tiles[0], c->dp_d, dt, c->stream);
+            launch_payload_mixed(c->box_d, c->drop_tiles_d[0], c->n_drop_tiles[0], c->dp, dt, c->stream);
         else
-            launch_payload64(c->box_d, c->drop_tiles_d[0], c->n_drop_tiles[0], c->dp_d, dt, c->stream);
+            launch_payload64(c->box_d, c->drop_tiles_d[0], c->n_drop_tiles[0], c->dp, dt, c->stream);
         phase_end(c, PH_OTHER, ep);
         c->launches += 1;
         c->payload_valid = true;
@@ -1193,9 +1201,9 @@ int ntlp_coupling(ntlp_ctx *c, double dt, int32_t layout, double *partsrc, doubl
     cudaEvent_t e0 = phase_begin(c);
     const int v = c->dep_variant;
     if (c->params.precision == NTLP_PREC_MIXED)
-        launch_deposit_mixed(v, c->box_d, c->dep_tiles_d[v], c->n_dep_tiles[v], c->dp_d, c->stream);
+        launch_deposit_mixed(v, c->box_d, c->dep_tiles_d[v], c->n_dep_tiles[v], c->dp, c->stream);
     else
-        launch_deposit64(v, c->box_d, c->dep_tiles_d[v], c->n_dep_tiles[v], c->dp_d, c->stream);
+        launch_deposit64(v, c->box_d, c->dep_tiles_d[v], c->n_dep_tiles[v], c->dp, c->stream);
     phase_end(c, PH_DEPOSIT, e0);
     c->launches += 1;
     CK(cudaGetLastError());

@@ -214,7 +214,7 @@ __host__ __device__ constexpr int dep_smem_bytes(bool mixed, int TX, int TY, int
 // tile shapes 2x4x32, 4x4x16 and 2x2x64 nodes are instantiated (autotuned).
 template <bool MIXED, int kDepTX, int kDepTY, int kDepTZ>
 __global__ void __launch_bounds__(kDepositThreads, MIXED ? 3 : 2)
-k_deposit_tiled(DevBox *boxes, const Tile *tiles, const DevParams *pp) {
+k_deposit_tiled(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevParams P) {
     static_assert(kDepTX * kDepTY * kDepTZ == kDepositThreads, "one thread per node of the tile");
     constexpr int kDepCols = (kDepTX + 1) * (kDepTY + 1);
     constexpr int kDepCSW = kDepTZ + 2;
@@ -229,7 +229,7 @@ k_deposit_tiled(DevBox *boxes, const Tile *tiles, const DevParams *pp) {
     __shared__ int s_total;
     const Tile tl = tiles[blockIdx.x];
     const DevBox &B = boxes[tl.box];
-    const DevParams &p = pp[0];
+    const DevParams &p = P;
     const DevGrid &g = B.g;
     const int ntz = (g.nz2 + kDepTZ - 1) / kDepTZ, nty = (g.sny + kDepTY - 1) / kDepTY;
     const int tzi = tl.start % ntz, tyi = (tl.start / ntz) % nty, txi = tl.start / (ntz * nty);

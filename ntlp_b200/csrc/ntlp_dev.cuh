@@ -69,6 +69,10 @@ struct DevParams {
     double radius_init, surf_rho, surf_p, tsfcc1, pi2;
     // derived on the host once: Cpa/Cpp (les.F:10759), Sc**(1./3.), Pra**(1./3.)
     double CpaCpp, Sc13, Pra13;
+    // mixed path only: per-run factors of the residual's constants
+    // 1/(36 Sc rhow), -CpaCpp/(12 Pra rhow), 2/nuf, 1/(rhow (2/3) pi2),
+    // 3 Lv/Cpp, 2 Mw Gam/(Ru rhow), Lv Mw/Ru, Mw/Ru
+    double m_rpre, m_tpre, m_rep, m_solv, m_clat, m_g, m_e1, m_q;
     // histogram binning (particles.f90:1909-1921), by NTLP_H_* kind
     ntlp_hbins hb[NTLP_H_STEP_KINDS];
 };

@@ -232,27 +232,27 @@ k_interp64(DevBox *boxes, const Tile *tiles) {
 
 template <int NT>
 __global__ void __launch_bounds__(NT, 512 / NT)
-k_be64(DevBox *boxes, const Tile *tiles, const DevParams *pp, StepIn in) {
+k_be64(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevParams P, StepIn in) {
     const Tile tl = tiles[blockIdx.x];
     const DevBox &B = boxes[tl.box];
     Counts cnt;
     for (int k = 0; k < kNumCounters; ++k) cnt.v[k] = 0;
     const int t = tl.start + threadIdx.x;
-    if (t < *B.n_alive) be_body<false, false>(B, pp[0], in, t, B.perm[t], cnt);
+    if (t < *B.n_alive) be_body<false, false>(B, P, in, t, B.perm[t], cnt);
     block_add_counters(B, cnt);
 }
 
 // droplets whose Gauss-Newton solve failed: the full body with the
 // Levenberg-Marquardt fallback (grid.y = box)
 __global__ void __launch_bounds__(kUpdateThreads)
-k_be_defer64(DevBox *boxes, const DevParams *pp, StepIn in) {
+k_be_defer64(DevBox *boxes, const __grid_constant__ DevParams P, StepIn in) {
     const DevBox &B = boxes[blockIdx.y];
     Counts cnt;
     for (int k = 0; k < kNumCounters; ++k) cnt.v[k] = 0;
     const int nd = *B.ndefer;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nd; i += gridDim.x * blockDim.x) {
         const int t = B.defer[i];
-        be_body<false, true>(B, pp[0], in, t, B.perm[t], cnt);
+        be_body<false, true>(B, P, in, t, B.perm[t], cnt);
     }
     block_add_counters(B, cnt);
 }
@@ -262,10 +262,10 @@ k_be_defer64(DevBox *boxes, const DevParams *pp, StepIn in) {
 // ---------------------------------------------------------------------------
 template <int ILIN>
 __global__ void __launch_bounds__(kUpdateThreads)
-k_update_rk3_64(DevBox *boxes, const Tile *tiles, const DevParams *pp, StepIn in) {
+k_update_rk3_64(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevParams P, StepIn in) {
     const Tile tl = tiles[blockIdx.x];
     const DevBox &B = boxes[tl.box];
-    const DevParams &p = pp[0];
+    const DevParams &p = P;
     Counts cnt;
     for (int k = 0; k < kNumCounters; ++k) cnt.v[k] = 0;
     const int t = tl.start + threadIdx.x;
@@ -384,10 +384,10 @@ k_update_rk3_64(DevBox *boxes, const Tile *tiles, const DevParams *pp, StepIn in
 // Payload from the stored state, for a coupling call whose dt differs from
 // the step's.  Runs after the finish kernel: st[cur] is the new state and
 // the payload is indexed like it.
-__global__ void k_payload64(DevBox *boxes, const Tile *tiles, const DevParams *pp, double dt) {
+__global__ void k_payload64(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevParams P, double dt) {
     const Tile tl = tiles[blockIdx.x];
     const DevBox &B = boxes[tl.box];
-    const DevParams &p = pp[0];
+    const DevParams &p = P;
     const int t = tl.start + threadIdx.x;
     if (t >= *B.n_alive) return;
     const DevState &S = B.st[B.cur];
@@ -401,40 +401,40 @@ __global__ void k_payload64(DevBox *boxes, const Tile *tiles, const DevParams *p
 // launchers
 // ---------------------------------------------------------------------------
 void launch_update_be64(int ilin, int nt, DevBox *boxes, const Tile *tiles, int ntiles, int nbox,
-                        const DevParams *pp, StepIn in, cudaStream_t st) {
+                        const DevParams &P, StepIn in, cudaStream_t st) {
     if (ntiles <= 0) return;
     if (nt == 256) {
         if (ilin == 1) k_interp64<1, 256><<<ntiles, 256, 0, st>>>(boxes, tiles);
         else k_interp64<0, 256><<<ntiles, 256, 0, st>>>(boxes, tiles);
-        k_be64<256><<<ntiles, 256, 0, st>>>(boxes, tiles, pp, in);
+        k_be64<256><<<ntiles, 256, 0, st>>>(boxes, tiles, P, in);
     } else {
         if (ilin == 1) k_interp64<1, 128><<<ntiles, 128, 0, st>>>(boxes, tiles);
         else k_interp64<0, 128><<<ntiles, 128, 0, st>>>(boxes, tiles);
-        k_be64<128><<<ntiles, 128, 0, st>>>(boxes, tiles, pp, in);
+        k_be64<128><<<ntiles, 128, 0, st>>>(boxes, tiles, P, in);
     }
-    k_be_defer64<<<dim3(kDeferBlocks, nbox), kUpdateThreads, 0, st>>>(boxes, pp, in);
+    k_be_defer64<<<dim3(kDeferBlocks, nbox), kUpdateThreads, 0, st>>>(boxes, P, in);
 }
 
-void launch_update_rk3_64(int ilin, DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp,
+void launch_update_rk3_64(int ilin, DevBox *boxes, const Tile *tiles, int ntiles, const DevParams &P,
                           StepIn in, cudaStream_t st) {
     if (ntiles <= 0) return;
     if (ilin == 1)
-        k_update_rk3_64<1><<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles, pp, in);
+        k_update_rk3_64<1><<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles, P, in);
     else
-        k_update_rk3_64<0><<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles, pp, in);
+        k_update_rk3_64<0><<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles, P, in);
 }
 
-void launch_payload64(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp, double dt,
+void launch_payload64(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams &P, double dt,
                       cudaStream_t st) {
     if (ntiles <= 0) return;
-    k_payload64<<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles, pp, dt);
+    k_payload64<<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles, P, dt);
 }
 
 template <int V>
-static void dep64(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp, cudaStream_t st) {
+static void dep64(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams &P, cudaStream_t st) {
     constexpr int TX = kDepShape[V][0], TY = kDepShape[V][1], TZ = kDepShape[V][2];
     k_deposit_tiled<false, TX, TY, TZ>
-        <<<ntiles, kDepositThreads, dep_smem_bytes(false, TX, TY, TZ), st>>>(boxes, tiles, pp);
+        <<<ntiles, kDepositThreads, dep_smem_bytes(false, TX, TY, TZ), st>>>(boxes, tiles, P);
 }
 
 template <int V>
@@ -453,13 +453,13 @@ void prepare_kernels64() {
     done = true;
 }
 
-void launch_deposit64(int variant, DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp,
+void launch_deposit64(int variant, DevBox *boxes, const Tile *tiles, int ntiles, const DevParams &P,
                       cudaStream_t st) {
     if (ntiles <= 0) return;
     prepare_kernels64();
-    if (variant == 1) dep64<1>(boxes, tiles, ntiles, pp, st);
-    else if (variant == 2) dep64<2>(boxes, tiles, ntiles, pp, st);
-    else dep64<0>(boxes, tiles, ntiles, pp, st);
+    if (variant == 1) dep64<1>(boxes, tiles, ntiles, P, st);
+    else if (variant == 2) dep64<2>(boxes, tiles, ntiles, P, st);
+    else dep64<0>(boxes, tiles, ntiles, P, st);
 }
 
 }  // namespace ntlp

@@ -36,20 +36,20 @@ struct StepIn {
 
 // FP64, reference operation order (ntlp_fp64.cu)
 void launch_update_be64(int ilin, int nt, DevBox *boxes, const Tile *tiles, int ntiles, int nbox,
-                        const DevParams *pp, StepIn in, cudaStream_t st);
-void launch_update_rk3_64(int ilin, DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp,
+                        const DevParams &P, StepIn in, cudaStream_t st);
+void launch_update_rk3_64(int ilin, DevBox *boxes, const Tile *tiles, int ntiles, const DevParams &P,
                           StepIn in, cudaStream_t st);
-void launch_payload64(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp, double dt,
+void launch_payload64(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams &P, double dt,
                       cudaStream_t st);
-void launch_deposit64(int variant, DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp,
+void launch_deposit64(int variant, DevBox *boxes, const Tile *tiles, int ntiles, const DevParams &P,
                       cudaStream_t st);
 
 // mixed precision (ntlp_mixed.cu)
 void launch_update_be_mixed(int ilin, int nt, DevBox *boxes, const Tile *tiles, int ntiles, const Tile *tiles128,
-                            int ntiles128, int nbox, const DevParams *pp, StepIn in, cudaStream_t st);
-void launch_payload_mixed(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp, double dt,
+                            int ntiles128, int nbox, const DevParams &P, StepIn in, cudaStream_t st);
+void launch_payload_mixed(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams &P, double dt,
                           cudaStream_t st);
-void launch_deposit_mixed(int variant, DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp,
+void launch_deposit_mixed(int variant, DevBox *boxes, const Tile *tiles, int ntiles, const DevParams &P,
                           cudaStream_t st);
 // one-time kernel attributes (dynamic shared memory of the deposition);
 // call outside stream capture

@@ -218,25 +218,25 @@ k_interp_mixed(DevBox *boxes, const Tile *tiles) {
 
 // 5 resident blocks of 128: 94 registers, 20 warps per SM, no spills
 __global__ void __launch_bounds__(128, 5)
-k_be_mixed(DevBox *boxes, const Tile *tiles, const DevParams *pp, StepIn in) {
+k_be_mixed(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevParams P, StepIn in) {
     const Tile tl = tiles[blockIdx.x];
     const DevBox &B = boxes[tl.box];
     Counts cnt;
     for (int k = 0; k < kNumCounters; ++k) cnt.v[k] = 0;
     const int t = tl.start + threadIdx.x;
-    if (t < *B.n_alive) be_body<true, false>(B, pp[0], in, t, B.perm[t], cnt);
+    if (t < *B.n_alive) be_body<true, false>(B, P, in, t, B.perm[t], cnt);
     block_add_counters(B, cnt);
 }
 
 __global__ void __launch_bounds__(kUpdateThreads)
-k_be_defer_mixed(DevBox *boxes, const DevParams *pp, StepIn in) {
+k_be_defer_mixed(DevBox *boxes, const __grid_constant__ DevParams P, StepIn in) {
     const DevBox &B = boxes[blockIdx.y];
     Counts cnt;
     for (int k = 0; k < kNumCounters; ++k) cnt.v[k] = 0;
     const int nd = *B.ndefer;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nd; i += gridDim.x * blockDim.x) {
         const int t = B.defer[i];
-        be_body<true, true>(B, pp[0], in, t, B.perm[t], cnt);
+        be_body<true, true>(B, P, in, t, B.perm[t], cnt);
     }
     block_add_counters(B, cnt);
 }
@@ -246,7 +246,7 @@ k_be_defer_mixed(DevBox *boxes, const DevParams *pp, StepIn in) {
 // arithmetic may be contracted by the code generator, and one register
 // budget for every tuning choice keeps the results identical across them.
 void launch_update_be_mixed(int ilin, int nt, DevBox *boxes, const Tile *tiles, int ntiles, const Tile *tiles128,
-                            int ntiles128, int nbox, const DevParams *pp, StepIn in, cudaStream_t st) {
+                            int ntiles128, int nbox, const DevParams &P, StepIn in, cudaStream_t st) {
     if (ntiles <= 0) return;
     if (nt == 256) {
         if (ilin == 1) k_interp_mixed<1, 256><<<ntiles, 256, 0, st>>>(boxes, tiles);
@@ -255,13 +255,13 @@ void launch_update_be_mixed(int ilin, int nt, DevBox *boxes, const Tile *tiles, 
         if (ilin == 1) k_interp_mixed<1, 128><<<ntiles, 128, 0, st>>>(boxes, tiles);
         else k_interp_mixed<0, 128><<<ntiles, 128, 0, st>>>(boxes, tiles);
     }
-    k_be_mixed<<<ntiles128, 128, 0, st>>>(boxes, tiles128, pp, in);
-    k_be_defer_mixed<<<dim3(kDeferBlocks, nbox), kUpdateThreads, 0, st>>>(boxes, pp, in);
+    k_be_mixed<<<ntiles128, 128, 0, st>>>(boxes, tiles128, P, in);
+    k_be_defer_mixed<<<dim3(kDeferBlocks, nbox), kUpdateThreads, 0, st>>>(boxes, P, in);
 }
 
 // Mixed payload from the stored state, for a coupling call whose dt differs
 // from the step's (runs after the finish kernel: st[cur] is the new state).
-__global__ void k_payload_mixed(DevBox *boxes, const Tile *tiles, const DevParams *pp, double dt) {
+__global__ void k_payload_mixed(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevParams P, double dt) {
     const Tile tl = tiles[blockIdx.x];
     const DevBox &B = boxes[tl.box];
     const int t = tl.start + threadIdx.x;
@@ -272,20 +272,20 @@ __global__ void k_payload_mixed(DevBox *boxes, const Tile *tiles, const DevParam
     for (int a = 0; a < 3; ++a) { x[a] = S.x[a][s]; v[a] = S.v[a][s]; vold[a] = S.vold[a][s]; }
     int ipt, jpt, kpt;
     if (cell_key(B.g, x[0], x[1], x[2], &ipt, &jpt, &kpt) >= (int)B.g.ncells) return;
-    write_payload_mixed(B, pp[0], s, ipt, jpt, kpt, x, v, vold, S.r[s], S.rold[s], S.Tp[s], S.Tpold[s], S.Tf[s],
+    write_payload_mixed(B, P, s, ipt, jpt, kpt, x, v, vold, S.r[s], S.rold[s], S.Tp[s], S.Tpold[s], S.Tf[s],
                         S.m_s[s], S.mult[s], dt);
 }
 
-void launch_payload_mixed(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp, double dt,
+void launch_payload_mixed(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams &P, double dt,
                           cudaStream_t st) {
-    if (ntiles > 0) k_payload_mixed<<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles, pp, dt);
+    if (ntiles > 0) k_payload_mixed<<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles, P, dt);
 }
 
 template <int V>
-static void depm(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp, cudaStream_t st) {
+static void depm(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams &P, cudaStream_t st) {
     constexpr int TX = kDepShape[V][0], TY = kDepShape[V][1], TZ = kDepShape[V][2];
     k_deposit_tiled<true, TX, TY, TZ>
-        <<<ntiles, kDepositThreads, dep_smem_bytes(true, TX, TY, TZ), st>>>(boxes, tiles, pp);
+        <<<ntiles, kDepositThreads, dep_smem_bytes(true, TX, TY, TZ), st>>>(boxes, tiles, P);
 }
 
 template <int V>
@@ -304,13 +304,13 @@ void prepare_kernels_mixed() {
     done = true;
 }
 
-void launch_deposit_mixed(int variant, DevBox *boxes, const Tile *tiles, int ntiles, const DevParams *pp,
+void launch_deposit_mixed(int variant, DevBox *boxes, const Tile *tiles, int ntiles, const DevParams &P,
                           cudaStream_t st) {
     if (ntiles <= 0) return;
     prepare_kernels_mixed();
-    if (variant == 1) depm<1>(boxes, tiles, ntiles, pp, st);
-    else if (variant == 2) depm<2>(boxes, tiles, ntiles, pp, st);
-    else depm<0>(boxes, tiles, ntiles, pp, st);
+    if (variant == 1) depm<1>(boxes, tiles, ntiles, P, st);
+    else if (variant == 2) depm<2>(boxes, tiles, ntiles, P, st);
+    else depm<0>(boxes, tiles, ntiles, P, st);
 }
 
 }  // namespace ntlp

@@ -237,8 +237,8 @@ extern "C" int ntlp_coupling_noalloc(const ntlp_grid *grid, const ntlp_params *p
     launch_keys_initial(B_d, drop_tiles, nd, st);
     launch_sort(B_d, plan, st);
     launch_finish(B_d, 1, st);
-    launch_payload64(B_d, drop_tiles, nd, P_d, dt, st);
-    launch_deposit64(0, B_d, node_tiles, nn, P_d, st);
+    launch_payload64(B_d, drop_tiles, nd, dp, dt, st);
+    launch_deposit64(0, B_d, node_tiles, nn, dp, st);
     e = cudaGetLastError();
     if (e != cudaSuccess) {
         fprintf(stderr, "ntlp_coupling_noalloc: %s\n", cudaGetErrorString(e));

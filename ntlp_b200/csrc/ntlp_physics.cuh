@@ -173,14 +173,26 @@ struct AdConst {
     double k_rpre;   // c_taup / (36 Sc rhow)
     double k_tpre;   // -CpaCpp c_taup / (12 Pra rhow)
     double k_rep;    // 2 diffnorm / nuf
-    double k_vol;    // (2/3) pi2
-    double k_sol;    // c_sol / rhow
-    double k_solv;   // k_sol / k_vol
+    double k_solv;   // c_sol / (rhow (2/3) pi2)
     double k_clat;   // 3 Lv / Cpp
     double k_g;      // 2 Mw Gam / (Ru rhow)
     double k_e1;     // Lv Mw / Ru
     double k_q;      // Mw esa / (Ru rhoa)
 };
+
+// the droplet's constants from the per-run factors of DevParams (m_*)
+__device__ __forceinline__ AdConst ad_const(const DevParams &p, const Drop &d) {
+    AdConst k;
+    k.k_rpre = d.c_taup * p.m_rpre;
+    k.k_tpre = d.c_taup * p.m_tpre;
+    k.k_rep = d.diffnorm * p.m_rep;
+    k.k_solv = d.c_sol * p.m_solv;
+    k.k_clat = p.m_clat;
+    k.k_g = p.m_g;
+    k.k_e1 = p.m_e1;
+    k.k_q = p.m_q * d.esa / d.rhoa;
+    return k;
+}
 
 __device__ __forceinline__ void resid_jac_ad(const DevParams &p, const Drop &d, const AdConst &k, double a,
                                              double b, double f[2], double J[4]) {
@@ -282,7 +294,8 @@ __device__ __forceinline__ void resid_jac_ad32(const AdConst32 &k, float a, floa
 // >= 0.01; 0 (a, b unchanged) when it did not, when the Jacobian is singular
 // or when a step leaves that range -- the FP64 phase then starts from the
 // original point with the reference's own rules.
-__device__ __forceinline__ int gauss_newton32(const DevParams &p, const Drop &d, double &a, double &b) {
+__device__ __forceinline__ int gauss_newton32(const DevParams &p, const Drop &d, const AdConst &c, double &a,
+                                              double &b) {
     AdConst32 k;
     k.R = (float)d.radius;
     k.Tp = (float)d.Tp;
@@ -293,14 +306,14 @@ __device__ __forceinline__ int gauss_newton32(const DevParams &p, const Drop &d,
     k.t0r = (float)d.t0r;
     k.rt0 = (float)d.rt0;
     k.t0T = (float)d.t0T;
-    k.k_rpre = (float)(d.c_taup / (36.0 * p.Sc * p.rhow));
-    k.k_tpre = (float)(-p.CpaCpp * d.c_taup / (12.0 * p.Pra * p.rhow));
-    k.k_rep = (float)(2.0 * d.diffnorm / p.nuf);
-    k.k_solv = (float)(d.c_sol / p.rhow / ((2.0 / 3.0) * p.pi2));
-    k.k_clat = (float)(3.0 * p.Lv / p.Cpp);
-    k.k_g = (float)(2.0 * p.Mw * p.Gam / (p.Ru * p.rhow));
-    k.k_e1 = (float)(p.Lv * p.Mw / p.Ru);
-    k.k_q = (float)(p.Mw * d.esa / (p.Ru * d.rhoa));
+    k.k_rpre = (float)c.k_rpre;
+    k.k_tpre = (float)c.k_tpre;
+    k.k_rep = (float)c.k_rep;
+    k.k_solv = (float)c.k_solv;
+    k.k_clat = (float)c.k_clat;
+    k.k_g = (float)c.k_g;
+    k.k_e1 = (float)c.k_e1;
+    k.k_q = (float)c.k_q;
     k.sc6 = (float)(0.6 * p.Sc13);
     k.pr6 = (float)(0.6 * p.Pra13);
     float va = (float)a, vb = (float)b;
@@ -325,19 +338,8 @@ __device__ __forceinline__ int gauss_newton32(const DevParams &p, const Drop &d,
 }
 
 // tol: the stopping tolerance on |correction| (1e-8 in gauss_newton_2d).
-__device__ int gauss_newton_ad(const DevParams &p, const Drop &d, const double vec1[2], double vec2[2],
-                               double tol) {
-    AdConst k;
-    k.k_rpre = d.c_taup / (36.0 * p.Sc * p.rhow);
-    k.k_tpre = -p.CpaCpp * d.c_taup / (12.0 * p.Pra * p.rhow);
-    k.k_rep = 2.0 * d.diffnorm / p.nuf;
-    k.k_vol = (2.0 / 3.0) * p.pi2;
-    k.k_sol = d.c_sol / p.rhow;
-    k.k_solv = k.k_sol / k.k_vol;
-    k.k_clat = 3.0 * p.Lv / p.Cpp;
-    k.k_g = 2.0 * p.Mw * p.Gam / (p.Ru * p.rhow);
-    k.k_e1 = p.Lv * p.Mw / p.Ru;
-    k.k_q = p.Mw * d.esa / (p.Ru * d.rhoa);
+__device__ int gauss_newton_ad(const DevParams &p, const Drop &d, const AdConst &k, const double vec1[2],
+                               double vec2[2], double tol) {
     int iterations = 0, flag = 0;
     double v1a = vec1[0], v1b = vec1[1];
     vec2[0] = 0.0;
@@ -748,6 +750,7 @@ __device__ __forceinline__ int be_body(const DevBox &B, const DevParams &p, cons
     // ---- phase 1: the radius/temperature solve --------------------------
     int solved = 0;                 // 1: rtz holds the solve's result
     double rtz[2] = {1.0, 1.0};
+    double esa1 = 0.0;              // mod_magnus(Tf) of the solve (same Tf as phase 2)
     int n100 = 0, nimpos = 0;
     if (p.ievap == 1 && O.qinf[t] > 0.0) {
         double Tf = O.Tf[t];
@@ -762,6 +765,7 @@ __device__ __forceinline__ int be_body(const DevBox &B, const DevParams &p, cons
         be_drag<MIXED>(p, radius, m_s, rhoa, dt, v, uf);
         const double taup0 = taup0_64(p, m_s, rhoa);
         const double esa = mod_magnus64(Tf);
+        esa1 = esa;
         int mflag;
         double guess = MIXED ? rad_solver2_32(p, Tf, qinf, rhoa, m_s, kap, radius, esa, mflag)
                              : rad_solver2_64(p, Tf, qinf, rhoa, m_s, kap, radius, esa, mflag);
@@ -790,9 +794,10 @@ __device__ __forceinline__ int be_body(const DevBox &B, const DevParams &p, cons
             // (normally one: the point it returns is within ~|c|^2 of the
             // root); without a converged FP32 phase, the FP64 iteration from
             // the reference's start under its 1e-8 rule.
+            const AdConst kc = ad_const(p, D);
             double gn0[2] = {rt_start[0], rt_start[1]};
-            const int ok32 = gauss_newton32(p, D, gn0[0], gn0[1]);
-            flag = gauss_newton_ad(p, D, gn0, rtz, ok32 ? 1.0e-6 : 1.0e-8);
+            const int ok32 = gauss_newton32(p, D, kc, gn0[0], gn0[1]);
+            flag = gauss_newton_ad(p, D, kc, gn0, rtz, ok32 ? 1.0e-6 : 1.0e-8);
         } else {
             flag = gauss_newton64(p, D, rt_start, rtz);
         }
@@ -863,7 +868,7 @@ __device__ __forceinline__ int be_body(const DevBox &B, const DevParams &p, cons
     }
     Volp = p.pi2 * 2.0 / 3.0 * cube(radius);
     rhop = (m_s + Volp * p.rhow) / Volp;
-    double einf = mod_magnus64(Tf);
+    const double einf = solved ? esa1 : mod_magnus64(Tf);
     double qstar = (p.Mw / (p.Ru * Tp * rhoa)) * einf *
                    ntlp_exp(((p.Lv * p.Mw / p.Ru) * ((1.0 / Tf) - (1.0 / Tp))) +
                             ((2.0 * p.Mw * p.Gam) / (p.Ru * p.rhow * radius * Tp)) -
