@@ -23,6 +23,7 @@
 #include <cstdarg>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -87,6 +88,8 @@ struct ntlp_ctx {
     cudaGraphExec_t gexec = nullptr;
     double g_dt = 0.0;
     int g_nsteps = 0, g_dep = -1, g_nt = -1;
+    bool tex_all = true;   // every box's FP32 fields have a texture (mixed)
+    int64_t g_launches = 0;
     int64_t bytes = 0;
     std::string err;
     // instrumentation
@@ -121,7 +124,7 @@ int fail(ntlp_ctx *c, int code, const char *fmt, ...) {
     } while (0)
 
 constexpr int kLutPerLevel = 4;    // search buckets per vertical level
-constexpr int kF32Guard = 8;       // guard elements around the FP32 field copies
+constexpr int kF32Guard = kF32GuardDev;   // guard elements around the FP32 field copies
 
 // Two-pass carving of one allocation: the first pass (base == nullptr) only
 // sums sizes, the second hands out 256-byte aligned pointers.
@@ -135,6 +138,28 @@ struct Carver {
         off += bytes;
     }
 };
+
+// f4 (count elements from its first guard element) as a 1D linear texture
+// of float4, read element by element; 0 when the device refuses it
+// (alignment, size)
+unsigned long long f4_texture(const float4 *base, size_t count) {
+    cudaResourceDesc rd{};
+    rd.resType = cudaResourceTypeLinear;
+    rd.res.linear.devPtr = (void *)base;
+    rd.res.linear.desc = cudaCreateChannelDesc<float4>();
+    rd.res.linear.sizeInBytes = count * sizeof(float4);
+    cudaTextureDesc td{};
+    td.addressMode[0] = cudaAddressModeClamp;
+    td.filterMode = cudaFilterModePoint;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 0;
+    cudaTextureObject_t t = 0;
+    if (cudaCreateTextureObject(&t, &rd, &td, nullptr) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return (unsigned long long)t;
+}
 
 void carve_state(Carver &cv, DevState &s, size_t n) {
     for (int a = 0; a < 3; ++a) {
@@ -177,7 +202,10 @@ void carve_box(Carver &cv, BoxHost &h, DevBox &B, bool mixed) {
         // after the last (with zero weight); the guards keep them in bounds
         float4 *f4;
         float *fw;
-        cv.take(&f4, npad + 2 * kF32Guard);
+        // + 1 KB, to start the texture on a 1 KB boundary (the device's
+        // texture alignment is smaller)
+        cv.take(&f4, npad + 2 * kF32Guard + 64);
+        if (f4) f4 = (float4 *)(((uintptr_t)f4 + 1023) & ~(uintptr_t)1023);
         cv.take(&fw, npad + 2 * kF32Guard);
         if (cv.base) {
             B.f4 = f4 + kF32Guard;
@@ -458,6 +486,8 @@ extern "C" void ntlp_ctx_destroy(ntlp_ctx *c) {
         cudaEventDestroy(r.b);
     }
     for (cudaEvent_t e : c->pool) cudaEventDestroy(e);
+    for (const DevBox &B : c->box)
+        if (B.tex_f4) cudaDestroyTextureObject((cudaTextureObject_t)B.tex_f4);
     for (auto &h : c->bh) {
         if (h.arena) cudaFreeAsync(h.arena, c->stream);
         if (h.arena_rk3) cudaFreeAsync(h.arena_rk3, c->stream);
@@ -582,6 +612,8 @@ int create(int nbox, const ntlp_grid *grids, const ntlp_params *params, const in
             if (cudaMemsetAsync((void *)(B.f4 - kF32Guard), 0, npad * sizeof(float4), c->stream) ||
                 cudaMemsetAsync((void *)(B.fw - kF32Guard), 0, npad * sizeof(float), c->stream))
                 return bail(fail(c, NTLP_ERR_CUDA, "initialising box %d failed", b));
+            B.tex_f4 = f4_texture(B.f4 - kF32Guard, npad);
+            if (!B.tex_f4) c->tex_all = false;
         }
         if (cudaMemcpyAsync((void *)B.g.lut_zz, h.lut.data(), h.lut.size() * sizeof(int), cudaMemcpyHostToDevice,
                             c->stream) ||
@@ -859,7 +891,7 @@ int launch_step(ntlp_ctx *c, int kind, int istage, double dt, int32_t it, bool w
         if (c->params.precision == NTLP_PREC_MIXED)
             launch_update_be_mixed(c->params.ilin, nt, c->box_d, c->drop_tiles_d[c->nt_variant],
                                    c->n_drop_tiles[c->nt_variant], c->drop_tiles_d[0], c->n_drop_tiles[0], c->nbox,
-                                   c->dp, in, c->stream);
+                                   c->dp, in, c->stream, c->tex_all);
         else
             launch_update_be64(c->params.ilin, nt, c->box_d, c->drop_tiles_d[c->nt_variant],
                                c->n_drop_tiles[c->nt_variant], c->nbox, c->dp, in, c->stream);
@@ -1278,6 +1310,7 @@ int ntlp_advance_graph(ntlp_ctx *c, double dt, int32_t it, int32_t nsteps) {
         cudaGraph_t graph = nullptr;
         cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
         c->prof = prof;
+        c->g_launches = c->launches - launches;   // kernels in the graph
         c->launches = launches;
         if (lrc) {
             if (graph) cudaGraphDestroy(graph);
@@ -1298,7 +1331,7 @@ int ntlp_advance_graph(ntlp_ctx *c, double dt, int32_t it, int32_t nsteps) {
     cudaEvent_t e0 = phase_begin(c);
     CK(cudaGraphLaunch(c->gexec, c->stream));
     phase_end(c, PH_OTHER, e0);
-    c->launches += (int64_t)nsteps * (1 + kUpdateLaunches + 1 + kSortLaunches + 1);
+    c->launches += c->g_launches;
     mirror_flip(c, nsteps);
     c->payload_valid = true;
     c->last_dt = dt;

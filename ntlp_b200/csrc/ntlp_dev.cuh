@@ -101,11 +101,16 @@ struct DevPayload32 {
     float *f[P32_N];
 };
 
+constexpr int kF32GuardDev = 8;   // guard elements before the FP32 field copies
+
 struct DevBox {
     DevGrid g;
     const double *f[5];    // u v w T q, halo-padded FP64
     const float4 *f4;      // mixed path: (u, v, T, q) deviations packed per point
     const float *fw;       // mixed path: w deviation
+    // mixed path: f4 as a 1D linear texture (element 0 = the first guard
+    // element, f4 - kF32GuardDev), 0 when the device refused it
+    unsigned long long tex_f4;
     DevState st[2];
     DevPayload pay;
     DevPayload32 pay32;    // mixed path

@@ -46,7 +46,8 @@ void launch_deposit64(int variant, DevBox *boxes, const Tile *tiles, int ntiles,
 
 // mixed precision (ntlp_mixed.cu)
 void launch_update_be_mixed(int ilin, int nt, DevBox *boxes, const Tile *tiles, int ntiles, const Tile *tiles128,
-                            int ntiles128, int nbox, const DevParams &P, StepIn in, cudaStream_t st);
+                            int ntiles128, int nbox, const DevParams &P, StepIn in, cudaStream_t st,
+                            bool tex);
 void launch_payload_mixed(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams &P, double dt,
                           cudaStream_t st);
 void launch_deposit_mixed(int variant, DevBox *boxes, const Tile *tiles, int ntiles, const DevParams &P,

@@ -65,6 +65,7 @@ __device__ __forceinline__ void lagrange6_win(double x, const double *lev, int k
 // every column is read as one contiguous 6-level window; the window may
 // reach outside the column (into the neighbour or the guard elements) only
 // where the weight is 0.
+template <bool TEX>
 __device__ void interp6_mixed(const DevBox &B, double x1, double x2, double x3, Interp &o, int &bad) {
     const DevGrid &g = B.g;
     const int nnz = g.nnz;
@@ -106,9 +107,14 @@ __device__ void interp6_mixed(const DevBox &B, double x1, double x2, double x3, 
             if (iy < -1 || iy > g.nny + 3) { bad = 1; iy = iy < -1 ? -1 : g.nny + 3; }
             const long long base = (long long)g.nz2 * ((long long)(iy + 1) + (long long)g.ny5 * (ix + 1));
             float au = 0.f, av = 0.f, aT = 0.f, aq = 0.f, aw = 0.f;
+            // TEX: the first two y-columns through the texture path (its
+            // own L1 data pipe; the values are the same elements)
+            const bool tex = TEX && j < 2;
+            const int tbase = (int)(base + (cu - 2) + kF32GuardDev);
 #pragma unroll
             for (int k = 0; k < 6; ++k) {
-                const float4 val = __ldg(f4 + base + k);
+                const float4 val = tex ? tex1Dfetch<float4>((cudaTextureObject_t)B.tex_f4, tbase + k)
+                                       : __ldg(f4 + base + k);
                 au = fmaf(val.x, wz[k], au);
                 av = fmaf(val.y, wz[k], av);
                 aT = fmaf(val.z, wz[k], aT);
@@ -194,7 +200,7 @@ __device__ void interp_lin_mixed(const DevBox &B, double x1, double x2, double x
     o.qinf = B.f[4][ridx] + (double)q;
 }
 
-template <int ILIN, int NT>
+template <int ILIN, int NT, bool TEX>
 __global__ void __launch_bounds__(NT, 512 / NT)
 k_interp_mixed(DevBox *boxes, const Tile *tiles) {
     const Tile tl = tiles[blockIdx.x];
@@ -207,7 +213,7 @@ k_interp_mixed(DevBox *boxes, const Tile *tiles) {
     Interp I;
     int bad = 0;
     if (ILIN == 1) interp_lin_mixed(B, S.x[0][s], S.x[1][s], S.x[2][s], I, bad);
-    else interp6_mixed(B, S.x[0][s], S.x[1][s], S.x[2][s], I, bad);
+    else interp6_mixed<TEX>(B, S.x[0][s], S.x[1][s], S.x[2][s], I, bad);
     O.uf[0][t] = I.uf[0];
     O.uf[1][t] = I.uf[1];
     O.uf[2][t] = I.uf[2];
@@ -246,14 +252,16 @@ k_be_defer_mixed(DevBox *boxes, const __grid_constant__ DevParams P, StepIn in) 
 // arithmetic may be contracted by the code generator, and one register
 // budget for every tuning choice keeps the results identical across them.
 void launch_update_be_mixed(int ilin, int nt, DevBox *boxes, const Tile *tiles, int ntiles, const Tile *tiles128,
-                            int ntiles128, int nbox, const DevParams &P, StepIn in, cudaStream_t st) {
+                            int ntiles128, int nbox, const DevParams &P, StepIn in, cudaStream_t st, bool tex) {
     if (ntiles <= 0) return;
     if (nt == 256) {
-        if (ilin == 1) k_interp_mixed<1, 256><<<ntiles, 256, 0, st>>>(boxes, tiles);
-        else k_interp_mixed<0, 256><<<ntiles, 256, 0, st>>>(boxes, tiles);
+        if (ilin == 1) k_interp_mixed<1, 256, false><<<ntiles, 256, 0, st>>>(boxes, tiles);
+        else if (tex) k_interp_mixed<0, 256, true><<<ntiles, 256, 0, st>>>(boxes, tiles);
+        else k_interp_mixed<0, 256, false><<<ntiles, 256, 0, st>>>(boxes, tiles);
     } else {
-        if (ilin == 1) k_interp_mixed<1, 128><<<ntiles, 128, 0, st>>>(boxes, tiles);
-        else k_interp_mixed<0, 128><<<ntiles, 128, 0, st>>>(boxes, tiles);
+        if (ilin == 1) k_interp_mixed<1, 128, false><<<ntiles, 128, 0, st>>>(boxes, tiles);
+        else if (tex) k_interp_mixed<0, 128, true><<<ntiles, 128, 0, st>>>(boxes, tiles);
+        else k_interp_mixed<0, 128, false><<<ntiles, 128, 0, st>>>(boxes, tiles);
     }
     k_be_mixed<<<ntiles128, 128, 0, st>>>(boxes, tiles128, P, in);
     k_be_defer_mixed<<<dim3(kDeferBlocks, nbox), kUpdateThreads, 0, st>>>(boxes, P, in);
