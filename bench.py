@@ -205,6 +205,12 @@ def run_device(case, precision: str, args, dist, rank):
         s.particle_update_BE(case.dt, it, counters=False)
         s.particle_coupling_update(case.dt, download=False)
         it += 1
+    tune = None
+    if args.tune_steps > 0:
+        # the library's autotuner on this box (deposition tile shape,
+        # interpolation block size); untimed, like the warm-up
+        tune = s.autotune(case.dt, it, steps=args.tune_steps)
+        it += 5 * (args.tune_steps + 1)
     s.sync()
     n0 = s.numpart
     s.profile(True)
@@ -230,7 +236,7 @@ def run_device(case, precision: str, args, dist, rank):
     n1 = s.numpart
     ms_max = max_over_ranks(dist, ms)
     s.close()
-    return dict(ms=ms_max, n0=n0, n1=n1, prof=prof, clocks=clocks)
+    return dict(ms=ms_max, n0=n0, n1=n1, prof=prof, clocks=clocks, tune=tune)
 
 
 def run_e2e(case, args, dist):
@@ -257,6 +263,9 @@ def run_e2e(case, args, dist):
         s.particle_update_BE(case.dt, it, counters=False)
         s.particle_coupling_update(case.dt, out=[mom] + rest)
         it += 1
+    if args.tune_steps > 0:
+        s.autotune(case.dt, it, steps=args.tune_steps)
+        it += 5 * (args.tune_steps + 1)
     n0 = s.numpart
     barrier(dist)
     t0 = time.perf_counter()
@@ -499,6 +508,9 @@ def main():
                    "droplets": n, "grid": [g["nnx"], g["nny"], g["nnz"]],
                    "l2": "state (~3.5 GB) >> L2; no flush needed", "parallelism": f"{ws} replica(s)"},
         "phases_ms_per_step": {k: v / args.steps for k, v in r["prof"].items() if k.endswith("_ms")},
+        "autotune": (None if not r.get("tune") else
+                     {"deposit_shape": ["2x4x32", "4x4x16", "2x2x64"][r["tune"]["deposit_variant"]],
+                      "block": [128, 256][r["tune"]["block_variant"]]}),
         "gpu_launches": int(r["prof"]["launches"]),
         "roofline": {"bound": "hbm",
                      "kernel": ("update phase: k_interp_mixed + k_be_mixed + k_be_defer_mixed" if head == "mixed"

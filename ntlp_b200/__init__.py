@@ -329,6 +329,15 @@ class DropletStep:
         self._check(self.L.ntlp_flux(self.h, *(abi.as_dptr(a) for a in out)), "ntlp_flux")
         return out
 
+    def autotune(self, dt: float, it: int, steps: int = 2) -> dict:
+        """Time the deposition tile shapes and droplet block sizes on this
+        context's boxes (the state advances by 5 * (steps + 1) steps) and keep the
+        fastest."""
+        choice = (C.c_int32 * 2)()
+        ms = (C.c_double * 5)()
+        self._check(self.L.ntlp_autotune(self.h, float(dt), int(it), int(steps), choice, ms), "ntlp_autotune")
+        return dict(deposit_variant=int(choice[0]), block_variant=int(choice[1]), ms=list(ms))
+
 
 class DropletBatch(DropletStep):
     """Many independent boxes (each its own grid, fields and droplets; shared
@@ -416,15 +425,6 @@ class DropletBatch(DropletStep):
         """nsteps of particle_update_BE + particle_coupling_update for every
         box, replayed as one CUDA graph launch (queued, not waited for)."""
         self._check(self.L.ntlp_advance_graph(self.h, float(dt), int(it), int(nsteps)), "ntlp_advance_graph")
-
-    def autotune(self, dt: float, it: int, steps: int = 2) -> dict:
-        """Time the deposition tile shapes and droplet block sizes on these
-        boxes (the state advances by 5 * (steps + 1) steps) and keep the
-        fastest."""
-        choice = (C.c_int32 * 2)()
-        ms = (C.c_double * 5)()
-        self._check(self.L.ntlp_autotune(self.h, float(dt), int(it), int(steps), choice, ms), "ntlp_autotune")
-        return dict(deposit_variant=int(choice[0]), block_variant=int(choice[1]), ms=list(ms))
 
 
 class SubdomainStep(DropletStep):
