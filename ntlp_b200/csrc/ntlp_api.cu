@@ -19,6 +19,7 @@
 // does so per job) does not go back to the driver each time.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdint>
@@ -80,6 +81,8 @@ struct ntlp_ctx {
     int n_dep_tiles[kDepVariants] = {};
     long long *tile_sums_d = nullptr;
     int *box_first_tile_d = nullptr;
+    int *any_big_d = nullptr;
+    int *edge_list_d = nullptr;   // mixed deposition: tiles left to the global-memory kernel
     void *small_arena = nullptr;
     SortPlan plan{};
     int dep_variant = 0, nt_variant = 0;
@@ -89,6 +92,7 @@ struct ntlp_ctx {
     double g_dt = 0.0;
     int g_nsteps = 0, g_dep = -1, g_nt = -1;
     bool tex_all = true;   // every box's FP32 fields have a texture (mixed)
+    bool any_dense = false;   // some box deposits through per-cell sums (mixed)
     int64_t g_launches = 0;
     int64_t bytes = 0;
     std::string err;
@@ -216,7 +220,13 @@ void carve_box(Carver &cv, BoxHost &h, DevBox &B, bool mixed) {
     carve_state(cv, B.st[1], n);
     if (mixed) {
         for (int q = 0; q < P32_N; ++q) cv.take(&B.pay32.f[q], n);
+        B.img = nullptr;
+        if (g.periodic) cv.take(&B.img, 6 * (size_t)img_count(g));
+        B.cellsum = nullptr;
+        if ((long long)h.cap >= (long long)kDenseRatio * g.ncells) cv.take(&B.cellsum, (size_t)g.ncells * 48);
     } else {
+        B.img = nullptr;
+        B.cellsum = nullptr;
         for (int a = 0; a < 3; ++a) { cv.take(&B.pay.D[a], n); cv.take(&B.pay.V[a], n); }
         cv.take(&B.pay.T0, n); cv.take(&B.pay.H0, n); cv.take(&B.pay.E1, n); cv.take(&B.pay.E2, n);
         cv.take(&B.pay.mult, n);
@@ -233,6 +243,7 @@ void carve_box(Carver &cv, BoxHost &h, DevBox &B, bool mixed) {
     const size_t nsrc = (size_t)g.nz2 * g.sny * g.snx;   // nnodes, or with the +1 column/row of a subdomain
     for (int q = 0; q < 6; ++q) cv.take(&B.src[q], nsrc);
     cv.take(&B.err, 1);
+    cv.take(&B.big_cells, 1);
     cv.take(&B.defer, n);
     cv.take(&B.ndefer, 1);
     if (!g.periodic) {
@@ -514,9 +525,17 @@ void box_geometry(const ntlp_grid &grid, int64_t cap, DevBox &B) {
     g.periodic = 1;
     g.ioff = 0; g.joff = 0;
     g.snx = grid.nnx; g.sny = grid.nny;
+    g.dnx = g.snx; g.dny = g.sny;
     g.xmin = 0.0; g.xmax = grid.xl; g.ymin = 0.0; g.ymax = grid.yl;
     B.cap = (int)cap;
     B.cur = 0;
+}
+
+// mixed periodic boxes deposit their periodic images (ix = nnx+1, nnx+2;
+// iy = nny+1, nny+2) as nodes of the tiles, folded in by k_fold32
+void deposit_extents(DevGrid &g, bool mixed) {
+    g.dnx = g.snx + (mixed && g.periodic ? 2 : 0);
+    g.dny = g.sny + (mixed && g.periodic ? 2 : 0);
 }
 
 // an x-y column subdomain of the periodic domain (set_bounds,
@@ -530,6 +549,8 @@ void subdomain_geometry(const ntlp_grid &grid, const ntlp_subdomain &sd, DevBox 
     g.joff = sd.j0;
     g.snx = grid.nnx + 1;
     g.sny = grid.nny + 1;
+    g.dnx = g.snx;
+    g.dny = g.sny;
     g.xmin = g.dx * (double)sd.i0;
     g.xmax = g.dx * (double)(sd.i0 + grid.nnx);
     g.ymin = g.dy * (double)sd.j0;
@@ -595,6 +616,7 @@ int create(int nbox, const ntlp_grid *grids, const ntlp_params *params, const in
         const DevGrid &g = B.g;
         box_geometry(*grid, h.cap, B);
         if (sd) subdomain_geometry(*grid, *sd, B);
+        deposit_extents(B.g, mixed);
         Carver cv;
         carve_box(cv, h, B, mixed);
         h.arena_bytes = cv.off;
@@ -614,6 +636,7 @@ int create(int nbox, const ntlp_grid *grids, const ntlp_params *params, const in
                 return bail(fail(c, NTLP_ERR_CUDA, "initialising box %d failed", b));
             B.tex_f4 = f4_texture(B.f4 - kF32Guard, npad);
             if (!B.tex_f4) c->tex_all = false;
+            if (B.cellsum) c->any_dense = true;
         }
         if (cudaMemcpyAsync((void *)B.g.lut_zz, h.lut.data(), h.lut.size() * sizeof(int), cudaMemcpyHostToDevice,
                             c->stream) ||
@@ -640,7 +663,7 @@ int create(int nbox, const ntlp_grid *grids, const ntlp_params *params, const in
         bft.push_back((int)ct.size());
         for (long long s = 0; s < g.ncells + 2; s += kScanTile) ct.push_back(Tile{b, (int)s});
         for (int v = 0; v < kDepVariants; ++v) {
-            long long nt = deposit_tile_count(v, g.snx, g.sny, g.nnz);
+            long long nt = deposit_tile_count(v, g.dnx, g.dny, g.nnz);
             for (long long s = 0; s < nt; ++s) dpt[v].push_back(Tile{b, (int)s});
         }
     }
@@ -652,6 +675,12 @@ int create(int nbox, const ntlp_grid *grids, const ntlp_params *params, const in
             for (int v = 0; v < kDepVariants; ++v) k.take(&c->dep_tiles_d[v], dpt[v].size());
             k.take(&c->tile_sums_d, ct.size());
             k.take(&c->box_first_tile_d, bft.size());
+            k.take(&c->any_big_d, 1);
+            {
+                size_t mx = 0;
+                for (int v = 0; v < kDepVariants; ++v) mx = std::max(mx, dpt[v].size());
+                k.take(&c->edge_list_d, 1 + mx);
+            }
             k.take(&c->dp_d, 1);
             k.take(&c->box_d, (size_t)nbox);
         };
@@ -690,6 +719,7 @@ int create(int nbox, const ntlp_grid *grids, const ntlp_params *params, const in
     c->plan.tile_sums = c->tile_sums_d;
     c->plan.box_first_tile = c->box_first_tile_d;
     c->plan.nbox = nbox;
+    c->plan.any_big = c->any_big_d;
     if (cudaMallocHost((void **)&c->counters_h, sizeof(long long) * kNumCounters * nbox) != cudaSuccess)
         return bail(fail(c, NTLP_ERR_NOMEM, "pinned counter buffer refused"));
     if (push_boxes(c)) return bail(NTLP_ERR_CUDA);
@@ -810,11 +840,12 @@ int droplets_upload(ntlp_ctx *c, int b, const ntlp_droplets *d) {
     Tile *ctd = dtd + dtl.size();
     long long *sums = (long long *)(ctd + ctl.size());
     int *bft = (int *)(sums + ctl.size());
+    int *any_big = bft + 2;
     const int bf[2] = {0, (int)ctl.size()};
     CK(cudaMemcpyAsync(dtd, dtl.data(), dtl.size() * sizeof(Tile), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(ctd, ctl.data(), ctl.size() * sizeof(Tile), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(bft, bf, sizeof bf, cudaMemcpyHostToDevice, c->stream));
-    SortPlan plan{dtd, (int)dtl.size(), ctd, (int)ctl.size(), sums, bft, 1};
+    SortPlan plan{dtd, (int)dtl.size(), ctd, (int)ctl.size(), sums, bft, 1, any_big};
     launch_keys_initial(view, dtd, (int)dtl.size(), c->stream);
     launch_sort(view, plan, c->stream);
     launch_finish(view, 1, c->stream);
@@ -875,6 +906,13 @@ int droplets_download(ntlp_ctx *c, int b, ntlp_droplets *d) {
     return NTLP_OK;
 }
 
+// kernels of one deposition: the tiles, plus the two cell-sum kernels when
+// a mixed box is dense
+int deposit_launches(const ntlp_ctx *c) {
+    if (c->params.precision != NTLP_PREC_MIXED) return 1;
+    return c->any_dense ? 5 : 3;   // tiles, overflow, fold (+ cell sums, dense nodes)
+}
+
 // launch the kernels of one step (no synchronisation; graph-capturable)
 int launch_step(ntlp_ctx *c, int kind, int istage, double dt, int32_t it, bool with_deposit) {
     const int nt = kNtValues[c->nt_variant];
@@ -911,11 +949,12 @@ int launch_step(ntlp_ctx *c, int kind, int istage, double dt, int32_t it, bool w
         e0 = phase_begin(c);
         const int v = c->dep_variant;
         if (c->params.precision == NTLP_PREC_MIXED)
-            launch_deposit_mixed(v, c->box_d, c->dep_tiles_d[v], c->n_dep_tiles[v], c->dp, c->stream);
+            launch_deposit_mixed(v, c->box_d, c->dep_tiles_d[v], c->n_dep_tiles[v], c->dp, c->stream, c->nbox,
+                                 c->any_dense, c->edge_list_d);
         else
             launch_deposit64(v, c->box_d, c->dep_tiles_d[v], c->n_dep_tiles[v], c->dp, c->stream);
         phase_end(c, PH_DEPOSIT, e0);
-        c->launches += 1;
+        c->launches += deposit_launches(c);
     }
     CK(cudaGetLastError());
     return NTLP_OK;
@@ -1087,6 +1126,7 @@ int64_t ntlp_bytes_required(int32_t nbox, const ntlp_grid *grids, const ntlp_par
         h.cap = capacities[b];
         DevBox B{};
         box_geometry(grids[b], h.cap, B);
+        deposit_extents(B.g, mixed);
         Carver cv;
         carve_box(cv, h, B, mixed);
         total += cv.off;
@@ -1095,7 +1135,7 @@ int64_t ntlp_bytes_required(int32_t nbox, const ntlp_grid *grids, const ntlp_par
         size_t tiles = 0;
         for (int v = 0; v < kNtVariants; ++v) tiles += (size_t)(h.cap + kNtValues[v] - 1) / kNtValues[v];
         tiles += 2 * (size_t)((g.ncells + 2 + kScanTile - 1) / kScanTile);
-        for (int v = 0; v < kDepVariants; ++v) tiles += (size_t)deposit_tile_count(v, g.snx, g.sny, g.nnz);
+        for (int v = 0; v < kDepVariants; ++v) tiles += (size_t)deposit_tile_count(v, g.dnx, g.dny, g.nnz);
         total += tiles * sizeof(Tile) + sizeof(DevBox) + 64;
     }
     return (int64_t)(total + 16 * 256 + sizeof(DevParams));
@@ -1233,11 +1273,12 @@ int ntlp_coupling(ntlp_ctx *c, double dt, int32_t layout, double *partsrc, doubl
     cudaEvent_t e0 = phase_begin(c);
     const int v = c->dep_variant;
     if (c->params.precision == NTLP_PREC_MIXED)
-        launch_deposit_mixed(v, c->box_d, c->dep_tiles_d[v], c->n_dep_tiles[v], c->dp, c->stream);
+        launch_deposit_mixed(v, c->box_d, c->dep_tiles_d[v], c->n_dep_tiles[v], c->dp, c->stream, c->nbox,
+                             c->any_dense, c->edge_list_d);
     else
         launch_deposit64(v, c->box_d, c->dep_tiles_d[v], c->n_dep_tiles[v], c->dp, c->stream);
     phase_end(c, PH_DEPOSIT, e0);
-    c->launches += 1;
+    c->launches += deposit_launches(c);
     CK(cudaGetLastError());
     double *host[6] = {partsrc, nullptr, nullptr, partTsrc, partHsrc, partTEsrc};
     if (partsrc) {

@@ -18,8 +18,11 @@
 // MIXED=false: each contribution is formed as the reference writes it,
 // ((P*wtt)/dV)*mult with wtt = wtx*wty*wtz, subtracted term by term.
 // MIXED=true: the FP32 payload (cell-relative fractions, momentum/heat/
-// vapour factors, mult/dV), FP32 weights, FP64 sums, taken cell by cell in a
-// fixed order instead of merged (deterministic, not list order).
+// vapour factors, mult/dV), FP32 weights, FP64 sums, grouped by cell: each
+// of the node's 8 cells sums its droplets in list order from zero (S_o),
+// and the node adds S_0 .. S_7 in order.  Deterministic, not list order;
+// the grouping lets boxes with many droplets per cell form every S_o once
+// per cell (k_cellsums32) instead of once per node visit.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -66,12 +69,27 @@ __device__ __forceinline__ void contribute32(const DevParams &p, const float *v,
     const float wy = j ? v[P32_FY] : 1.0f - v[P32_FY];
     const float wz = k ? v[P32_FZ] : 1.0f - v[P32_FZ];
     const double c = (double)(wx * wy * wz * v[P32_FAC]);
+    // explicit FMAs: every kernel that forms a cell sum rounds alike
     if (p.icouple == 1)
-        for (int a = 0; a < 3; ++a) acc[a] -= (double)v[P32_DV0 + a] * c;
-    if (p.iTcouple == 1) acc[3] -= (double)v[P32_T0] * c;
+        for (int a = 0; a < 3; ++a) acc[a] = fma(-(double)v[P32_DV0 + a], c, acc[a]);
+    if (p.iTcouple == 1) acc[3] = fma(-(double)v[P32_T0], c, acc[3]);
     if (p.iHcouple == 1) {
-        acc[4] -= (double)v[P32_H0] * c;
-        acc[5] += (double)v[P32_E] * c;
+        acc[4] = fma(-(double)v[P32_H0], c, acc[4]);
+        acc[5] = fma((double)v[P32_E], c, acc[5]);
+    }
+}
+
+// one cell's sum for corner o = (i, j, k): its droplets (sorted positions
+// a..e) in list order, from zero
+__device__ __forceinline__ void cell_sum32(const DevBox &B, const DevParams &p, int a, int e, int i, int j, int k,
+                                           double S[6]) {
+    for (int q = 0; q < 6; ++q) S[q] = 0.0;
+    for (int at = a; at < e; ++at) {
+        const int t = B.perm[at];
+        float v[P32_N];
+#pragma unroll
+        for (int q = 0; q < P32_N; ++q) v[q] = B.pay32.f[q][t];
+        contribute32(p, v, i, j, k, S);
     }
 }
 
@@ -142,20 +160,33 @@ __device__ __forceinline__ void image_global32(const DevBox &B, const DevParams 
                                                double acc[6]) {
     const DevGrid &g = B.g;
     for (int q = 0; q < 6; ++q) acc[q] = 0.0;
-#pragma unroll
+#pragma unroll 1
     for (int o = 0; o < 8; ++o) {
         const int i = o >> 2, j = (o >> 1) & 1, k = o & 1;
         const int ci = px - i, cj = py - j, ckk = pz - k;
         if (ci < 1 || ci > g.nnx + 1 || cj < 1 || cj > g.nny + 1 || ckk < 0 || ckk > g.nnz) continue;
         const int key = ckk + (g.nnz + 1) * ((cj - 1) + (g.nny + 1) * (ci - 1));
         const int a = B.cell_start[key], b = B.cell_start[key + 1];
-        for (int at = a; at < b; ++at) {
-            const int t = B.perm[at];
-            float v[P32_N];
+        if (a == b) continue;
+        double S[6];
+        cell_sum32(B, p, a, b, i, j, k, S);
+        for (int q = 0; q < 6; ++q) acc[q] += S[q];
+    }
+}
+
+// one pre-fold node image from the per-cell sums of a dense box
+__device__ __forceinline__ void image_cells32(const DevBox &B, int px, int py, int pz, double acc[6]) {
+    const DevGrid &g = B.g;
+    for (int q = 0; q < 6; ++q) acc[q] = 0.0;
 #pragma unroll
-            for (int q = 0; q < P32_N; ++q) v[q] = B.pay32.f[q][t];
-            contribute32(p, v, i, j, k, acc);
-        }
+    for (int o = 0; o < 8; ++o) {
+        const int i = o >> 2, j = (o >> 1) & 1, k = o & 1;
+        const int ci = px - i, cj = py - j, ckk = pz - k;
+        if (ci < 1 || ci > g.nnx + 1 || cj < 1 || cj > g.nny + 1 || ckk < 0 || ckk > g.nnz) continue;
+        const long long key = ckk + (long long)(g.nnz + 1) * ((cj - 1) + (long long)(g.nny + 1) * (ci - 1));
+        if (B.cell_start[key] == B.cell_start[key + 1]) continue;
+        const double *S = B.cellsum + (key * 8 + o) * 6;
+        for (int q = 0; q < 6; ++q) acc[q] += S[q];
     }
 }
 
@@ -182,25 +213,118 @@ __device__ __forceinline__ void image_global(const DevBox &B, const DevParams &p
     merge_ranges<MIXED, false>(B, p, nullptr, nullptr, nullptr, n, pos, end, ck, off, px, py, pz, acc);
 }
 
-// a whole output node (with its periodic images) from global memory
-template <bool MIXED>
-__device__ __forceinline__ void node_global(const DevBox &B, const DevParams &p, int ix, int iy, int iz,
-                                            double out[6]) {
-    const DevGrid &g = B.g;
+// a whole output node (with its periodic images, folded x first, then y)
+template <class Image>
+__device__ __forceinline__ void node_fold(const DevGrid &g, int ix, int iy, int iz, double out[6],
+                                          const Image &image) {
     double a1[6];
-    image_global<MIXED>(B, p, ix, iy, iz, out);
+    image(ix, iy, iz, out);
     if (g.periodic && ix <= 2) {
-        image_global<MIXED>(B, p, ix + g.nnx, iy, iz, a1);
+        image(ix + g.nnx, iy, iz, a1);
         for (int q = 0; q < 6; ++q) out[q] = out[q] + a1[q];
     }
     if (g.periodic && iy <= 2) {
         double b0[6];
-        image_global<MIXED>(B, p, ix, iy + g.nny, iz, b0);
+        image(ix, iy + g.nny, iz, b0);
         if (g.periodic && ix <= 2) {
-            image_global<MIXED>(B, p, ix + g.nnx, iy + g.nny, iz, a1);
+            image(ix + g.nnx, iy + g.nny, iz, a1);
             for (int q = 0; q < 6; ++q) b0[q] = b0[q] + a1[q];
         }
         for (int q = 0; q < 6; ++q) out[q] = out[q] + b0[q];
+    }
+}
+
+template <bool MIXED>
+__device__ __forceinline__ void node_global(const DevBox &B, const DevParams &p, int ix, int iy, int iz,
+                                            double out[6]) {
+    node_fold(B.g, ix, iy, iz, out,
+              [&](int px, int py, int pz, double acc[6]) { image_global<MIXED>(B, p, px, py, pz, acc); });
+}
+
+// Dense boxes (mixed): every cell's 8 corner sums S_o once, one thread per
+// (cell, corner) -- grid.y = box, grid-stride over cells x 8
+__global__ void k_cellsums32(DevBox *boxes, const __grid_constant__ DevParams P) {
+    const DevBox &B = boxes[blockIdx.y];
+    if (B.cellsum == nullptr) return;
+    const long long total = B.g.ncells * 8;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const long long cell = idx >> 3;
+        const int o = (int)(idx & 7);
+        double S[6];
+        cell_sum32(B, P, B.cell_start[cell], B.cell_start[cell + 1], o >> 2, (o >> 1) & 1, o & 1, S);
+        double *out = B.cellsum + idx * 6;
+        for (int q = 0; q < 6; ++q) out[q] = S[q];
+    }
+}
+
+// Dense boxes (mixed): every output node from the cell sums
+__global__ void k_nodes_dense32(DevBox *boxes) {
+    const DevBox &B = boxes[blockIdx.y];
+    if (B.cellsum == nullptr) return;
+    const DevGrid &g = B.g;
+    const long long total = (long long)g.snx * g.sny * g.nz2;
+    for (long long node = (long long)blockIdx.x * blockDim.x + threadIdx.x; node < total;
+         node += (long long)gridDim.x * blockDim.x) {
+        const int iz = (int)(node % g.nz2);
+        const int iy = 1 + (int)((node / g.nz2) % g.sny);
+        const int ix = 1 + (int)(node / ((long long)g.nz2 * g.sny));
+        double out[6];
+        node_fold(g, ix, iy, iz, out,
+                  [&](int px, int py, int pz, double acc[6]) { image_cells32(B, px, py, pz, acc); });
+        for (int q = 0; q < 6; ++q) B.src[q][node] = out[q];
+    }
+}
+
+// a mixed deposition node: the box's own nodes to the sources, the
+// periodic images (mixed periodic boxes) to B.img
+__device__ __forceinline__ void store_node32(const DevBox &B, int ix, int iy, int iz, const double out[6]) {
+    const DevGrid &g = B.g;
+    if (ix <= g.snx && iy <= g.sny) {
+        const long long node = (long long)iz + (long long)g.nz2 * ((long long)(iy - 1) + (long long)g.sny * (ix - 1));
+        for (int q = 0; q < 6; ++q) B.src[q][node] = out[q];
+    } else {
+        const long long at = img_index(g, ix, iy, iz), per = img_count(g);
+        for (int q = 0; q < 6; ++q) B.img[q * per + at] = out[q];
+    }
+}
+
+// Mixed periodic boxes: the fold of particle_coupling_exchange on the nodes
+// with ix <= 2 or iy <= 2, from their own image (in the sources) and the
+// image nodes, in node_fold's order; grid.y = box
+__global__ void k_fold32(DevBox *boxes) {
+    const DevBox &B = boxes[blockIdx.y];
+    const DevGrid &g = B.g;
+    if (!g.periodic || B.img == nullptr || B.cellsum != nullptr) return;
+    const int ya = g.nny < 2 ? g.nny : 2, xb = g.nnx < 2 ? g.nnx : 2;
+    const long long na = (long long)ya * g.nnx * g.nz2;                       // iy <= 2, every ix
+    const long long nb = g.nny > 2 ? (long long)xb * (g.nny - 2) * g.nz2 : 0;  // ix <= 2, iy >= 3
+    const long long per = img_count(g);
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < na + nb;
+         idx += (long long)gridDim.x * blockDim.x) {
+        int ix, iy, iz;
+        if (idx < na) {
+            iz = (int)(idx % g.nz2);
+            iy = 1 + (int)((idx / g.nz2) % ya);
+            ix = 1 + (int)(idx / ((long long)g.nz2 * ya));
+        } else {
+            const long long r = idx - na;
+            iz = (int)(r % g.nz2);
+            iy = 3 + (int)((r / g.nz2) % (g.nny - 2));
+            ix = 1 + (int)(r / ((long long)g.nz2 * (g.nny - 2)));
+        }
+        const long long node = (long long)iz + (long long)g.nz2 * ((long long)(iy - 1) + (long long)g.sny * (ix - 1));
+        for (int q = 0; q < 6; ++q) {
+            const double *I = B.img + q * per;
+            double out = B.src[q][node];
+            if (ix <= 2) out = out + I[img_index(g, ix + g.nnx, iy, iz)];
+            if (iy <= 2) {
+                double b0 = I[img_index(g, ix, iy + g.nny, iz)];
+                if (ix <= 2) b0 = b0 + I[img_index(g, ix + g.nnx, iy + g.nny, iz)];
+                out = out + b0;
+            }
+            B.src[q][node] = out;
+        }
     }
 }
 
@@ -213,8 +337,9 @@ __host__ __device__ constexpr int dep_smem_bytes(bool mixed, int TX, int TY, int
 // Tiled deposition: tiles enumerate (z fastest) the node tiles of each box;
 // tile shapes 2x4x32, 4x4x16 and 2x2x64 nodes are instantiated (autotuned).
 template <bool MIXED, int kDepTX, int kDepTY, int kDepTZ>
-__global__ void __launch_bounds__(kDepositThreads, MIXED ? 3 : 2)
-k_deposit_tiled(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevParams P) {
+__global__ void __launch_bounds__(kDepositThreads, MIXED ? 4 : 2)
+k_deposit_tiled(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevParams P, int *edge_list,
+                int any_dense) {
     static_assert(kDepTX * kDepTY * kDepTZ == kDepositThreads, "one thread per node of the tile");
     constexpr int kDepCols = (kDepTX + 1) * (kDepTY + 1);
     constexpr int kDepCSW = kDepTZ + 2;
@@ -229,17 +354,20 @@ k_deposit_tiled(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevPar
     __shared__ int s_total;
     const Tile tl = tiles[blockIdx.x];
     const DevBox &B = boxes[tl.box];
+    if (MIXED && any_dense && B.cellsum != nullptr) return;   // dense box: k_cellsums32 + k_nodes_dense32
     const DevParams &p = P;
     const DevGrid &g = B.g;
-    const int ntz = (g.nz2 + kDepTZ - 1) / kDepTZ, nty = (g.sny + kDepTY - 1) / kDepTY;
+    const int ntz = (g.nz2 + kDepTZ - 1) / kDepTZ, nty = (g.dny + kDepTY - 1) / kDepTY;
     const int tzi = tl.start % ntz, tyi = (tl.start / ntz) % nty, txi = tl.start / (ntz * nty);
     const int x0 = 1 + txi * kDepTX, y0 = 1 + tyi * kDepTY, z0 = tzi * kDepTZ;
     const int lz = threadIdx.x % kDepTZ, ly = (threadIdx.x / kDepTZ) % kDepTY, lx = threadIdx.x / (kDepTZ * kDepTY);
     const int ix = x0 + lx, iy = y0 + ly, iz = z0 + lz;
-    const bool valid = ix <= g.snx && iy <= g.sny && iz <= g.nnz + 1;
+    const bool valid = ix <= g.dnx && iy <= g.dny && iz <= g.nnz + 1;
     const long long node = (long long)iz + (long long)g.nz2 * ((long long)(iy - 1) + (long long)g.sny * (ix - 1));
     double out[6];
-    bool staged = (x0 > 2) && (y0 > 2);
+    // FP64: tiles on the periodic edges merge from global memory with their
+    // images; mixed: every tile stages (images are nodes of their own)
+    bool staged = MIXED || ((x0 > 2) && (y0 > 2));
     if (staged) {
         const int ck_lo = max(z0 - 1, 0), ck_hi = min(z0 + kDepTZ - 1, g.nnz);
         // cell starts of the tile's columns (absolute positions in the sorted list)
@@ -247,7 +375,7 @@ k_deposit_tiled(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevPar
             const int cc = e / kDepCSW, lzz = e % kDepCSW;
             const int ci = x0 - 1 + cc / (kDepTY + 1), cj = y0 - 1 + cc % (kDepTY + 1);
             int v = 0;
-            if (ci <= g.nnx + 1 && cj <= g.nny + 1) {
+            if (ci >= 1 && cj >= 1 && ci <= g.nnx + 1 && cj <= g.nny + 1) {
                 const int ck = min(max(z0 - 1 + lzz, ck_lo), ck_hi + 1);
                 v = B.cell_start[ck + (g.nnz + 1) * ((cj - 1) + (g.nny + 1) * (ci - 1))];
             }
@@ -302,12 +430,15 @@ k_deposit_tiled(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevPar
                     const int base = s_off[cc] - s_cs[cc * kDepCSW];
                     const int a = base + s_cs[cc * kDepCSW + lzz];
                     const int b = base + s_cs[cc * kDepCSW + lzz + 1];
+                    if (a == b) continue;
+                    double S[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
                     for (int at = a; at < b; ++at) {
                         float v[P32_N];
 #pragma unroll
                         for (int q = 0; q < P32_N; ++q) v[q] = s_f[q * CAP + at];
-                        contribute32(p, v, i, j, k, out);
+                        contribute32(p, v, i, j, k, S);
                     }
+                    for (int q = 0; q < 6; ++q) out[q] += S[q];
                 }
             } else if (valid) {
                 int pos[8], end[8], ck[8], off[8];
@@ -330,9 +461,42 @@ k_deposit_tiled(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevPar
             }
         }
     }
+    if (MIXED) {
+        if (!staged) {
+            // above the stage capacity: k_deposit_overflow32, which has the
+            // registers of the global path
+            if (threadIdx.x == 0) edge_list[1 + atomicAdd(edge_list, 1)] = blockIdx.x;
+            return;
+        }
+        if (valid) store_node32(B, ix, iy, iz, out);
+        return;
+    }
     if (!staged && valid) node_global<MIXED>(B, p, ix, iy, iz, out);
     if (valid)
         for (int q = 0; q < 6; ++q) B.src[q][node] = out[q];
+}
+
+// Mixed tiles listed by k_deposit_tiled (edge_list[0] of them in
+// edge_list[1..], above the stage capacity): each node's own image from
+// global memory, stored like the tiled kernel's; grid-stride over the list
+template <int kDepTX, int kDepTY, int kDepTZ>
+__global__ void __launch_bounds__(kDepositThreads)
+k_deposit_overflow32(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevParams P, const int *edge_list) {
+    const int n = edge_list[0];
+    for (int e = blockIdx.x; e < n; e += gridDim.x) {
+        const Tile tl = tiles[edge_list[1 + e]];
+        const DevBox &B = boxes[tl.box];
+        const DevGrid &g = B.g;
+        const int ntz = (g.nz2 + kDepTZ - 1) / kDepTZ, nty = (g.dny + kDepTY - 1) / kDepTY;
+        const int tzi = tl.start % ntz, tyi = (tl.start / ntz) % nty, txi = tl.start / (ntz * nty);
+        const int lz = threadIdx.x % kDepTZ, ly = (threadIdx.x / kDepTZ) % kDepTY,
+                  lx = threadIdx.x / (kDepTZ * kDepTY);
+        const int ix = 1 + txi * kDepTX + lx, iy = 1 + tyi * kDepTY + ly, iz = tzi * kDepTZ + lz;
+        if (ix > g.dnx || iy > g.dny || iz > g.nnz + 1) continue;
+        double out[6];
+        image_global32(B, P, ix, iy, iz, out);
+        store_node32(B, ix, iy, iz, out);
+    }
 }
 
 }  // namespace

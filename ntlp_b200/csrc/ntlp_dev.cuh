@@ -59,6 +59,10 @@ struct DevGrid {
     int periodic;
     int ioff, joff;
     int snx, sny;
+    // node extents of the deposition tiles: snx, sny, and for mixed
+    // periodic boxes 2 more (the periodic images, deposited as nodes and
+    // folded in afterwards)
+    int dnx, dny;
     double xmin, xmax, ymin, ymax;   // set_bounds (particles.f90:1766-1781)
 };
 
@@ -127,6 +131,10 @@ struct DevBox {
     long long *flux_fx;    // [2][nnz+1][kFluxLimbs]
     double *src[6];        // [nnodes] each, column layout
     int *err;              // device error word (0 = fine)
+    int *big_cells;        // this sort has cells of more than kSmallCell droplets
+    double *img;           // mixed periodic boxes: [6][img_count] image nodes (ix > nnx or iy > nny)
+    double *cellsum;       // mixed boxes with many droplets per cell: [ncells][8 corners][6]
+                           // per-cell source sums (nullptr: tiled deposition)
     int *defer;            // [cap] droplets whose Gauss-Newton solve failed this step
     int *ndefer;           // their count
     long long *hist;       // [NTLP_H_STEP_KINDS][NTLP_HIST_N] step histograms (weights are integers)
@@ -213,6 +221,16 @@ __device__ __forceinline__ long long ext_index(const DevGrid &g, int k, int j, i
 }
 
 __device__ __forceinline__ double cube(double r) { return (r * r) * r; }
+
+// image nodes of a mixed periodic box (its deposition nodes with ix > nnx,
+// iy in 1..nny+2, then those with iy > nny, ix in 1..nnx), per quantity
+__host__ __device__ __forceinline__ long long img_count(const DevGrid &g) {
+    return (long long)(2 * (g.nny + 2) + 2 * g.nnx) * g.nz2;
+}
+__host__ __device__ __forceinline__ long long img_index(const DevGrid &g, int ix, int iy, int iz) {
+    if (ix > g.nnx) return ((long long)(ix - g.nnx - 1) * (g.nny + 2) + (iy - 1)) * g.nz2 + iz;
+    return 2LL * (g.nny + 2) * g.nz2 + ((long long)(iy - g.nny - 1) * g.nnx + (ix - 1)) * g.nz2 + iz;
+}
 
 // The FP32 field copies hold deviations from the value at the interior
 // point (k, j, i) = (1, 1, 1): T ~ 293 K would otherwise keep only ~3e-5 K

@@ -434,7 +434,7 @@ template <int V>
 static void dep64(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams &P, cudaStream_t st) {
     constexpr int TX = kDepShape[V][0], TY = kDepShape[V][1], TZ = kDepShape[V][2];
     k_deposit_tiled<false, TX, TY, TZ>
-        <<<ntiles, kDepositThreads, dep_smem_bytes(false, TX, TY, TZ), st>>>(boxes, tiles, P);
+        <<<ntiles, kDepositThreads, dep_smem_bytes(false, TX, TY, TZ), st>>>(boxes, tiles, P, nullptr, 0);
 }
 
 template <int V>

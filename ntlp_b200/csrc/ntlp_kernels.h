@@ -50,8 +50,14 @@ void launch_update_be_mixed(int ilin, int nt, DevBox *boxes, const Tile *tiles, 
                             bool tex);
 void launch_payload_mixed(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams &P, double dt,
                           cudaStream_t st);
+// dense: some box has per-cell sums (cellsum), deposited by the cell-sum
+// kernels instead of the tiles
+// edge_list: [1 + tiles] ints of scratch (count, then tile indices)
 void launch_deposit_mixed(int variant, DevBox *boxes, const Tile *tiles, int ntiles, const DevParams &P,
-                          cudaStream_t st);
+                          cudaStream_t st, int nbox, bool dense, int *edge_list);
+constexpr int kDenseRatio = 16;     // mixed boxes with capacity >= 16 x cells use per-cell sums
+constexpr int kDenseBlocks = 1184;  // grid.x of the cell-sum kernels
+constexpr int kFoldBlocks = 148;    // grid.x of the periodic fold (mixed)
 // one-time kernel attributes (dynamic shared memory of the deposition);
 // call outside stream capture
 void prepare_kernels64();
@@ -66,8 +72,11 @@ struct SortPlan {
     long long *tile_sums;    // [n_cell_tiles]
     const int *box_first_tile;  // [nbox+1] first cell tile of each box
     int nbox;
+    int *any_big;            // some box has cells above kSmallCell (set by k_cellsort)
 };
-constexpr int kSortLaunches = 6;   // kernels launched by launch_sort
+constexpr int kSortLaunches = 8;   // kernels launched by launch_sort
+constexpr int kSmallCell = 32;     // cells up to this size are insertion-sorted by one thread
+constexpr int kRankBlocks = 1184;  // grid of the large-cell ranking (8 blocks per SM)
 void launch_sort(DevBox *boxes, const SortPlan &plan, cudaStream_t st);
 void launch_finish(DevBox *boxes, int nbox, cudaStream_t st);
 void launch_reset_step(DevBox *boxes, int nbox, cudaStream_t st);

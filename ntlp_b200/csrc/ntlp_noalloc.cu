@@ -159,6 +159,7 @@ extern "C" int ntlp_coupling_noalloc(const ntlp_grid *grid, const ntlp_params *p
     g.ncells = ncells; g.nnodes = nnodes;
     g.periodic = 1;
     g.snx = grid->nnx; g.sny = grid->nny;
+    g.dnx = g.snx; g.dny = g.sny;
     g.xmax = grid->xl; g.ymax = grid->yl;
     g.z = zg; g.zz = zg + (kMaxNz + 3); g.dzw = zg + 2 * (kMaxNz + 3); g.dzu = zg + 3 * (kMaxNz + 3);
     int *ints = (int *)(S + kOffInts);
@@ -185,6 +186,7 @@ extern "C" int ntlp_coupling_noalloc(const ntlp_grid *grid, const ntlp_params *p
     B.cap = (int)n;
     B.n_alive = (int *)(S + kOffSmall);
     B.err = (int *)(S + kOffSmall) + 1;
+    B.big_cells = (int *)(S + kOffSmall) + 2;
     B.counters = (long long *)(S + kOffSmall + 64);
     B.pflux = (double *)(S + kOffFlux);
     B.flux_fx = (long long *)(S + kOffFlux + (kMaxNz + 1) * 8);
@@ -234,6 +236,7 @@ extern "C" int ntlp_coupling_noalloc(const ntlp_grid *grid, const ntlp_params *p
     plan.tile_sums = sums;
     plan.box_first_tile = box_first;
     plan.nbox = 1;
+    plan.any_big = (int *)(S + kOffSmall) + 3;
     launch_keys_initial(B_d, drop_tiles, nd, st);
     launch_sort(B_d, plan, st);
     launch_finish(B_d, 1, st);

@@ -48,8 +48,12 @@ __global__ void k_scan_sums(DevBox *boxes, const Tile *tiles, long long *sums) {
 }
 
 // one block per box: exclusive scan of the box's tile sums, in place
-__global__ void k_scan_offsets(DevBox *boxes, const int *box_first_tile, long long *sums) {
+__global__ void k_scan_offsets(DevBox *boxes, const int *box_first_tile, long long *sums, int *any_big) {
     const int b = blockIdx.x;
+    if (threadIdx.x == 0) {
+        *boxes[b].big_cells = 0;    // set again by k_cellsort
+        if (b == 0) *any_big = 0;
+    }
     const int a = box_first_tile[b], e = box_first_tile[b + 1];
     __shared__ long long carry;
     if (threadIdx.x == 0) carry = 0;
@@ -140,7 +144,7 @@ __global__ void k_scatter(DevBox *boxes, const Tile *tiles) {
 }
 
 // ---- per-cell list order (ascending lid), clears the cursor ---------------
-__global__ void k_cellsort(DevBox *boxes, const Tile *tiles) {
+__global__ void k_cellsort(DevBox *boxes, const Tile *tiles, int *any_big) {
     const Tile tl = tiles[blockIdx.x];
     const DevBox &B = boxes[tl.box];
     const long long nb = nbuckets(B);
@@ -152,7 +156,12 @@ __global__ void k_cellsort(DevBox *boxes, const Tile *tiles) {
         if (c == nb - 1) continue;       // killed droplets: order irrelevant
         const int a = B.cell_start[c], e = B.cell_start[c + 1];
         if (e - a < 2) continue;
-        // insertion sort by lid (cells hold few droplets)
+        if (e - a > kSmallCell) {       // ranked by k_cellrank / k_cellcopy
+            *B.big_cells = 1;
+            *any_big = 1;
+            continue;
+        }
+        // insertion sort by lid (few droplets)
         for (int p = a + 1; p < e; ++p) {
             const int tv = B.sorted[p];
             const int lv = lid[tv];
@@ -166,13 +175,68 @@ __global__ void k_cellsort(DevBox *boxes, const Tile *tiles) {
     }
 }
 
+// Cells with more than kSmallCell droplets (dense configurations: hundreds
+// per cell): one thread per sorted position counts the cell's droplets
+// with a smaller lid (ties, which unique lids never make, by position) and
+// writes its droplet to that rank in the previous permutation, which is
+// dead between the update and the finish; k_cellcopy then moves the ranked
+// ranges back.  O(n) per droplet instead of the O(n^2) insertion sort of
+// one thread per cell.
+// grid-stride over the droplet tiles: a fixed grid, so that a sort without
+// large cells costs two short launches
+__global__ void k_cellrank(DevBox *boxes, const Tile *tiles, int ntiles, const int *any_big) {
+    if (*any_big == 0) return;
+    for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
+        const Tile tl = tiles[ti];
+        const DevBox &B = boxes[tl.box];
+        if (*B.big_cells == 0) continue;
+        const int p = tl.start + threadIdx.x;
+        if (p >= *B.n_alive) continue;
+        const long long nb = nbuckets(B);
+        const int tv = B.sorted[p];
+        const int c = B.key[tv];
+        if (c == nb - 1) continue;
+        const int a = B.cell_start[c], e = B.cell_start[c + 1];
+        if (e - a <= kSmallCell) continue;
+        const int *lid = B.st[1 - B.cur].lid;
+        const int lv = lid[tv];
+        int r = 0;
+        for (int q = a; q < e; ++q) {
+            const int lq = lid[B.sorted[q]];
+            r += (lq < lv) || (lq == lv && q < p);
+        }
+        B.perm[a + r] = tv;
+    }
+}
+
+__global__ void k_cellcopy(DevBox *boxes, const Tile *tiles, int ntiles, const int *any_big) {
+    if (*any_big == 0) return;
+    for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
+        const Tile tl = tiles[ti];
+        const DevBox &B = boxes[tl.box];
+        if (*B.big_cells == 0) continue;
+        const int p = tl.start + threadIdx.x;
+        if (p >= *B.n_alive) continue;
+        const long long nb = nbuckets(B);
+        const int c = B.key[B.sorted[p]];
+        if (c == nb - 1) continue;
+        if (B.cell_start[c + 1] - B.cell_start[c] <= kSmallCell) continue;
+        B.sorted[p] = B.perm[p];
+    }
+}
+
 void launch_sort(DevBox *boxes, const SortPlan &plan, cudaStream_t st) {
     k_hist<<<plan.n_drop_tiles, kUpdateThreads, 0, st>>>(boxes, plan.drop_tiles);
     k_scan_sums<<<plan.n_cell_tiles, 256, 0, st>>>(boxes, plan.cell_tiles, plan.tile_sums);
-    k_scan_offsets<<<plan.nbox, 1024, 0, st>>>(boxes, plan.box_first_tile, plan.tile_sums);
+    k_scan_offsets<<<plan.nbox, 1024, 0, st>>>(boxes, plan.box_first_tile, plan.tile_sums, plan.any_big);
     k_scan_local<<<plan.n_cell_tiles, kCellThreads, 0, st>>>(boxes, plan.cell_tiles, plan.tile_sums);
     k_scatter<<<plan.n_drop_tiles, kUpdateThreads, 0, st>>>(boxes, plan.drop_tiles);
-    k_cellsort<<<plan.n_cell_tiles, 256, 0, st>>>(boxes, plan.cell_tiles);
+    k_cellsort<<<plan.n_cell_tiles, 256, 0, st>>>(boxes, plan.cell_tiles, plan.any_big);
+    const int g = plan.n_drop_tiles < kRankBlocks ? plan.n_drop_tiles : kRankBlocks;
+    if (g > 0) {
+        k_cellrank<<<g, kUpdateThreads, 0, st>>>(boxes, plan.drop_tiles, plan.n_drop_tiles, plan.any_big);
+        k_cellcopy<<<g, kUpdateThreads, 0, st>>>(boxes, plan.drop_tiles, plan.n_drop_tiles, plan.any_big);
+    }
 }
 
 // ---- finish: flip buffers, adopt the sorted order, count survivors ---------

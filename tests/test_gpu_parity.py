@@ -82,6 +82,59 @@ def test_be_fp64_bitexact(ilin, icase):
     s.close()
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_dense_cells(precision):
+    # ~100 droplets per cell: cells above the insertion-sort size are put in
+    # lid order by ranking, and every tile overflows the deposition stage
+    params = gen.default_params(ilin=0)
+    case = small_case(params=params, n=20000, grid_n=(4, 4, 6))
+    p = dict(params, precision=abi.NTLP_PREC_MIXED if precision == "mixed" else abi.NTLP_PREC_FP64)
+    s = _gpu(case, p)
+    o = _oracle(case)
+    od = clone(case.droplets)
+    for it in (1, 2):
+        gc = s.particle_update_BE(case.dt, it)
+        oc, _ = o.step_be(od, case.dt, it)
+        assert gc["numpart"] == oc["numpart"]
+    gd = s.get_droplets()
+    assert np.array_equal(gd["lid"], od["lid"])
+    gsrc = s.particle_coupling_update(case.dt)
+    osrc, oabs = o.coupling(od, case.dt, with_abs=True)
+    if precision == "fp64":
+        _assert_state_bitexact(gd, od)
+        _assert_sources_bitexact(gsrc, osrc)
+    else:
+        assert max_rel(gd["radius"], od["radius"], 1e-300) <= MIXED_TOL["radius"]
+        for q in range(6):
+            scale = np.abs(oabs[q]).max()
+            assert np.max(np.abs(np.asarray(gsrc[q]) - osrc[q])) <= 1e-3 * scale, q
+    s.close()
+
+
+def test_mixed_cell_sums_match_tiles():
+    # the same droplets deposited by the per-cell-sum kernels (capacity at
+    # least 16 x cells) and by the tiles (smaller capacity): bit-identical
+    params = dict(gen.default_params(ilin=0), precision=abi.NTLP_PREC_MIXED)
+    case = small_case(params=params, n=2000, grid_n=(4, 4, 6))
+    ncells = 5 * 5 * 7
+    out = []
+    for cap in (2000, 16 * ncells):
+        import ntlp_b200
+        s = ntlp_b200.DropletStep(case.grid, params, capacity=cap)
+        s.set_fields_ext(case.ext())
+        s.set_droplets(case.droplets)
+        for it in (1, 2):
+            s.particle_update_BE(case.dt, it)
+        src = [np.asarray(x).copy() for x in s.particle_coupling_update(case.dt)]
+        out.append((s.get_droplets(), src))
+        s.close()
+    (d0, s0), (d1, s1) = out
+    for k in STATE_KEYS:
+        assert bitwise_equal(d0[k], d1[k]), k
+    for q in range(6):
+        assert bitwise_equal(s0[q], s1[q]), q
+
+
 @pytest.mark.parametrize("ilin", [1, 0])
 def test_rk3_fp64_bitexact(ilin):
     # explicit RK3 needs dt below the droplet response time: 20-60 um
