@@ -394,14 +394,36 @@ k_deposit_tiled(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevPar
         staged = s_total <= CAP;
         if (staged) {
             const DevState &O = B.st[B.cur];
-            for (int k = threadIdx.x; k < s_total; k += blockDim.x) {
+            if (MIXED) {
+                // two droplets per pass: their perm and payload loads are in
+                // flight together
+                for (int k0 = threadIdx.x; k0 < s_total; k0 += 2 * blockDim.x) {
+                    const int k1 = k0 + blockDim.x;
+                    int c0 = 0, c1 = 0;
+                    while (c0 + 1 < kDepCols && s_off[c0 + 1] <= k0) ++c0;
+                    while (c1 + 1 < kDepCols && s_off[c1 + 1] <= k1) ++c1;
+                    const bool two = k1 < s_total;
+                    const int t0 = B.perm[s_cs[c0 * kDepCSW] + (k0 - s_off[c0])];
+                    const int t1 = two ? B.perm[s_cs[c1 * kDepCSW] + (k1 - s_off[c1])] : t0;
+                    float v0[P32_N], v1[P32_N];
+#pragma unroll
+                    for (int q = 0; q < P32_N; ++q) {
+                        v0[q] = B.pay32.f[q][t0];
+                        v1[q] = B.pay32.f[q][t1];
+                    }
+#pragma unroll
+                    for (int q = 0; q < P32_N; ++q) s_f[q * CAP + k0] = v0[q];
+                    if (two)
+#pragma unroll
+                        for (int q = 0; q < P32_N; ++q) s_f[q * CAP + k1] = v1[q];
+                }
+            }
+            for (int k = threadIdx.x; !MIXED && k < s_total; k += blockDim.x) {
                 int cc = 0;
                 while (cc + 1 < kDepCols && s_off[cc + 1] <= k) ++cc;
                 const int t = B.perm[s_cs[cc * kDepCSW] + (k - s_off[cc])];
-                if (!MIXED) s_lid[k] = O.lid[t];
-                if (MIXED) {
-                    for (int q = 0; q < P32_N; ++q) s_f[q * CAP + k] = B.pay32.f[q][t];
-                } else {
+                s_lid[k] = O.lid[t];
+                {
                     const DevPayload &P = B.pay;
                     s_v[k] = O.x[0][t];
                     s_v[CAP + k] = O.x[1][t];
