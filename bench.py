@@ -59,7 +59,7 @@ B_D = {"fp64": 248, "mixed": 224}       # algorithmic bytes per droplet
 # DRAM bytes per droplet of the update phase (interpolation + droplet body)
 # measured by ncu at 1M droplets / 128^3 (fields subtracted), used to scale
 # the measured traffic to the bench workload; see
-# profiles/k_update_mixed_1M_droplets_128cube.md
+# profiles/k_interp_be_deposit_mixed_1M_droplets_128cube.md
 NCU_BYTES_PER_DROPLET = {"mixed": 400.0}
 METRIC = "droplet-updates/s (mixed vs FP64 GPU) at 16M; p50/p99 serving step latency"
 
