@@ -393,7 +393,6 @@ k_deposit_tiled(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevPar
         __syncthreads();
         staged = s_total <= CAP;
         if (staged) {
-            const DevState &O = B.st[B.cur];
             if (MIXED) {
                 // two droplets per pass: their perm and payload loads are in
                 // flight together
@@ -418,25 +417,35 @@ k_deposit_tiled(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevPar
                         for (int q = 0; q < P32_N; ++q) s_f[q * CAP + k1] = v1[q];
                 }
             }
-            for (int k = threadIdx.x; !MIXED && k < s_total; k += blockDim.x) {
-                int cc = 0;
-                while (cc + 1 < kDepCols && s_off[cc + 1] <= k) ++cc;
-                const int t = B.perm[s_cs[cc * kDepCSW] + (k - s_off[cc])];
-                s_lid[k] = O.lid[t];
-                {
-                    const DevPayload &P = B.pay;
-                    s_v[k] = O.x[0][t];
-                    s_v[CAP + k] = O.x[1][t];
-                    s_v[2 * CAP + k] = O.x[2][t];
-                    for (int q = 0; q < 3; ++q) {
-                        s_v[(3 + q) * CAP + k] = P.D[q][t];
-                        s_v[(6 + q) * CAP + k] = P.V[q][t];
+            if (!MIXED) {
+                // two droplets per pass, as for the mixed stage
+                const DevState &O = B.st[B.cur];
+                const DevPayload &P = B.pay;
+                for (int k0 = threadIdx.x; k0 < s_total; k0 += 2 * blockDim.x) {
+                    const int k1 = k0 + blockDim.x;
+                    const bool two = k1 < s_total;
+                    int c0 = 0, c1 = 0;
+                    while (c0 + 1 < kDepCols && s_off[c0 + 1] <= k0) ++c0;
+                    while (c1 + 1 < kDepCols && s_off[c1 + 1] <= k1) ++c1;
+                    const int t0 = B.perm[s_cs[c0 * kDepCSW] + (k0 - s_off[c0])];
+                    const int t1 = two ? B.perm[s_cs[c1 * kDepCSW] + (k1 - s_off[c1])] : t0;
+                    const double *src[14] = {O.x[0], O.x[1], O.x[2], P.D[0], P.D[1], P.D[2], P.V[0],
+                                             P.V[1], P.V[2], P.T0, P.H0, P.E1, P.E2, P.mult};
+                    double w0[14], w1[14];
+#pragma unroll
+                    for (int q = 0; q < 14; ++q) {
+                        w0[q] = src[q][t0];
+                        w1[q] = src[q][t1];
                     }
-                    s_v[9 * CAP + k] = P.T0[t];
-                    s_v[10 * CAP + k] = P.H0[t];
-                    s_v[11 * CAP + k] = P.E1[t];
-                    s_v[12 * CAP + k] = P.E2[t];
-                    s_v[13 * CAP + k] = P.mult[t];
+                    const int l0 = O.lid[t0], l1 = O.lid[t1];
+                    s_lid[k0] = l0;
+#pragma unroll
+                    for (int q = 0; q < 14; ++q) s_v[q * CAP + k0] = w0[q];
+                    if (two) {
+                        s_lid[k1] = l1;
+#pragma unroll
+                        for (int q = 0; q < 14; ++q) s_v[q * CAP + k1] = w1[q];
+                    }
                 }
             }
             __syncthreads();
