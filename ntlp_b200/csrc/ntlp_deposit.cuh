@@ -93,14 +93,14 @@ __device__ __forceinline__ void cell_sum32(const DevBox &B, const DevParams &p, 
     }
 }
 
-// Merge of up to 8 lid-sorted ranges.  Source: global memory through the
-// sorted list (STAGED false; positions index B.perm) or the shared-memory
-// stage (STAGED true; positions index the stage).
-template <bool MIXED, bool STAGED>
+// FP64: merge of up to 8 lid-sorted ranges.  Source: global memory through
+// the sorted list (STAGED false; positions index B.perm) or the
+// shared-memory stage (STAGED true; positions index the stage).
+template <bool STAGED>
 __device__ __forceinline__ void merge_ranges(const DevBox &B, const DevParams &p, const int *s_lid,
-                                             const double *s_v, const float *s_f, int n, int pos[8],
-                                             const int end[8], const int ck[8], const int off[8], int px,
-                                             int py, int pz, double acc[6]) {
+                                             const double *s_v, int n, int pos[8], const int end[8],
+                                             const int ck[8], const int off[8], int px, int py, int pz,
+                                             double acc[6]) {
     const DevGrid &g = B.g;
     for (int q = 0; q < 6; ++q) acc[q] = 0.0;
     if (n == 0) return;
@@ -117,19 +117,9 @@ __device__ __forceinline__ void merge_ranges(const DevBox &B, const DevParams &p
         if (best < 0) break;
         const int at = pos[best];
         const int kpt = ck[best];
-        const int o = off[best];
         pos[best]++;
         if (pos[best] < end[best]) head[best] = STAGED ? s_lid[pos[best]] : O.lid[B.perm[pos[best]]];
-        if (MIXED) {
-            float v[P32_N];
-            if (STAGED) {
-                for (int q = 0; q < P32_N; ++q) v[q] = s_f[q * kDepCapMixed + at];
-            } else {
-                const int t = B.perm[at];
-                for (int q = 0; q < P32_N; ++q) v[q] = B.pay32.f[q][t];
-            }
-            contribute32(p, v, o >> 2, (o >> 1) & 1, o & 1, acc);
-        } else {
+        {
             DropVals d;
             if (STAGED) {
                 d.x1 = s_v[at]; d.x2 = s_v[kDepCap64 + at]; d.x3 = s_v[2 * kDepCap64 + at];
@@ -194,7 +184,7 @@ __device__ __forceinline__ void image_cells32(const DevBox &B, int px, int py, i
 template <bool MIXED>
 __device__ __forceinline__ void image_global(const DevBox &B, const DevParams &p, int px, int py, int pz,
                                              double acc[6]) {
-    if (MIXED) {
+    if constexpr (MIXED) {
         image_global32(B, p, px, py, pz, acc);
         return;
     }
@@ -210,7 +200,7 @@ __device__ __forceinline__ void image_global(const DevBox &B, const DevParams &p
                 const int a = B.cell_start[key], b = B.cell_start[key + 1];
                 if (a < b) { pos[n] = a; end[n] = b; ck[n] = ckk; off[n] = (i << 2) | (j << 1) | k; n++; }
             }
-    merge_ranges<MIXED, false>(B, p, nullptr, nullptr, nullptr, n, pos, end, ck, off, px, py, pz, acc);
+    merge_ranges<false>(B, p, nullptr, nullptr, n, pos, end, ck, off, px, py, pz, acc);
 }
 
 // a whole output node (with its periodic images, folded x first, then y)
@@ -449,7 +439,8 @@ k_deposit_tiled(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevPar
                 }
             }
             __syncthreads();
-            if (valid && MIXED) {
+            if constexpr (MIXED) {
+              if (valid) {
                 for (int q = 0; q < 6; ++q) out[q] = 0.0;
 #pragma unroll
                 for (int o = 0; o < 8; ++o) {
@@ -471,6 +462,7 @@ k_deposit_tiled(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevPar
                     }
                     for (int q = 0; q < 6; ++q) out[q] += S[q];
                 }
+              }
             } else if (valid) {
                 int pos[8], end[8], ck[8], off[8];
                 int n = 0;
@@ -488,7 +480,7 @@ k_deposit_tiled(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevPar
                                 pos[n] = a; end[n] = b; ck[n] = ckk; off[n] = (i << 2) | (j << 1) | k; n++;
                             }
                         }
-                merge_ranges<MIXED, true>(B, p, s_lid, s_v, s_f, n, pos, end, ck, off, ix, iy, iz, out);
+                merge_ranges<true>(B, p, s_lid, s_v, n, pos, end, ck, off, ix, iy, iz, out);
             }
         }
     }

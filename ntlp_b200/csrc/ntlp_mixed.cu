@@ -222,9 +222,10 @@ k_interp_mixed(DevBox *boxes, const Tile *tiles) {
     B.key[t] = bad;
 }
 
-// 6 resident blocks of 128: 80 registers, 24 warps per SM (a few spills, to
-// L1); faster than 5 blocks at 94 registers without spills
-__global__ void __launch_bounds__(128, 6)
+// 7 resident blocks of 128: 72 registers, 28 warps per SM (spills, to L1).
+// Measured at 16.8 M droplets: faster than 5 blocks (94 registers, no
+// spills) and 6 (80); 8 blocks (64 registers) is no faster.
+__global__ void __launch_bounds__(128, 7)
 k_be_mixed(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevParams P, StepIn in) {
     const Tile tl = tiles[blockIdx.x];
     const DevBox &B = boxes[tl.box];

@@ -167,6 +167,36 @@ def test_autotune_changes_no_result(precision):
         _same_sources(a.box_sources(k), b.box_sources(k))
 
 
+@pytest.mark.parametrize("precision", [abi.NTLP_PREC_FP64, abi.NTLP_PREC_MIXED])
+def test_dense_box_in_a_batch(precision):
+    # a box of ~100 droplets per cell (large-cell ranking; mixed: per-cell
+    # sums) beside sparse boxes: every box equals itself alone, eager and graph
+    import ntlp_b200
+    params = gen.default_params(ilin=0, precision=precision)
+    dense = small_case(n=20000, grid_n=(4, 4, 6), params=params, seed=21)
+    cases = [_cases(params)[0], dense, _cases(params)[3]]
+    a = _batch(cases, params)
+    dt = cases[0].dt
+    a.particle_update_BE(dt, 1)
+    a.particle_coupling_update(dt, download=False)
+    a.advance_graph(dt, 2, 2)
+    a.particle_update_BE(dt, 4)
+    a.particle_coupling_update(dt, download=False)
+    a.sync()
+    for k, c in enumerate(cases):
+        s = ntlp_b200.DropletBatch([c.grid], params, [max(8, c.droplets["radius"].shape[0])])
+        s.set_box_fields_ext(0, c.ext(), sync=False)
+        s.set_box_droplets(0, c.droplets)
+        for it in range(1, 5):
+            s.particle_update_BE(dt, it)
+            s.particle_coupling_update(dt, download=False)
+        s.sync()
+        assert a.box_counters(k) == s.box_counters(0)
+        _same_state(a.get_box_droplets(k), s.get_box_droplets(0))
+        _same_sources(a.box_sources(k), s.box_sources(0))
+        s.close()
+
+
 def test_batch_argument_errors():
     import ntlp_b200
     params = gen.default_params()
