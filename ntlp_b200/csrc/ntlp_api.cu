@@ -82,7 +82,7 @@ struct ntlp_ctx {
     long long *tile_sums_d = nullptr;
     int *box_first_tile_d = nullptr;
     int *any_big_d = nullptr;
-    int *edge_list_d = nullptr;   // mixed deposition: tiles left to the global-memory kernel
+    int *overflow_list_d = nullptr;   // mixed deposition: tiles left to the global-memory kernel
     void *small_arena = nullptr;
     SortPlan plan{};
     int dep_variant = 0, nt_variant = 0;
@@ -679,7 +679,7 @@ int create(int nbox, const ntlp_grid *grids, const ntlp_params *params, const in
             {
                 size_t mx = 0;
                 for (int v = 0; v < kDepVariants; ++v) mx = std::max(mx, dpt[v].size());
-                k.take(&c->edge_list_d, 1 + mx);
+                k.take(&c->overflow_list_d, 1 + mx);
             }
             k.take(&c->dp_d, 1);
             k.take(&c->box_d, (size_t)nbox);
@@ -950,7 +950,7 @@ int launch_step(ntlp_ctx *c, int kind, int istage, double dt, int32_t it, bool w
         const int v = c->dep_variant;
         if (c->params.precision == NTLP_PREC_MIXED)
             launch_deposit_mixed(v, c->box_d, c->dep_tiles_d[v], c->n_dep_tiles[v], c->dp, c->stream, c->nbox,
-                                 c->any_dense, c->edge_list_d);
+                                 c->any_dense, c->overflow_list_d);
         else
             launch_deposit64(v, c->box_d, c->dep_tiles_d[v], c->n_dep_tiles[v], c->dp, c->stream);
         phase_end(c, PH_DEPOSIT, e0);
@@ -1274,7 +1274,7 @@ int ntlp_coupling(ntlp_ctx *c, double dt, int32_t layout, double *partsrc, doubl
     const int v = c->dep_variant;
     if (c->params.precision == NTLP_PREC_MIXED)
         launch_deposit_mixed(v, c->box_d, c->dep_tiles_d[v], c->n_dep_tiles[v], c->dp, c->stream, c->nbox,
-                             c->any_dense, c->edge_list_d);
+                             c->any_dense, c->overflow_list_d);
     else
         launch_deposit64(v, c->box_d, c->dep_tiles_d[v], c->n_dep_tiles[v], c->dp, c->stream);
     phase_end(c, PH_DEPOSIT, e0);

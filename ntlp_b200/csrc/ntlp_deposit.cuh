@@ -328,7 +328,7 @@ __host__ __device__ constexpr int dep_smem_bytes(bool mixed, int TX, int TY, int
 // tile shapes 2x4x32, 4x4x16 and 2x2x64 nodes are instantiated (autotuned).
 template <bool MIXED, int kDepTX, int kDepTY, int kDepTZ>
 __global__ void __launch_bounds__(kDepositThreads, MIXED ? 4 : 2)
-k_deposit_tiled(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevParams P, int *edge_list,
+k_deposit_tiled(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevParams P, int *overflow_list,
                 int any_dense) {
     static_assert(kDepTX * kDepTY * kDepTZ == kDepositThreads, "one thread per node of the tile");
     constexpr int kDepCols = (kDepTX + 1) * (kDepTY + 1);
@@ -488,7 +488,7 @@ k_deposit_tiled(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevPar
         if (!staged) {
             // above the stage capacity: k_deposit_overflow32, which has the
             // registers of the global path
-            if (threadIdx.x == 0) edge_list[1 + atomicAdd(edge_list, 1)] = blockIdx.x;
+            if (threadIdx.x == 0) overflow_list[1 + atomicAdd(overflow_list, 1)] = blockIdx.x;
             return;
         }
         if (valid) store_node32(B, ix, iy, iz, out);
@@ -499,15 +499,15 @@ k_deposit_tiled(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevPar
         for (int q = 0; q < 6; ++q) B.src[q][node] = out[q];
 }
 
-// Mixed tiles listed by k_deposit_tiled (edge_list[0] of them in
-// edge_list[1..], above the stage capacity): each node's own image from
+// Mixed tiles listed by k_deposit_tiled (overflow_list[0] of them in
+// overflow_list[1..], above the stage capacity): each node's own image from
 // global memory, stored like the tiled kernel's; grid-stride over the list
 template <int kDepTX, int kDepTY, int kDepTZ>
 __global__ void __launch_bounds__(kDepositThreads)
-k_deposit_overflow32(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevParams P, const int *edge_list) {
-    const int n = edge_list[0];
+k_deposit_overflow32(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevParams P, const int *overflow_list) {
+    const int n = overflow_list[0];
     for (int e = blockIdx.x; e < n; e += gridDim.x) {
-        const Tile tl = tiles[edge_list[1 + e]];
+        const Tile tl = tiles[overflow_list[1 + e]];
         const DevBox &B = boxes[tl.box];
         const DevGrid &g = B.g;
         const int ntz = (g.nz2 + kDepTZ - 1) / kDepTZ, nty = (g.dny + kDepTY - 1) / kDepTY;

@@ -52,9 +52,9 @@ void launch_payload_mixed(DevBox *boxes, const Tile *tiles, int ntiles, const De
                           cudaStream_t st);
 // dense: some box has per-cell sums (cellsum), deposited by the cell-sum
 // kernels instead of the tiles
-// edge_list: [1 + tiles] ints of scratch (count, then tile indices)
+// overflow_list: [1 + tiles] ints of scratch (count, then tile indices)
 void launch_deposit_mixed(int variant, DevBox *boxes, const Tile *tiles, int ntiles, const DevParams &P,
-                          cudaStream_t st, int nbox, bool dense, int *edge_list);
+                          cudaStream_t st, int nbox, bool dense, int *overflow_list);
 constexpr int kDenseRatio = 16;     // mixed boxes with capacity >= 16 x cells use per-cell sums
 constexpr int kDenseBlocks = 1184;  // grid.x of the cell-sum kernels
 constexpr int kFoldBlocks = 148;    // grid.x of the periodic fold (mixed)

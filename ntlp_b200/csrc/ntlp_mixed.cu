@@ -293,14 +293,14 @@ void launch_payload_mixed(DevBox *boxes, const Tile *tiles, int ntiles, const De
 
 template <int V>
 static void depm(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams &P, cudaStream_t st,
-                 int *edge_list, bool dense) {
+                 int *overflow_list, bool dense) {
     constexpr int TX = kDepShape[V][0], TY = kDepShape[V][1], TZ = kDepShape[V][2];
-    cudaMemsetAsync(edge_list, 0, sizeof(int), st);
+    cudaMemsetAsync(overflow_list, 0, sizeof(int), st);
     k_deposit_tiled<true, TX, TY, TZ>
-        <<<ntiles, kDepositThreads, dep_smem_bytes(true, TX, TY, TZ), st>>>(boxes, tiles, P, edge_list,
+        <<<ntiles, kDepositThreads, dep_smem_bytes(true, TX, TY, TZ), st>>>(boxes, tiles, P, overflow_list,
                                                                            dense ? 1 : 0);
     const int g = ntiles < kDenseBlocks ? ntiles : kDenseBlocks;
-    k_deposit_overflow32<TX, TY, TZ><<<g, kDepositThreads, 0, st>>>(boxes, tiles, P, edge_list);
+    k_deposit_overflow32<TX, TY, TZ><<<g, kDepositThreads, 0, st>>>(boxes, tiles, P, overflow_list);
 }
 
 template <int V>
@@ -320,12 +320,12 @@ void prepare_kernels_mixed() {
 }
 
 void launch_deposit_mixed(int variant, DevBox *boxes, const Tile *tiles, int ntiles, const DevParams &P,
-                          cudaStream_t st, int nbox, bool dense, int *edge_list) {
+                          cudaStream_t st, int nbox, bool dense, int *overflow_list) {
     if (ntiles <= 0) return;
     prepare_kernels_mixed();
-    if (variant == 1) depm<1>(boxes, tiles, ntiles, P, st, edge_list, dense);
-    else if (variant == 2) depm<2>(boxes, tiles, ntiles, P, st, edge_list, dense);
-    else depm<0>(boxes, tiles, ntiles, P, st, edge_list, dense);
+    if (variant == 1) depm<1>(boxes, tiles, ntiles, P, st, overflow_list, dense);
+    else if (variant == 2) depm<2>(boxes, tiles, ntiles, P, st, overflow_list, dense);
+    else depm<0>(boxes, tiles, ntiles, P, st, overflow_list, dense);
     k_fold32<<<dim3(kFoldBlocks, nbox), 256, 0, st>>>(boxes);
     if (dense) {
         k_cellsums32<<<dim3(kDenseBlocks, nbox), 256, 0, st>>>(boxes, P);
