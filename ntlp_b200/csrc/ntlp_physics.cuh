@@ -452,9 +452,9 @@ __device__ double rad_solver2_32(const DevParams &p, double Tf, double qinf, dou
                                  double kap, double radius, double esa, int &mflag) {
     mflag = 0;
     const float pi2 = (float)p.pi2;
-    const float lg = logf((float)((p.Ru * Tf * rhoa * qinf) / (p.Mw * esa)));
-    const float a = -(float)((2.0 * p.Mw * p.Gam) / (p.Ru * p.rhow * Tf)) / lg;
-    const float c = (float)((kap * m_s) / ((2.0 / 3.0) * p.pi2 * p.rhos)) / lg;
+    const float lg = logf((float)Tf * (float)rhoa * (float)qinf / ((float)esa * (float)p.m_q));
+    const float a = -((float)p.m_g / (float)Tf) / lg;
+    const float c = (float)(kap * m_s) / ((float)((2.0 / 3.0) * p.pi2 * p.rhos) * lg);
     const float Q = (a * a) / 9.0f;
     const float R = (2.0f * a * a * a + 27.0f * c) / 54.0f;
     const float M = R * R - Q * Q * Q;
@@ -689,11 +689,11 @@ __device__ __forceinline__ void write_payload_mixed(const DevBox &B, const DevPa
 template <bool MIXED>
 __device__ __forceinline__ double be_drag(const DevParams &p, double radius, double m_s, double rhoa, double dt,
                                           double v[3], const double uf[3]) {
-    const double Volp = p.pi2 * 2.0 / 3.0 * cube(radius);
-    const double rhop = (m_s + Volp * p.rhow) / Volp;
     if (MIXED) {
         const float rr = (float)radius;
-        const float taup_if = 18.0f * (float)rhoa * (float)p.nuf / (float)rhop / ((2.0f * rr) * (2.0f * rr));
+        const float volp = (float)(p.pi2 * 2.0 / 3.0) * (rr * rr * rr);
+        const float rhopf = ((float)m_s + volp * (float)p.rhow) / volp;
+        const float taup_if = 18.0f * (float)rhoa * (float)p.nuf / rhopf / ((2.0f * rr) * (2.0f * rr));
         const float dtf = (float)dt;
         const float den = 1.0f + dtf * taup_if;
         float d0 = (float)(v[0] - uf[0]), d1 = (float)(v[1] - uf[1]), d2 = (float)(v[2] - uf[2]);
@@ -702,6 +702,8 @@ __device__ __forceinline__ double be_drag(const DevParams &p, double radius, dou
             v[a] = (double)(((float)v[a] + taup_if * dtf * (float)uf[a] + dtf * (float)p.g[a]) / den);
         return Rep;
     } else {
+        const double Volp = p.pi2 * 2.0 / 3.0 * cube(radius);
+        const double rhop = (m_s + Volp * p.rhow) / Volp;
         double d0 = v[0] - uf[0], d1 = v[1] - uf[1], d2 = v[2] - uf[2];
         double diffnorm = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
         double taup_i = 18.0 * rhoa * p.nuf / rhop / ((2.0 * radius) * (2.0 * radius));
@@ -869,10 +871,23 @@ __device__ __forceinline__ int be_body(const DevBox &B, const DevParams &p, cons
     Volp = p.pi2 * 2.0 / 3.0 * cube(radius);
     rhop = (m_s + Volp * p.rhow) / Volp;
     const double einf = solved ? esa1 : mod_magnus64(Tf);
-    double qstar = (p.Mw / (p.Ru * Tp * rhoa)) * einf *
-                   ntlp_exp(((p.Lv * p.Mw / p.Ru) * ((1.0 / Tf) - (1.0 / Tp))) +
-                            ((2.0 * p.Mw * p.Gam) / (p.Ru * p.rhow * radius * Tp)) -
-                            ((kap * m_s * p.rhow / p.rhos) / (Volp * rhop - m_s)));
+    double qstar;
+    if (MIXED) {
+        // the diagnostic saturation humidity in FP32: 1/Tf - 1/Tp as
+        // (Tp - Tf)/(Tf Tp) from the FP64 difference, and Volp*rhop - m_s
+        // as Volp*rhow (the same quantity)
+        const float Tpf = (float)Tp, Tff = (float)Tf, rf = (float)radius;
+        const float volp = (float)(p.pi2 * 2.0 / 3.0) * (rf * rf * rf);
+        const float dinv = (float)(Tp - Tf) / (Tff * Tpf);
+        const float E = (float)p.m_e1 * dinv + (float)p.m_g / (rf * Tpf) -
+                        (float)(kap * m_s) / ((float)p.rhos * volp);
+        qstar = (double)((float)p.m_q / (Tpf * (float)rhoa) * (float)einf * expf(E));
+    } else {
+        qstar = (p.Mw / (p.Ru * Tp * rhoa)) * einf *
+                ntlp_exp(((p.Lv * p.Mw / p.Ru) * ((1.0 / Tf) - (1.0 / Tp))) +
+                         ((2.0 * p.Mw * p.Gam) / (p.Ru * p.rhow * radius * Tp)) -
+                         ((kap * m_s * p.rhow / p.rhos) / (Volp * rhop - m_s)));
+    }
     res = res + dt;
     actres = actres + dt;
 
