@@ -661,26 +661,31 @@ __device__ __forceinline__ void write_payload_mixed(const DevBox &B, const DevPa
                                                     const double vold[3], double r, double rold, double Tp,
                                                     double Tpold, double Tf, double m_s, long long mult, double dt) {
     const DevGrid &g = B.g;
-    const double pi2 = p.pi2;
-    double vrhs[3];
-    for (int a = 0; a < 3; ++a) vrhs[a] = (v[a] - vold[a]) / dt;
-    const double radrhs = (r - rold) / dt;
-    const double Tprhs_L = 3.0 * p.Lv / p.Cpp / r * radrhs;
-    const double Tprhs_s = (Tp - Tpold) / dt - Tprhs_L;
+    // the rates from FP64 differences; the factors, stored in FP32, computed
+    // in FP32 (the reference's expressions, with Volp*rhop for partmass and
+    // H0*Cpv/Cpa*(Tf - Tp) for the latent-heat term)
+    const double inv_dt = 1.0 / dt;
+    float vrhs[3];
+    for (int a = 0; a < 3; ++a) vrhs[a] = (float)((v[a] - vold[a]) * inv_dt);
+    const double radrhs = (r - rold) * inv_dt;
+    const double Tprhs_L = p.m_clat * radrhs / r;
+    const double Tprhs_s = (Tp - Tpold) * inv_dt - Tprhs_L;
     const double rhoa =
         (p.iexner == 1) ? func_p_base64(p, p.surf_p, p.tsfcc1, x[2]) / p.Rd / Tf : p.surf_rho;
-    const double rhop = (m_s + pi2 * 2.0 / 3.0 * cube(r) * p.rhow) / (pi2 * 2.0 / 3.0 * cube(r));
-    const double partmass = rhop * 2.0 / 3.0 * pi2 * cube(r);
-    const double taup_i = 18.0 * rhoa * p.nuf / rhop / ((2.0 * r) * (2.0 * r));
-    const double H0 = p.rhow / rhoa * pi2 * 2.0 * (r * r) * radrhs;
+    const float rf = (float)r, rhoaf = (float)rhoa, pi2 = (float)p.pi2, rhow = (float)p.rhow;
+    const float volp = (float)(p.pi2 * 2.0 / 3.0) * (rf * rf * rf);
+    const float rhop = ((float)m_s + volp * rhow) / volp;
+    const float partmass = rhop * volp;
+    const float taup_i = 18.0f * rhoaf * (float)p.nuf / rhop / ((2.0f * rf) * (2.0f * rf));
+    const float H0 = rhow / rhoaf * pi2 * 2.0f * (rf * rf) * (float)radrhs;
     float *const *f = B.pay32.f;
     f[P32_FX][t] = (float)((x[0] - g.dx * (double)(ipt + g.ioff - 1)) / g.dx);
     f[P32_FY][t] = (float)((x[1] - g.dy * (double)(jpt + g.joff - 1)) / g.dy);
     f[P32_FZ][t] = (float)((x[2] - g.zz[kpt]) / g.dzu[kpt + 1]);
-    for (int a = 0; a < 3; ++a) f[P32_DV0 + a][t] = (float)(partmass / rhoa * (vrhs[a] - p.g[a]) + H0 * v[a]);
-    f[P32_T0][t] = (float)(Tprhs_s * 6.0 * p.rhow / rhop / p.CpaCpp / taup_i * (pi2 / 2.0) * r * p.nuf);
-    f[P32_H0][t] = (float)H0;
-    f[P32_E][t] = (float)(H0 * p.Cpv / p.Cpa * Tf - H0 * p.Cpv / p.Cpa * Tp);
+    for (int a = 0; a < 3; ++a) f[P32_DV0 + a][t] = partmass / rhoaf * (vrhs[a] - (float)p.g[a]) + H0 * (float)v[a];
+    f[P32_T0][t] = (float)Tprhs_s * 6.0f * rhow / rhop / (float)p.CpaCpp / taup_i * (pi2 / 2.0f) * rf * (float)p.nuf;
+    f[P32_H0][t] = H0;
+    f[P32_E][t] = H0 * (float)(p.Cpv / p.Cpa) * (float)(Tf - Tp);
     f[P32_FAC][t] = (float)((double)mult / (g.dx * g.dy * g.dzu[kpt + 1]));
 }
 
