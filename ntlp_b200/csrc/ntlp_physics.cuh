@@ -777,11 +777,8 @@ __device__ __forceinline__ int be_body(const DevBox &B, const DevParams &p, cons
         double guess = MIXED ? rad_solver2_32(p, Tf, qinf, rhoa, m_s, kap, radius, esa, mflag)
                              : rad_solver2_64(p, Tf, qinf, rhoa, m_s, kap, radius, esa, mflag);
         double rt_start[2];
-        if (mflag == 0) { rt_start[0] = guess / radius; rt_start[1] = Tf / Tp; }
-        else { rt_start[0] = 1.0; rt_start[1] = 1.0; }
         Drop D;
         D.Tf = Tf; D.qinf = qinf; D.m_s = m_s; D.radius = radius; D.Tp = Tp; D.rhoa = rhoa;
-        D.h = dt / taup0;
         {
             double e0 = uf[0] - v[0], e1 = uf[1] - v[1], e2 = uf[2] - v[2];
             D.diffnorm = sqrt(e0 * e0 + e1 * e1 + e2 * e2);
@@ -791,9 +788,23 @@ __device__ __forceinline__ int be_body(const DevBox &B, const DevParams &p, cons
         D.inv_Tf = 1.0 / Tf;
         D.c_taup = 18.0 * rhoa * p.nuf;
         D.c_sol = kap * m_s * p.rhow / p.rhos;
-        D.t0r = taup0 / radius;
-        D.rt0 = radius / taup0;
-        D.t0T = taup0 / Tp;
+        if (MIXED) {
+            // three reciprocals instead of seven divides
+            const double ir = 1.0 / radius, it0 = 1.0 / taup0, iTp = 1.0 / Tp;
+            if (mflag == 0) { rt_start[0] = guess * ir; rt_start[1] = Tf * iTp; }
+            else { rt_start[0] = 1.0; rt_start[1] = 1.0; }
+            D.h = dt * it0;
+            D.t0r = taup0 * ir;
+            D.rt0 = radius * it0;
+            D.t0T = taup0 * iTp;
+        } else {
+            if (mflag == 0) { rt_start[0] = guess / radius; rt_start[1] = Tf / Tp; }
+            else { rt_start[0] = 1.0; rt_start[1] = 1.0; }
+            D.h = dt / taup0;
+            D.t0r = taup0 / radius;
+            D.rt0 = radius / taup0;
+            D.t0T = taup0 / Tp;
+        }
         int flag;
         if (MIXED) {
             // FP32 Gauss-Newton to within ~1e-6 of the root, then FP64
