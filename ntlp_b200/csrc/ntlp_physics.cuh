@@ -884,8 +884,10 @@ __device__ __forceinline__ int be_body(const DevBox &B, const DevParams &p, cons
         double tmp_coeff = Nup / 3.0 / p.Pra * p.CpaCpp * rhop / p.rhow * taup_i;
         Tp = (Tp + tmp_coeff * dt * Tf) / (1.0 + dt * tmp_coeff);
     }
-    Volp = p.pi2 * 2.0 / 3.0 * cube(radius);
-    rhop = (m_s + Volp * p.rhow) / Volp;
+    if (!MIXED) {
+        Volp = p.pi2 * 2.0 / 3.0 * cube(radius);
+        rhop = (m_s + Volp * p.rhow) / Volp;
+    }
     const double einf = solved ? esa1 : mod_magnus64(Tf);
     double qstar;
     if (MIXED) {
@@ -926,8 +928,11 @@ __device__ __forceinline__ int be_body(const DevBox &B, const DevParams &p, cons
         if (xp3i < x[2]) { lo = fluxloci; hi = fluxloc - 1; sgn = 1.0; }
         else if (xp3i > x[2]) { lo = fluxloc; hi = fluxloci - 1; sgn = -1.0; }
         if (hi >= lo) {
-            double mterm = rhop * Volp * mult;
-            double eterm = rhop * Volp * p.Cpp * Tp * mult;
+            // the droplet's mass rhop*Volp; mixed: as m_s + Volp*rhow (the
+            // same quantity, no divide)
+            const double pmass = MIXED ? m_s + (p.pi2 * 2.0 / 3.0 * cube(radius)) * p.rhow : rhop * Volp;
+            double mterm = pmass * mult;
+            double eterm = pmass * p.Cpp * Tp * mult;
             const int nz1 = g.nnz + 1;
             for (int iz = lo; iz <= hi; ++iz) {
                 if (iz < 0 || iz > g.nnz) continue;
