@@ -492,8 +492,7 @@ __device__ __forceinline__ void block_add_counters(const DevBox &B, const Counts
     if (threadIdx.x < kNumCounters) sh[threadIdx.x] = 0;
     __syncthreads();
     for (int k = 0; k < kNumCounters; ++k) {
-        int v = c.v[k];
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        const int v = (int)__reduce_add_sync(0xffffffffu, (unsigned)c.v[k]);   // one warp reduction
         if ((threadIdx.x & 31) == 0 && v) atomicAdd(&sh[k], v);
     }
     __syncthreads();
