@@ -372,13 +372,18 @@ k_deposit_tiled(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevPar
             s_cs[e] = v;
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
-            int o = 0;
-            for (int cc = 0; cc < kDepCols; ++cc) {
-                s_off[cc] = o;
-                o += s_cs[cc * kDepCSW + kDepCSW - 1] - s_cs[cc * kDepCSW];
+        static_assert(kDepCols <= 32, "one warp scans the column counts");
+        if (threadIdx.x < 32) {
+            // exclusive scan of the columns' droplet counts (stage offsets)
+            const int cc = threadIdx.x;
+            const int cnt = cc < kDepCols ? s_cs[cc * kDepCSW + kDepCSW - 1] - s_cs[cc * kDepCSW] : 0;
+            int incl = cnt;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (cc >= o) incl += y;
             }
-            s_total = o;
+            if (cc < kDepCols) s_off[cc] = incl - cnt;
+            if (cc == kDepCols - 1) s_total = incl;
         }
         __syncthreads();
         staged = s_total <= CAP;
