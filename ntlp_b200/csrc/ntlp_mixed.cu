@@ -73,6 +73,7 @@ __device__ void interp6_mixed(const DevBox &B, double x1, double x2, double x3, 
     const int ip3 = ip3g - g.ioff, jp3 = jp3g - g.joff;     // local (array indices)
     const int ku2 = minloc_zz(g, x3) - 2;
     const int kw2 = minloc_z(g, x3) - 2;
+    o.kw = kw2 + 2;
     if (ku2 < 0 || ku2 > nnz + 1 || kw2 < 0) bad = 1;
     float wx[6], wy[6], wz[6], wzw[6];
     // xn(a) = dx*(ip3-3+a): s = x/dx - (ip3-3) in [2, 3)
@@ -150,6 +151,7 @@ __device__ void interp_lin_mixed(const DevBox &B, double x1, double x2, double x
     int jpt = jptg - g.joff;
     int kpt = minloc_zz(g, x3) - 2;
     int kwpt = minloc_z(g, x3) - 2;
+    o.kw = kwpt + 2;
     if (kpt + 1 < 0 || kpt + 1 > g.nnz + 2 || kwpt + 1 < 0 || kwpt + 1 > g.nnz + 2) {
         bad = 1;
         kpt = kpt < -1 ? -1 : (kpt > g.nnz + 1 ? g.nnz + 1 : kpt);
@@ -219,7 +221,7 @@ k_interp_mixed(DevBox *boxes, const Tile *tiles) {
     O.uf[2][t] = I.uf[2];
     O.Tf[t] = I.Tf;
     O.qinf[t] = I.qinf;
-    B.key[t] = bad;
+    B.key[t] = bad | (I.kw << 1);
 }
 
 // 7 resident blocks of 128: 72 registers, 28 warps per SM (spills, to L1).

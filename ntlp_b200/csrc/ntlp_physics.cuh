@@ -19,6 +19,7 @@ namespace {
 
 struct Interp {
     double uf[3], Tf, qinf;
+    int kw;   // mixed path: minloc_z of the droplet's height, for the flux tally
 };
 
 // ---------------------------------------------------------------------------
@@ -851,7 +852,9 @@ __device__ __forceinline__ int be_body(const DevBox &B, const DevParams &p, cons
     double res = S.res[s], actres = S.actres[s], numact = S.numact[s];
     const long long multi = S.mult[s];
     const double mult = (double)multi;
-    const int bad = B.key[t];
+    // mixed: the interpolation left bad | minloc_z(x3) << 1 in key[t]
+    const int bad = MIXED ? (B.key[t] & 1) : B.key[t];
+    const int kw_old = MIXED ? (B.key[t] >> 1) : 0;
     for (int a = 0; a < 3; ++a) vold[a] = v[a];
     const double Tpold = Tp, rold = radius;
     double Tf = O.Tf[t];
@@ -914,13 +917,13 @@ __device__ __forceinline__ int be_body(const DevBox &B, const DevParams &p, cons
         int fluxloc, fluxloci;
         if (x[2] > g.zl) {
             fluxloc = g.nnz + 1;
-            fluxloci = minloc_z(g, xp3i) - 1;
+            fluxloci = (MIXED ? kw_old : minloc_z(g, xp3i)) - 1;
         } else if (x[2] < 0.0) {
-            fluxloci = minloc_z(g, xp3i) - 1;
+            fluxloci = (MIXED ? kw_old : minloc_z(g, xp3i)) - 1;
             fluxloc = 0;
         } else {
             fluxloc = minloc_z(g, x[2]) - 1;
-            fluxloci = minloc_z(g, xp3i) - 1;
+            fluxloci = (MIXED ? kw_old : minloc_z(g, xp3i)) - 1;
         }
         int lo = 0, hi = -1;
         double sgn = 0.0;
