@@ -379,6 +379,7 @@ k_update_rk3_64(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevPar
                 write_payload(B, p, t, x, v, vold, radius, rold, Tp, Tpold, Tf, m_s, multi, dt);
         }
         B.key[t] = key;
+        atomicAdd(&B.cell_cnt[key], 1);   // the sort's histogram
     }
     block_add_counters(B, cnt);
 }

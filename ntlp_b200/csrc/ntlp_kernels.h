@@ -74,7 +74,7 @@ struct SortPlan {
     int nbox;
     int *any_big;            // some box has cells above kSmallCell (set by k_cellsort)
 };
-constexpr int kSortLaunches = 8;   // kernels launched by launch_sort
+constexpr int kSortLaunches = 7;   // kernels launched by launch_sort
 constexpr int kSmallCell = 32;     // cells up to this size are insertion-sorted by one thread
 constexpr int kRankBlocks = 1184;  // grid of the large-cell ranking (8 blocks per SM)
 void launch_sort(DevBox *boxes, const SortPlan &plan, cudaStream_t st);

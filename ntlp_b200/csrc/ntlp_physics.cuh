@@ -978,6 +978,7 @@ __device__ __forceinline__ int be_body(const DevBox &B, const DevParams &p, cons
         }
     }
     B.key[t] = key;
+    atomicAdd(&B.cell_cnt[key], 1);   // the sort's histogram (cell_cnt is zero between sorts)
     for (int k = 0; k < kNumCounters; ++k) cnt.v[k] += dc.v[k];
     return 0;
 }

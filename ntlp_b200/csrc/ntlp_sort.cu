@@ -15,15 +15,10 @@
 
 namespace ntlp {
 
-// ---- histogram -------------------------------------------------------------
-__global__ void k_hist(DevBox *boxes, const Tile *tiles) {
-    const Tile tl = tiles[blockIdx.x];
-    const DevBox &B = boxes[tl.box];
-    const int t = tl.start + threadIdx.x;
-    if (t >= *B.n_alive) return;
-    atomicAdd(&B.cell_cnt[B.key[t]], 1);
-}
-
+// ---- histogram: counted by the kernels that write the keys (the update
+// kernels and k_keys_initial add 1 to cell_cnt[key]); cell_cnt is zero
+// between sorts (k_scan_local clears it for the scatter's cursors and
+// k_cellsort after them)
 // ---- scan (three phases over tiles of kScanTile buckets) -----------------
 __device__ __forceinline__ long long nbuckets(const DevBox &B) { return B.g.ncells + 2; }
 
@@ -226,7 +221,6 @@ __global__ void k_cellcopy(DevBox *boxes, const Tile *tiles, int ntiles, const i
 }
 
 void launch_sort(DevBox *boxes, const SortPlan &plan, cudaStream_t st) {
-    k_hist<<<plan.n_drop_tiles, kUpdateThreads, 0, st>>>(boxes, plan.drop_tiles);
     k_scan_sums<<<plan.n_cell_tiles, 256, 0, st>>>(boxes, plan.cell_tiles, plan.tile_sums);
     k_scan_offsets<<<plan.nbox, 1024, 0, st>>>(boxes, plan.box_first_tile, plan.tile_sums, plan.any_big);
     k_scan_local<<<plan.n_cell_tiles, kCellThreads, 0, st>>>(boxes, plan.cell_tiles, plan.tile_sums);
@@ -284,6 +278,7 @@ __global__ void k_keys_initial(DevBox *boxes, const Tile *tiles) {
     const DevState &O = B.st[1 - B.cur];
     int key = cell_key(B.g, O.x[0][t], O.x[1][t], O.x[2][t]);
     B.key[t] = key;
+    atomicAdd(&B.cell_cnt[key], 1);   // the sort's histogram
 }
 
 void launch_keys_initial(DevBox *boxes, const Tile *tiles, int ntiles, cudaStream_t st) {
