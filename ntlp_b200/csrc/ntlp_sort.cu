@@ -17,8 +17,7 @@ namespace ntlp {
 
 // ---- histogram: counted by the kernels that write the keys (the update
 // kernels and k_keys_initial add 1 to cell_cnt[key]); cell_cnt is zero
-// between sorts (k_scan_local clears it for the scatter's cursors and
-// k_cellsort after them)
+// between sorts (the scatter counts each cell back down to zero)
 // ---- scan (three phases over tiles of kScanTile buckets) -----------------
 __device__ __forceinline__ long long nbuckets(const DevBox &B) { return B.g.ncells + 2; }
 
@@ -120,7 +119,6 @@ __global__ void k_scan_local(DevBox *boxes, const Tile *tiles, const long long *
         long long c = base + k;
         if (c < nb) {
             B.cell_start[c] = (int)run;
-            B.cell_cnt[c] = 0;
             run += v[k];
             if (c == nb - 1) B.cell_start[nb] = (int)run;
         }
@@ -134,11 +132,14 @@ __global__ void k_scatter(DevBox *boxes, const Tile *tiles) {
     const int t = tl.start + threadIdx.x;
     if (t >= *B.n_alive) return;
     const int k = B.key[t];
-    const int pos = B.cell_start[k] + atomicAdd(&B.cell_cnt[k], 1);
+    // counts down: the last droplet of a cell leaves its count at zero,
+    // ready for the next step's histogram (the order inside a cell is
+    // k_cellsort's)
+    const int pos = B.cell_start[k] + atomicSub(&B.cell_cnt[k], 1) - 1;
     B.sorted[pos] = t;
 }
 
-// ---- per-cell list order (ascending lid), clears the cursor ---------------
+// ---- per-cell list order (ascending lid) -----------------------------------
 __global__ void k_cellsort(DevBox *boxes, const Tile *tiles, int *any_big) {
     const Tile tl = tiles[blockIdx.x];
     const DevBox &B = boxes[tl.box];
@@ -147,7 +148,6 @@ __global__ void k_cellsort(DevBox *boxes, const Tile *tiles, int *any_big) {
     for (int i = threadIdx.x; i < kScanTile; i += blockDim.x) {
         const long long c = (long long)tl.start + i;
         if (c >= nb) break;
-        B.cell_cnt[c] = 0;
         if (c == nb - 1) continue;       // killed droplets: order irrelevant
         const int a = B.cell_start[c], e = B.cell_start[c + 1];
         if (e - a < 2) continue;
