@@ -60,7 +60,7 @@ B_D = {"fp64": 248, "mixed": 224}       # algorithmic bytes per droplet
 # measured by ncu at 1M droplets / 128^3 (fields subtracted), used to scale
 # the measured traffic to the bench workload; see
 # profiles/k_interp_be_deposit_mixed_1M_droplets_128cube.md
-NCU_BYTES_PER_DROPLET = {"mixed": 400.0}
+NCU_BYTES_PER_DROPLET = {"mixed": 440.0}
 METRIC = "droplet-updates/s (mixed vs FP64 GPU) at 16M; p50/p99 serving step latency"
 
 
@@ -150,17 +150,32 @@ class ClockSampler:
                                        "-lms", "50"], stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
+        # nvidia-smi takes a while to start: wait for its first sample, so the
+        # samples kept (those after this mark) fall in the timed region
+        self.mark = 0
+        t0 = time.perf_counter()
+        while self.p is not None and time.perf_counter() - t0 < 5.0:
+            size = os.path.getsize(self.f.name)
+            if size > 0:
+                self.mark = size
+                break
+            time.sleep(0.02)
 
     def stop(self) -> dict:
         if self.p is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        # a timed region shorter than the sampling interval: take the sample
+        # that follows it
+        t0 = time.perf_counter()
+        while os.path.getsize(self.f.name) <= self.mark and time.perf_counter() - t0 < 0.5:
+            time.sleep(0.01)
         self.p.terminate()
         try:
             self.p.wait(timeout=5)
         except Exception:
             self.p.kill()
         self.f.flush()
-        self.f.seek(0)
+        self.f.seek(self.mark)
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in self.f.read().splitlines():
