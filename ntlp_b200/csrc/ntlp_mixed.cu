@@ -1,10 +1,11 @@
 // ntlp_mixed.cu -- mixed-precision droplet-step kernels.
 //
 // Interpolation weights and stencil products in FP32 with FP32 accumulation,
-// reading FP32 copies of the fields (half the bytes of the FP64 path); drag
-// in FP32.  The FP32 copies hold deviations from a reference value of each
-// field (its value at the interior point (1,1,1)), which is added back in
-// FP64 after the contraction.  Positions, the Newton radius/temperature solve and the source
+// reading FP32 copies of the fields (half the bytes of the FP64 path); drag,
+// equilibrium guess and the first Gauss-Newton iterations in FP32.  The FP32
+// copies hold deviations from a reference value of each field (its value at
+// the interior point (1,1,1)), which is added back in FP64 after the
+// contraction.  Positions, the final Gauss-Newton step and the source
 // accumulation stay FP64.  Offsets from the droplet to the stencil nodes are
 // formed in FP64 and only then rounded to FP32, so positions up to a few
 // hundred metres keep their sub-cell resolution.

@@ -640,22 +640,8 @@ __device__ __forceinline__ void write_payload(const DevBox &B, const DevParams &
 }
 
 
-// ---------------------------------------------------------------------------
-// backward-Euler droplet body (particles.f90:3043-3242 + 3248-3260): all of
-// the per-droplet work after the interpolation, which an earlier kernel has
-// written to the output buffer at the droplet's slot t (uf, Tf before the
-// Exner factor, qinf; out-of-range flag in key[t]).  MIXED computes the drag
-// (taup_i and the implicit velocity update) in FP32; positions, the Newton
-// radius/temperature solve and everything else stay FP64.
-//
-// With ALLOW_LM false, a droplet whose Gauss-Newton solve fails is appended
-// to the box's defer list and left untouched (no output, no counter, no
-// tally); a second pass re-runs it with ALLOW_LM true, where the rare
-// Levenberg-Marquardt fallback (up to 1000 iterations) does not hold back
-// the 31 other droplets of a warp.  Returns 1 if deferred.
-// ---------------------------------------------------------------------------
-// Mixed-precision payload: the same FP64 factors as write_payload, stored
-// as FP32 with the cell-relative fractions that make the trilinear weights.
+// Mixed-precision payload: the factors of write_payload, stored as FP32 with
+// the cell-relative fractions that make the trilinear weights.
 __device__ __forceinline__ void write_payload_mixed(const DevBox &B, const DevParams &p, int t, int ipt, int jpt,
                                                     int kpt, const double x[3], const double v[3],
                                                     const double vold[3], double r, double rold, double Tp,
@@ -733,9 +719,11 @@ __device__ __forceinline__ double air_density(const DevParams &p, double x3, dou
 // backward-Euler droplet body (particles.f90:3043-3242 + 3248-3260): all of
 // the per-droplet work after the interpolation, which an earlier kernel has
 // written to the output buffer at the droplet's slot t (uf, Tf before the
-// Exner factor, qinf; out-of-range flag in key[t]).  MIXED computes the drag
-// (taup_i and the implicit velocity update) in FP32; positions, the Newton
-// radius/temperature solve and everything else stay FP64.
+// Exner factor, qinf; out-of-range flag in key[t], and for MIXED the height
+// index of the old position).  MIXED computes in FP32 the drag (taup_i and
+// the implicit velocity update), the equilibrium guess, the first
+// Gauss-Newton iterations, the diagnostic qstar and the deposition factors;
+// positions, the final Gauss-Newton step and the state stay FP64.
 //
 // The Newton solve runs first with only its own inputs loaded; everything
 // else is (re)loaded and (re)computed after it with the same operations, so
