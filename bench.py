@@ -442,6 +442,15 @@ def cpu_baseline(case, seconds: float, dist=None):
                 seconds_per_step=t_full)
 
 
+def workload_config(args, parallelism: str) -> dict:
+    """The `config` object of both arms (the same workload)."""
+    nx, ny, nz = args.grid
+    return {"workload": f"BE droplet step + coupling, {args.n} droplets, {nx}x{ny}x{nz} grid, "
+                        f"ilin={args.ilin} ({'6th-order' if args.ilin == 0 else 'trilinear'}), dt=5e-4",
+            "droplets": args.n, "grid": [nx, ny, nz],
+            "l2": "state (~3.5 GB) >> L2; no flush needed", "parallelism": parallelism}
+
+
 def main():
     args = parse()
     rank, ws, dist = dist_setup(args)
@@ -460,8 +469,7 @@ def main():
         line = {"metric": METRIC, "value": v, "unit": "droplet-updates/s", "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64", "data": "synthetic (seeded generator; no dataset)", "impl": "reference",
-                "config": {"workload": f"BE droplet step, {args.n} droplets, {args.grid[0]}x{args.grid[1]}x{args.grid[2]} grid, "
-                                       f"ilin={args.ilin}, dt=5e-4", "parallelism": "host OpenMP"},
+                "config": workload_config(args, f"host OpenMP, {cb['cores']} threads"),
                 "cpu_baseline": cb,
                 "e2e": {"value": v, "unit": "droplet-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
@@ -518,10 +526,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": r["ms"] / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 interp/drag + f64 state/Newton/sources" if head == "mixed" else "f64",
         "data": "synthetic (seeded generator; no dataset)",
-        "config": {"workload": f"BE droplet step + coupling, {n} droplets, {g['nnx']}x{g['nny']}x{g['nnz']} grid, "
-                               f"ilin={args.ilin} ({'6th-order' if args.ilin == 0 else 'trilinear'}), dt=5e-4",
-                   "droplets": n, "grid": [g["nnx"], g["nny"], g["nnz"]],
-                   "l2": "state (~3.5 GB) >> L2; no flush needed", "parallelism": f"{ws} replica(s)"},
+        "config": workload_config(args, f"{ws} replica(s)"),
         "phases_ms_per_step": {k: v / args.steps for k, v in r["prof"].items() if k.endswith("_ms")},
         "autotune": (None if not r.get("tune") else
                      {"deposit_shape": ["2x4x32", "4x4x16", "2x2x64"][r["tune"]["deposit_variant"]],
