@@ -384,6 +384,8 @@ void fill_devparams(const ntlp_params *p, DevParams &d) {
     d.m_g = 2.0 * p->Mw * p->Gam / (p->Ru * p->rhow);
     d.m_e1 = p->Lv * p->Mw / p->Ru;
     d.m_q = p->Mw / p->Ru;
+    d.m_vri = 1.0 / ((2.0 / 3.0) * p->pi2 * (p->radius_init * p->radius_init * p->radius_init));
+    d.m_t0 = (2.0 * p->radius_init) * (2.0 * p->radius_init) / (18.0 * p->nuf);
     // set_binsdata calls of particles.f90:1909-1921
     d.hb[NTLP_H_ACTRES] = ntlp_hist_log_bins(1.0e-1, 1.0e4);
     d.hb[NTLP_H_RES] = ntlp_hist_log_bins(1.0e-1, 1.0e4);

@@ -77,6 +77,8 @@ struct DevParams {
     // 1/(36 Sc rhow), -CpaCpp/(12 Pra rhow), 2/nuf, 1/(rhow (2/3) pi2),
     // 3 Lv/Cpp, 2 Mw Gam/(Ru rhow), Lv Mw/Ru, Mw/Ru
     double m_rpre, m_tpre, m_rep, m_solv, m_clat, m_g, m_e1, m_q;
+    // and of taup0: 1/((2/3) pi2 radius_init^3), (2 radius_init)^2/(18 nuf)
+    double m_vri, m_t0;
     // histogram binning (particles.f90:1909-1921), by NTLP_H_* kind
     ntlp_hbins hb[NTLP_H_STEP_KINDS];
 };

@@ -47,6 +47,7 @@ struct Drop {
     double c_taup;               // 18.0*rhoa*nuf
     double c_sol;                // kappa_s*m_s*rhow/rhos
     double t0r, rt0, t0T;        // taup0/radius, radius/taup0, taup0/Tp
+    double irhoa;                // mixed path: 1/rhoa
 };
 
 // ie_vrt_nd split in its r-dependent and T-dependent parts; the evaluation
@@ -191,7 +192,7 @@ __device__ __forceinline__ AdConst ad_const(const DevParams &p, const Drop &d) {
     k.k_clat = p.m_clat;
     k.k_g = p.m_g;
     k.k_e1 = p.m_e1;
-    k.k_q = p.m_q * d.esa / d.rhoa;
+    k.k_q = p.m_q * d.esa * d.irhoa;
     return k;
 }
 
@@ -758,7 +759,10 @@ __device__ __forceinline__ int be_body(const DevBox &B, const DevParams &p, cons
             v[a] = (in.it <= 1) ? uf[a] : S.v[a][s];
         }
         be_drag<MIXED>(p, radius, m_s, rhoa, dt, v, uf);
-        const double taup0 = taup0_64(p, m_s, rhoa);
+        const double irhoa = MIXED ? 1.0 / rhoa : 0.0;
+        // mixed: taup0 from the per-run factors (one reciprocal of rhoa,
+        // shared with the solve's constants)
+        const double taup0 = MIXED ? (m_s * p.m_vri + p.rhow) * p.m_t0 * irhoa : taup0_64(p, m_s, rhoa);
         const double esa = mod_magnus64(Tf);
         esa1 = esa;
         int mflag;
@@ -776,6 +780,7 @@ __device__ __forceinline__ int be_body(const DevBox &B, const DevParams &p, cons
         D.inv_Tf = 1.0 / Tf;
         D.c_taup = 18.0 * rhoa * p.nuf;
         D.c_sol = kap * m_s * p.rhow / p.rhos;
+        D.irhoa = irhoa;
         if (MIXED) {
             // three reciprocals instead of seven divides
             const double ir = 1.0 / radius, it0 = 1.0 / taup0, iTp = 1.0 / Tp;
