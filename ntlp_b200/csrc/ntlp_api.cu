@@ -92,6 +92,7 @@ struct ntlp_ctx {
     double g_dt = 0.0;
     int g_nsteps = 0, g_dep = -1, g_nt = -1;
     bool tex_all = true;   // every box's FP32 fields have a texture (mixed)
+    bool tex_all64 = true;   // every box's FP64 fields have textures (FP64)
     bool any_dense = false;   // some box deposits through per-cell sums (mixed)
     int64_t g_launches = 0;
     int64_t bytes = 0;
@@ -165,6 +166,27 @@ unsigned long long f4_texture(const float4 *base, size_t count) {
     return (unsigned long long)t;
 }
 
+// an FP64 field (count elements) as a 1D linear texture of int2, read
+// element by element; 0 when the device refuses it
+unsigned long long f64_texture(const double *base, size_t count) {
+    cudaResourceDesc rd{};
+    rd.resType = cudaResourceTypeLinear;
+    rd.res.linear.devPtr = (void *)base;
+    rd.res.linear.desc = cudaCreateChannelDesc<int2>();
+    rd.res.linear.sizeInBytes = count * sizeof(double);
+    cudaTextureDesc td{};
+    td.addressMode[0] = cudaAddressModeClamp;
+    td.filterMode = cudaFilterModePoint;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 0;
+    cudaTextureObject_t t = 0;
+    if (cudaCreateTextureObject(&t, &rd, &td, nullptr) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return (unsigned long long)t;
+}
+
 void carve_state(Carver &cv, DevState &s, size_t n) {
     for (int a = 0; a < 3; ++a) {
         cv.take(&s.x[a], n); cv.take(&s.v[a], n); cv.take(&s.uf[a], n); cv.take(&s.vold[a], n);
@@ -197,7 +219,9 @@ void carve_box(Carver &cv, BoxHost &h, DevBox &B, bool mixed) {
     }
     for (int k = 0; k < 5; ++k) {
         double *f;
-        cv.take(&f, npad);
+        // FP64 path: + 1 KB, to start the texture on a 1 KB boundary
+        cv.take(&f, npad + (mixed ? 0 : 128));
+        if (f && !mixed) f = (double *)(((uintptr_t)f + 1023) & ~(uintptr_t)1023);
         B.f[k] = f;
     }
     if (mixed) {
@@ -499,8 +523,11 @@ extern "C" void ntlp_ctx_destroy(ntlp_ctx *c) {
         cudaEventDestroy(r.b);
     }
     for (cudaEvent_t e : c->pool) cudaEventDestroy(e);
-    for (const DevBox &B : c->box)
+    for (const DevBox &B : c->box) {
         if (B.tex_f4) cudaDestroyTextureObject((cudaTextureObject_t)B.tex_f4);
+        for (int q = 0; q < 5; ++q)
+            if (B.tex_f64[q]) cudaDestroyTextureObject((cudaTextureObject_t)B.tex_f64[q]);
+    }
     for (auto &h : c->bh) {
         if (h.arena) cudaFreeAsync(h.arena, c->stream);
         if (h.arena_rk3) cudaFreeAsync(h.arena_rk3, c->stream);
@@ -636,9 +663,16 @@ int create(int nbox, const ntlp_grid *grids, const ntlp_params *params, const in
             if (cudaMemsetAsync((void *)(B.f4 - kF32Guard), 0, npad * sizeof(float4), c->stream) ||
                 cudaMemsetAsync((void *)(B.fw - kF32Guard), 0, npad * sizeof(float), c->stream))
                 return bail(fail(c, NTLP_ERR_CUDA, "initialising box %d failed", b));
+            for (int q = 0; q < 5; ++q) B.tex_f64[q] = 0;
             B.tex_f4 = f4_texture(B.f4 - kF32Guard, npad);
             if (!B.tex_f4) c->tex_all = false;
             if (B.cellsum) c->any_dense = true;
+        } else {
+            B.tex_f4 = 0;
+            for (int q = 0; q < 5; ++q) {
+                B.tex_f64[q] = f64_texture(B.f[q], (size_t)nz2 * B.g.ny5 * B.g.nx5);
+                if (!B.tex_f64[q]) c->tex_all64 = false;
+            }
         }
         if (cudaMemcpyAsync((void *)B.g.lut_zz, h.lut.data(), h.lut.size() * sizeof(int), cudaMemcpyHostToDevice,
                             c->stream) ||
@@ -934,7 +968,7 @@ int launch_step(ntlp_ctx *c, int kind, int istage, double dt, int32_t it, bool w
                                    c->dp, in, c->stream, c->tex_all);
         else
             launch_update_be64(c->params.ilin, nt, c->box_d, c->drop_tiles_d[c->nt_variant],
-                               c->n_drop_tiles[c->nt_variant], c->nbox, c->dp, in, c->stream);
+                               c->n_drop_tiles[c->nt_variant], c->nbox, c->dp, in, c->stream, c->tex_all64);
         c->launches += kUpdateLaunches;
     } else {
         launch_update_rk3_64(c->params.ilin, c->box_d, c->drop_tiles_d[0], c->n_drop_tiles[0], c->dp, in,

@@ -117,6 +117,9 @@ struct DevBox {
     // mixed path: f4 as a 1D linear texture (element 0 = the first guard
     // element, f4 - kF32GuardDev), 0 when the device refused it
     unsigned long long tex_f4;
+    // FP64 path: the five FP64 fields as 1D linear textures of int2 (the
+    // same 8 bytes per element), 0 when the device refused them
+    unsigned long long tex_f64[5];
     DevState st[2];
     DevPayload pay;
     DevPayload32 pay32;    // mixed path

@@ -96,6 +96,19 @@ __device__ __forceinline__ void lagrange6(double x, const double xn[6], int firs
 }
 
 // uf_interp, particles.f90:554-765
+// one field value; TEXPATH: through the texture path (the same 8 bytes)
+template <bool TEXPATH>
+__device__ __forceinline__ double ld64(const double *f, unsigned long long tex, long long a) {
+    if (TEXPATH) {
+        const int2 v = tex1Dfetch<int2>((cudaTextureObject_t)tex, (int)a);
+        return __hiloint2double(v.y, v.x);
+    }
+    return __ldg(f + a);
+}
+
+// TEX: the first two x columns of the stencil through the texture path (its
+// own L1 data pipe)
+template <bool TEX>
 __device__ void interp6_64(const DevBox &B, double x1, double x2, double x3, Interp &o, int &bad) {
     const DevGrid &g = B.g;
     const int nnz = g.nnz;
@@ -186,11 +199,25 @@ __device__ void interp6_64(const DevBox &B, double x1, double x2, double x3, Int
             for (int i = 0; i < 6; ++i) {
                 const double wi = wx[i];
                 const long long a = bu + xo[i], aw = bw + xo[i];
-                u1 = u1 + __ldg(fu + a) * wi * wj * wk;
-                u2 = u2 + __ldg(fv + a) * wi * wj * wk;
-                u3 = u3 + __ldg(fw + aw) * wi * wj * wkw;
-                T = T + __ldg(fT + a) * wi * wj * wk;
-                q = q + __ldg(fq + a) * wi * wj * wk;
+                double vu, vv, vw, vT, vq;
+                if (TEX && i < 2) {
+                    vu = ld64<true>(fu, B.tex_f64[0], a);
+                    vv = ld64<true>(fv, B.tex_f64[1], a);
+                    vw = ld64<true>(fw, B.tex_f64[2], aw);
+                    vT = ld64<true>(fT, B.tex_f64[3], a);
+                    vq = ld64<true>(fq, B.tex_f64[4], a);
+                } else {
+                    vu = ld64<false>(fu, 0, a);
+                    vv = ld64<false>(fv, 0, a);
+                    vw = ld64<false>(fw, 0, aw);
+                    vT = ld64<false>(fT, 0, a);
+                    vq = ld64<false>(fq, 0, a);
+                }
+                u1 = u1 + vu * wi * wj * wk;
+                u2 = u2 + vv * wi * wj * wk;
+                u3 = u3 + vw * wi * wj * wkw;
+                T = T + vT * wi * wj * wk;
+                q = q + vq * wi * wj * wk;
             }
 #pragma unroll
             for (int r = 0; r < 5; ++r) { wyr[r] = wyr[r + 1]; yor[r] = yor[r + 1]; }
@@ -208,7 +235,7 @@ __device__ void interp6_64(const DevBox &B, double x1, double x2, double x3, Int
 // launches: interpolation, droplet body with Gauss-Newton, deferred
 // Levenberg-Marquardt droplets.
 // ---------------------------------------------------------------------------
-template <int ILIN, int NT>
+template <int ILIN, int NT, bool TEX>
 __global__ void __launch_bounds__(NT)
 k_interp64(DevBox *boxes, const Tile *tiles) {
     const Tile tl = tiles[blockIdx.x];
@@ -221,7 +248,7 @@ k_interp64(DevBox *boxes, const Tile *tiles) {
     Interp I;
     int bad = 0;
     if (ILIN == 1) interp_lin64(B, S.x[0][s], S.x[1][s], S.x[2][s], I, bad);
-    else interp6_64(B, S.x[0][s], S.x[1][s], S.x[2][s], I, bad);
+    else interp6_64<TEX>(B, S.x[0][s], S.x[1][s], S.x[2][s], I, bad);
     O.uf[0][t] = I.uf[0];
     O.uf[1][t] = I.uf[1];
     O.uf[2][t] = I.uf[2];
@@ -304,7 +331,7 @@ k_update_rk3_64(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevPar
         Interp I;
         int bad = 0;
         if (ILIN == 1) interp_lin64(B, x[0], x[1], x[2], I, bad);
-        else interp6_64(B, x[0], x[1], x[2], I, bad);
+        else interp6_64<false>(B, x[0], x[1], x[2], I, bad);
         double Tf = I.Tf, qinf = I.qinf, rhoa;
         if (p.iexner == 1) {
             Tf = Tf * exner64(p, p.surf_p, func_p_base64(p, p.surf_p, p.tsfcc1, x[2]));
@@ -404,15 +431,17 @@ __global__ void k_payload64(DevBox *boxes, const Tile *tiles, const __grid_const
 // launchers
 // ---------------------------------------------------------------------------
 void launch_update_be64(int ilin, int nt, DevBox *boxes, const Tile *tiles, int ntiles, int nbox,
-                        const DevParams &P, StepIn in, cudaStream_t st) {
+                        const DevParams &P, StepIn in, cudaStream_t st, bool tex) {
     if (ntiles <= 0) return;
     if (nt == 256) {
-        if (ilin == 1) k_interp64<1, 256><<<ntiles, 256, 0, st>>>(boxes, tiles);
-        else k_interp64<0, 256><<<ntiles, 256, 0, st>>>(boxes, tiles);
+        if (ilin == 1) k_interp64<1, 256, false><<<ntiles, 256, 0, st>>>(boxes, tiles);
+        else if (tex) k_interp64<0, 256, true><<<ntiles, 256, 0, st>>>(boxes, tiles);
+        else k_interp64<0, 256, false><<<ntiles, 256, 0, st>>>(boxes, tiles);
         k_be64<256><<<ntiles, 256, 0, st>>>(boxes, tiles, P, in);
     } else {
-        if (ilin == 1) k_interp64<1, 128><<<ntiles, 128, 0, st>>>(boxes, tiles);
-        else k_interp64<0, 128><<<ntiles, 128, 0, st>>>(boxes, tiles);
+        if (ilin == 1) k_interp64<1, 128, false><<<ntiles, 128, 0, st>>>(boxes, tiles);
+        else if (tex) k_interp64<0, 128, true><<<ntiles, 128, 0, st>>>(boxes, tiles);
+        else k_interp64<0, 128, false><<<ntiles, 128, 0, st>>>(boxes, tiles);
         k_be64<128><<<ntiles, 128, 0, st>>>(boxes, tiles, P, in);
     }
     k_be_defer64<<<dim3(kDeferBlocks, nbox), kUpdateThreads, 0, st>>>(boxes, P, in);

@@ -36,7 +36,7 @@ struct StepIn {
 
 // FP64, reference operation order (ntlp_fp64.cu)
 void launch_update_be64(int ilin, int nt, DevBox *boxes, const Tile *tiles, int ntiles, int nbox,
-                        const DevParams &P, StepIn in, cudaStream_t st);
+                        const DevParams &P, StepIn in, cudaStream_t st, bool tex);
 void launch_update_rk3_64(int ilin, DevBox *boxes, const Tile *tiles, int ntiles, const DevParams &P,
                           StepIn in, cudaStream_t st);
 void launch_payload64(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams &P, double dt,
