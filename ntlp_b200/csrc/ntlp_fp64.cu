@@ -106,7 +106,7 @@ __device__ __forceinline__ double ld64(const double *f, unsigned long long tex, 
     return __ldg(f + a);
 }
 
-// TEX: the first two x columns of the stencil through the texture path (its
+// TEX: the first three x columns of the stencil through the texture path (its
 // own L1 data pipe)
 template <bool TEX>
 __device__ void interp6_64(const DevBox &B, double x1, double x2, double x3, Interp &o, int &bad) {
@@ -200,7 +200,7 @@ __device__ void interp6_64(const DevBox &B, double x1, double x2, double x3, Int
                 const double wi = wx[i];
                 const long long a = bu + xo[i], aw = bw + xo[i];
                 double vu, vv, vw, vT, vq;
-                if (TEX && i < 2) {
+                if (TEX && i < 3) {
                     vu = ld64<true>(fu, B.tex_f64[0], a);
                     vv = ld64<true>(fv, B.tex_f64[1], a);
                     vw = ld64<true>(fw, B.tex_f64[2], aw);
