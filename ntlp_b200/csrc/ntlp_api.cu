@@ -26,6 +26,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -35,6 +36,23 @@
 #include "ntlp_math.h"
 
 using namespace ntlp;
+
+namespace ntlp {
+
+bool first_on_device(int which) {
+    constexpr int kMaxDevices = 64;
+    static std::mutex mu;
+    static bool seen[kMaxDevices][kOnceKinds] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices || which < 0 || which >= kOnceKinds)
+        return true;   // out of the table's range: set up every time (idempotent)
+    std::lock_guard<std::mutex> lock(mu);
+    if (seen[dev][which]) return false;
+    seen[dev][which] = true;
+    return true;
+}
+
+}  // namespace ntlp
 
 namespace {
 

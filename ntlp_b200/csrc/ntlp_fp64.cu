@@ -477,12 +477,10 @@ static void dep64_attr() {
 }
 
 void prepare_kernels64() {
-    static bool done = false;
-    if (done) return;
+    if (!first_on_device(ONCE_DEP64)) return;
     dep64_attr<0>();
     dep64_attr<1>();
     dep64_attr<2>();
-    done = true;
 }
 
 void launch_deposit64(int variant, DevBox *boxes, const Tile *tiles, int ntiles, const DevParams &P,

@@ -58,10 +58,15 @@ void launch_deposit_mixed(int variant, DevBox *boxes, const Tile *tiles, int nti
 constexpr int kDenseRatio = 16;     // mixed boxes with capacity >= 16 x cells use per-cell sums
 constexpr int kDenseBlocks = 1184;  // grid.x of the cell-sum kernels
 constexpr int kFoldBlocks = 148;    // grid.x of the periodic fold (mixed)
-// one-time kernel attributes (dynamic shared memory of the deposition);
-// call outside stream capture
+// kernel attributes (dynamic shared memory of the deposition), set once per
+// device, on the device that is current; call outside stream capture
 void prepare_kernels64();
 void prepare_kernels_mixed();
+// true exactly once per (current device, which): guards per-device set-up
+// (thread-safe); which < kOnceKinds
+constexpr int kOnceKinds = 4;
+enum { ONCE_DEP64 = 0, ONCE_DEP_MIXED = 1, ONCE_INTERP_BLOCK = 2 };
+bool first_on_device(int which);
 
 // sort and bookkeeping (ntlp_sort.cu)
 struct SortPlan {

@@ -314,12 +314,10 @@ static void depm_attr() {
 }
 
 void prepare_kernels_mixed() {
-    static bool done = false;
-    if (done) return;
+    if (!first_on_device(ONCE_DEP_MIXED)) return;
     depm_attr<0>();
     depm_attr<1>();
     depm_attr<2>();
-    done = true;
 }
 
 void launch_deposit_mixed(int variant, DevBox *boxes, const Tile *tiles, int ntiles, const DevParams &P,

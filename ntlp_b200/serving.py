@@ -334,6 +334,9 @@ class CudaEngine:
 
     def prepare(self, job: JobSpec):
         torch = self.torch
+        # runs on an ingest thread: the contexts are created on the current
+        # device, which is per thread
+        torch.cuda.set_device(self.device)
         box = self._payload.pop(job.jid, None)
         if box is None:
             ist = self._ingest_stream()
