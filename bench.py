@@ -58,8 +58,7 @@ sys.path.insert(0, ROOT)
 B_D = {"fp64": 248, "mixed": 224}       # algorithmic bytes per droplet
 # DRAM bytes per droplet of the update phase (interpolation + droplet body)
 # measured by ncu at 1M droplets / 128^3 (fields subtracted), used to scale
-# the measured traffic to the bench workload; see
-# profiles/k_interp_be_deposit_mixed_1M_droplets_128cube.md
+# the measured traffic to the bench workload
 NCU_BYTES_PER_DROPLET = {"mixed": 440.0}
 METRIC = "droplet-updates/s (mixed vs FP64 GPU) at 16M; p50/p99 serving step latency"
 
@@ -91,6 +90,10 @@ def parse():
     ap.add_argument("--serve-max-large", type=int, default=1)
     ap.add_argument("--serve-max-active", type=int, default=4)
     ap.add_argument("--serve-ingest-priority", choices=["job", "high"], default="high")
+    ap.add_argument("--skip-errors", action="store_true", help="no error tables (configs[0], [1] and [2])")
+    ap.add_argument("--skip-c2", action="store_true", help="no configs[2] section")
+    ap.add_argument("--err-sample", type=int, default=200_000)
+    ap.add_argument("--c2-n", type=int, default=None, help="droplets of the configs[2] section (default: its 67M)")
     ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
                     help="run one precision only (profiling)")
     return ap.parse_args()
@@ -204,8 +207,9 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def run_device(case, precision: str, args, dist, rank):
-    """Device-timed steps; returns dict with throughput and per-phase times."""
+def run_device(case, precision: str, args, dist, rank, keep: bool = False):
+    """Device-timed steps; returns dict with throughput and per-phase times
+    (and, with keep, the context itself for the error comparison)."""
     import torch
     import ntlp_b200
     from ntlp_b200 import abi
@@ -250,53 +254,350 @@ def run_device(case, precision: str, args, dist, rank):
     prof = s.profile_read()
     n1 = s.numpart
     ms_max = max_over_ranks(dist, ms)
-    s.close()
-    return dict(ms=ms_max, n0=n0, n1=n1, prof=prof, clocks=clocks, tune=tune)
+    s.profile(False)
+    out = dict(ms=ms_max, n0=n0, n1=n1, prof=prof, clocks=clocks, tune=tune, it=it)
+    if keep:
+        out["ctx"] = s
+    else:
+        s.close()
+    return out
+
+
+# ---- errors against the FP64 path and the oracle -------------------------
+
+ERR_KEYS = ("radius", "Tp", "Tf", "qinf", "qstar", "vp", "uf", "xp")
+SRC_NAMES = ("partsrc_x", "partsrc_y", "partsrc_z", "partTsrc", "partHsrc", "partTEsrc")
+
+
+def device_state(s, dt):
+    """A context's droplets (list order) and the sources of its deposition
+    at dt, as device tensors."""
+    import torch
+    d = s.get_droplets_device(("xp", "vp", "uf", "Tp", "Tf", "radius", "qinf", "qstar", "lid"))
+    g = s.grid
+    shape = (g["nnx"], g["nny"], g["nnz"] + 2)
+    dev = d["radius"].device
+    mom = torch.empty((3,) + shape, dtype=torch.float64, device=dev)
+    rest = [torch.empty(shape, dtype=torch.float64, device=dev) for _ in range(3)]
+    src = s.particle_coupling_update(dt, out=[mom] + rest)
+    s.sync()
+    return d, src
+
+
+def host_state(d: dict, src: list, device):
+    """Oracle results (numpy) as device tensors, for compare()."""
+    import torch
+    keys = ERR_KEYS + ("lid",)
+    return ({k: torch.from_numpy(np.ascontiguousarray(d[k])).to(device) for k in keys},
+            [torch.from_numpy(np.ascontiguousarray(a)).to(device) for a in src])
+
+
+def compare(a: dict, asrc: list, b: dict, bsrc: list, grid: dict) -> dict:
+    """Max and RMS error of state a against reference b, droplets matched by
+    list id: relative for radius, Tp, Tf, qinf, qstar; as a fraction of the
+    reference's largest |value| for vp and uf; of the longest domain edge
+    for xp.  Sources per array: the largest |difference| over the largest
+    |reference value|, and the RMS difference over the reference's RMS."""
+    import torch
+    la, lb = a["lid"].long(), b["lid"].long()
+    same = la.shape == lb.shape and bool(torch.equal(la, lb))
+    if same:
+        ia = ib = None
+        ncmp = int(la.numel())
+    else:
+        m = int(max(int(la.max()), int(lb.max()))) + 1 if la.numel() and lb.numel() else 1
+        pa = torch.full((m,), -1, dtype=torch.int64, device=la.device)
+        pb = torch.full((m,), -1, dtype=torch.int64, device=la.device)
+        pa[la] = torch.arange(la.numel(), device=la.device)
+        pb[lb] = torch.arange(lb.numel(), device=la.device)
+        both = (pa >= 0) & (pb >= 0)
+        ia, ib = pa[both], pb[both]
+        ncmp = int(ia.numel())
+    out = {"droplets": [int(la.numel()), int(lb.numel())], "compared": ncmp, "same_list": same}
+    span = max(grid["xl"], grid["yl"], grid["zl"])
+    bitexact = True
+    for k in ERR_KEYS:
+        x, y = a[k], b[k]
+        if ia is not None:
+            x, y = x[..., ia], y[..., ib]
+        if x.numel() == 0:
+            out[k] = {"max": 0.0, "rms": 0.0}
+            continue
+        d = (x - y).abs()
+        bitexact = bitexact and bool(torch.equal(x, y))
+        if k in ("vp", "uf"):
+            e = d / y.abs().max().clamp_min(1e-300)
+        elif k == "xp":
+            e = d / span
+        else:
+            e = d / y.abs().clamp_min(1e-300)
+        out[k] = {"max": float(e.max()), "rms": float(e.pow(2).mean().sqrt())}
+    src = {}
+    for q in range(6):
+        x, y = asrc[q].reshape(-1), bsrc[q].reshape(-1)
+        d = x - y
+        bitexact = bitexact and bool(torch.equal(x, y))
+        mx = float(y.abs().max())
+        rms = float(y.pow(2).mean().sqrt())
+        src[SRC_NAMES[q]] = {"max": float(d.abs().max()) / max(mx, 1e-300),
+                             "rms": float(d.pow(2).mean().sqrt()) / max(rms, 1e-300)}
+    out["sources"] = src
+    out["bitexact"] = bitexact
+    return out
+
+
+def _sample(d: dict, n: int) -> dict:
+    return {k: (np.ascontiguousarray(v[..., :n]) if isinstance(v, np.ndarray) and v.ndim == 2 else
+                (np.ascontiguousarray(v[:n]) if isinstance(v, np.ndarray) else v))
+            for k, v in d.items()}
+
+
+def oracle_run(case_grid, params, ext, droplets, dt, steps, with_sources_each_step=False):
+    """The oracle over `steps` BE steps (OpenMP update, serial list-order
+    deposition at the end, or every step when asked); returns the final
+    droplets, the last sources and the seconds of each part."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    L = pyoracle.lib("ntlp")
+    threads = int(L.oracle_max_threads())
+    o = pyoracle.Oracle(case_grid, params, ext)
+    d = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in droplets.items()}
+    t_upd = t_dep = 0.0
+    src = None
+    for it in range(1, steps + 1):
+        t0 = time.perf_counter()
+        o.step_be_omp(d, dt, it, threads, with_sources=False)
+        t_upd += time.perf_counter() - t0
+        if with_sources_each_step or it == steps:
+            t0 = time.perf_counter()
+            src, _ = o.coupling(d, dt)
+            t_dep += time.perf_counter() - t0
+    return d, src, dict(update_s=t_upd, deposit_s=t_dep, threads=threads)
+
+
+def gpu_run(grid, params, precision, droplets, dt, steps, ext=None, flow=None):
+    """A fresh context over `steps` BE steps from it = 1 (untimed); returns
+    the context."""
+    import ntlp_b200
+    from ntlp_b200 import abi
+    p = dict(params, precision=abi.NTLP_PREC_MIXED if precision == "mixed" else abi.NTLP_PREC_FP64)
+    n = droplets["radius"].shape[0]
+    s = ntlp_b200.DropletStep(grid, p, capacity=max(n, 1))
+    if flow is not None:
+        s.fill_ext(flow)
+    else:
+        s.set_fields_ext(ext)
+    s.set_droplets(droplets)
+    for it in range(1, steps + 1):
+        s.particle_update_BE(dt, it, counters=False)
+    return s
+
+
+def run_errors_c1(case, ctx_mixed, ctx_fp64, args):
+    """the mixed path against the FP64 path over all droplets
+    (the two timed contexts, after the same steps), and both against the
+    oracle on a sample of the same droplets and fields run from it = 1."""
+    import torch
+    dev = torch.device("cuda", torch.cuda.current_device())
+    t0 = time.perf_counter()
+    a, asrc = device_state(ctx_mixed, case.dt)
+    b, bsrc = device_state(ctx_fp64, case.dt)
+    out = {"mixed_vs_fp64_all": compare(a, asrc, b, bsrc, case.grid)}
+    out["mixed_vs_fp64_all"]["steps"] = int(ctx_steps(args))
+    del a, asrc, b, bsrc
+    n = min(args.err_sample, case.droplets["radius"].shape[0])
+    smp = _sample(case.droplets, n)
+    steps = case.steps
+    od, osrc, ot = oracle_run(case.grid, case.params, case.ext_cache, smp, case.dt, steps)
+    ref = host_state(od, osrc, dev)
+    for prec in ("fp64", "mixed"):
+        s = gpu_run(case.grid, case.params, prec, smp, case.dt, steps, ext=case.ext_cache)
+        g, gsrc = device_state(s, case.dt)
+        s.close()
+        out[f"{prec}_vs_oracle_sample"] = dict(compare(g, gsrc, *ref, case.grid), sample=n, steps=steps)
+    out["oracle_sample_seconds"] = ot
+    out["seconds"] = time.perf_counter() - t0
+    return out
+
+
+def ctx_steps(args) -> int:
+    """Steps a timed context has taken when the timing ends."""
+    return args.warmup + (5 * (args.tune_steps + 1) if args.tune_steps > 0 else 0) + args.steps
+
+
+def run_c0(args):
+    """configs[0] in full (1,000,000 droplets, 128^3, dt = 1e-3 s, 10
+    steps): the FP64 and mixed GPU paths against the oracle, which is also
+    timed here on the host cores, update and deposition every step (the
+    designated CPU configuration)."""
+    import torch
+    from ntlp_b200 import generator as gen
+    dev = torch.device("cuda", torch.cuda.current_device())
+    t0 = time.perf_counter()
+    case = gen.make_case("c0", params=gen.default_params(ilin=args.ilin))
+    ext = case.ext()
+    n = case.droplets["radius"].shape[0]
+    od, osrc, ot = oracle_run(case.grid, case.params, ext, case.droplets, case.dt, case.steps,
+                              with_sources_each_step=True)
+    ref = host_state(od, osrc, dev)
+    out = {"workload": f"{n} droplets, 128x128x128, dt={case.dt}, {case.steps} steps, ilin={args.ilin}"}
+    for prec in ("fp64", "mixed"):
+        s = gpu_run(case.grid, case.params, prec, case.droplets, case.dt, case.steps, ext=ext)
+        g, gsrc = device_state(s, case.dt)
+        s.close()
+        out[f"{prec}_vs_oracle"] = compare(g, gsrc, *ref, case.grid)
+    cpu_s = ot["update_s"] + ot["deposit_s"]
+    out["cpu"] = {"value": n * case.steps / cpu_s, "unit": "droplet-updates/s", "cores": ot["threads"],
+                  "mpi_ranks": 0, "kind": "port",
+                  "sample": (f"configs[0] in full: {case.steps} steps of {n} droplets, BE update on "
+                             f"{ot['threads']} OpenMP threads {ot['update_s']:.2f} s, serial list-order "
+                             f"deposition {ot['deposit_s']:.2f} s")}
+    out["seconds"] = time.perf_counter() - t0
+    return out
+
+
+def run_c2(args, dist):
+    """configs[2], the spray-like case in full: 67,108,864 droplets (bimodal
+    3/40 um, bottom 20%) on the stretched 512x512x128 grid, generated in
+    device memory; 3 warm-up and 10 timed steps of the mixed path
+    (update + coupling), the FP64 path over the same steps, and the mixed
+    path's errors against it."""
+    import torch
+    import ntlp_b200
+    from ntlp_b200 import abi, devgen
+    from ntlp_b200 import generator as gen
+    dev = torch.device("cuda", torch.cuda.current_device())
+    cfg = gen.CONFIGS["c2"]
+    params = gen.default_params(ilin=args.ilin)
+    t_all = time.perf_counter()
+    box = devgen.make_config_box("c2", params, dev, n=args.c2_n)
+    grid = box["grid"]
+    n = box["droplets"]["radius"].shape[0]
+    dt, steps, warm = cfg["dt"], cfg["steps"], 3
+    res = {}
+    ctxs = {}
+    for prec in ("mixed", "fp64"):
+        p = dict(params, precision=abi.NTLP_PREC_MIXED if prec == "mixed" else abi.NTLP_PREC_FP64)
+        s = ntlp_b200.DropletStep(grid, p, capacity=n)
+        s.fill_ext(box["flow"])
+        s.set_droplets(box["droplets"])
+        stream = torch.cuda.ExternalStream(s.stream_handle)
+        it = 1
+        for _ in range(warm):
+            s.particle_update_BE(dt, it, counters=False)
+            s.particle_coupling_update(dt, download=False)
+            it += 1
+        s.sync()
+        n0 = s.numpart
+        s.profile(True)
+        s.profile_read()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        clk = ClockSampler() if prec == "mixed" else None
+        if clk:
+            clk.start()
+        e0.record(stream)
+        for _ in range(steps):
+            s.particle_update_BE(dt, it, counters=False)
+            s.particle_coupling_update(dt, download=False)
+            it += 1
+        e1.record(stream)
+        e1.synchronize()
+        clocks = clk.stop() if clk else None
+        ms = e0.elapsed_time(e1)
+        prof = s.profile_read()
+        s.profile(False)
+        n1 = s.numpart
+        res[prec] = {"value": 0.5 * (n0 + n1) * steps / (ms * 1e-3), "unit": "droplet-updates/s",
+                     "ms_per_step": ms / steps,
+                     "phases_ms_per_step": {k: v / steps for k, v in prof.items() if k.endswith("_ms")},
+                     "numpart": [int(n0), int(n1)], "device_bytes": s.device_bytes}
+        if clocks:
+            res[prec]["clocks"] = clocks
+        ctxs[prec] = s
+    del box
+    torch.cuda.empty_cache()
+    hbm, src = peaks()
+    npad = (grid["nnx"] + 5) * (grid["nny"] + 5) * (grid["nnz"] + 2)
+    alg = n * B_D["mixed"] + npad * 5 * 4
+    upd = res["mixed"]["phases_ms_per_step"]["update_ms"]
+    res["mixed"]["update_hbm_frac"] = alg / (upd * 1e-3) / 1e9 / hbm
+    a, asrc = device_state(ctxs["mixed"], dt)
+    b, bsrc = device_state(ctxs["fp64"], dt)
+    res["mixed_vs_fp64_all"] = dict(compare(a, asrc, b, bsrc, grid), steps=warm + steps)
+    for s in ctxs.values():
+        s.close()
+    res["mixed_over_fp64"] = res["mixed"]["value"] / res["fp64"]["value"]
+    res["workload"] = (f"configs[2]: {n} droplets (bimodal 3/40 um, bottom 20%), 512x512x128 stretched 1.02, "
+                       f"log-law wind, dt={dt}, {warm} warm-up + {steps} timed steps, ilin={args.ilin}, "
+                       "inputs generated in device memory")
+    res["seconds"] = time.perf_counter() - t_all
+    return res
 
 
 def run_e2e(case, args, dist):
-    """Through the C ABI with host buffers: fields up, step, sources down."""
+    """Through the C ABI with host buffers, every step: the five fields go
+    up in the flow layout from pinned host memory and the six source arrays
+    come down into pinned host memory.  The copies run on the context's two
+    copy streams (ntlp_fields_upload_async, ntlp_coupling_async), so the
+    upload of step k+1's fields and the download of step k's sources overlap
+    the device's work; every copy is inside the timed region, which ends
+    when all of them have completed.  The serial form (upload, step,
+    download, one after the other on one stream) is timed too."""
     import torch
     import ntlp_b200
     from ntlp_b200 import abi
     p = dict(case.params, precision=abi.NTLP_PREC_MIXED)
     n = case.droplets["radius"].shape[0]
-    s = ntlp_b200.DropletStep(case.grid, p, capacity=n)
-    pinned = {}
-    for k, v in case.ext_cache.items():
-        t = torch.empty(v.shape, dtype=torch.float64, pin_memory=True)
-        t.numpy()[...] = v
-        pinned[k] = t.numpy()
     g = case.grid
     shape = (g["nnx"], g["nny"], g["nnz"] + 2)
-    mom = torch.empty((3,) + shape, dtype=torch.float64, pin_memory=True).numpy()
-    rest = [torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy() for _ in range(3)]
-    s.set_droplets(case.droplets)
-    it = 1
-    for _ in range(max(1, args.warmup)):
-        s.set_fields_ext(pinned)
-        s.particle_update_BE(case.dt, it, counters=False)
-        s.particle_coupling_update(case.dt, out=[mom] + rest)
-        it += 1
-    if args.tune_steps > 0:
-        s.autotune(case.dt, it, steps=args.tune_steps)
-        it += 5 * (args.tune_steps + 1)
-    n0 = s.numpart
-    barrier(dist)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        s.set_fields_ext(pinned)
-        s.particle_update_BE(case.dt, it, counters=False)
-        s.particle_coupling_update(case.dt, out=[mom] + rest)
-        it += 1
-    s.sync()
-    dt = time.perf_counter() - t0
-    dt = max_over_ranks(dist, dt)
-    n1 = s.numpart
-    s.close()
-    npad = (g["nnx"] + 5) * (g["nny"] + 5) * (g["nnz"] + 2)
+    flow = case.flow()
+    pflow = {}
+    for k, v in flow.items():
+        t = torch.empty(v.shape, dtype=torch.float64, pin_memory=True)
+        t.numpy()[...] = v
+        pflow[k] = t.numpy()
+    del flow
+    outs = [[torch.empty((3,) + shape, dtype=torch.float64, pin_memory=True).numpy()] +
+            [torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy() for _ in range(3)] for _ in range(2)]
+    nflow = g["nnx"] * g["nny"] * (g["nnz"] + 2)
     nsrc = g["nnx"] * g["nny"] * (g["nnz"] + 2)
-    return dict(seconds=dt, n0=n0, n1=n1, h2d=5 * npad * 8, d2h=6 * nsrc * 8)
+    res = {}
+    for mode in ("overlapped", "serial"):
+        s = ntlp_b200.DropletStep(g, p, capacity=n)
+        s.set_droplets(case.droplets)
+
+        def step(k, it):
+            if mode == "overlapped":
+                s.fill_ext_async(pflow)
+                s.particle_update_BE(case.dt, it, counters=False)
+                s.particle_coupling_update_async(case.dt, outs[k % 2])
+            else:
+                s.fill_ext(pflow)
+                s.particle_update_BE(case.dt, it, counters=False)
+                s.particle_coupling_update(case.dt, out=outs[k % 2])
+
+        it = 1
+        for k in range(max(1, args.warmup)):
+            step(k, it)
+            it += 1
+        if args.tune_steps > 0:
+            s.sync()
+            s.autotune(case.dt, it, steps=args.tune_steps)
+            it += 5 * (args.tune_steps + 1)
+        s.sync()
+        n0 = s.numpart
+        barrier(dist)
+        t0 = time.perf_counter()
+        for k in range(args.steps):
+            step(k, it)
+            it += 1
+        s.sync()
+        sec = max_over_ranks(dist, time.perf_counter() - t0)
+        n1 = s.numpart
+        s.close()
+        res[mode] = dict(seconds=sec, n0=n0, n1=n1)
+    return dict(res["overlapped"], serial=res["serial"], h2d=5 * nflow * 8, d2h=6 * nsrc * 8)
 
 
 def run_batch(args, precision: str):
@@ -435,7 +736,7 @@ def cpu_baseline(case, seconds: float, dist=None):
     o.coupling(d, case.dt)
     t_dep = time.perf_counter() - t0 - t_grid
     t_full = (t_upd + max(t_dep, 0.0)) * (N / n) + t_grid
-    return dict(value=N / t_full, unit="droplet-updates/s", cores=threads, kind="port",
+    return dict(value=N / t_full, unit="droplet-updates/s", cores=threads, mpi_ranks=0, kind="port",
                 sample=(f"{n} of {N} droplets of the same workload: BE update on {threads} OpenMP threads "
                         f"{t_upd:.2f} s, serial list-order deposition {max(t_dep, 0):.2f} s, both scaled by N/n; "
                         f"grid-sized deposition work {t_grid:.2f} s measured at full size"),
@@ -492,10 +793,17 @@ def main():
     nsrc = g["nnx"] * g["nny"] * (g["nnz"] + 2)
 
     res = {}
+    errors_on = ws == 1 and not args.skip_errors and args.only is None and not args.skip_fp64
     for prec in (["mixed", "fp64"] if args.only is None else [args.only]):
         if prec == "fp64" and args.skip_fp64:
             continue
-        res[prec] = run_device(case, prec, args, dist, rank)
+        res[prec] = run_device(case, prec, args, dist, rank, keep=errors_on)
+    errors = {}
+    if errors_on:
+        errors["c1"] = run_errors_c1(case, res["mixed"]["ctx"], res["fp64"]["ctx"], args)
+    for r_ in res.values():
+        if "ctx" in r_:
+            r_.pop("ctx").close()
     e2e = None if args.skip_e2e else run_e2e(case, args, dist)
     batch, serve = {}, None
     if ws == 1 and not args.skip_batch:
@@ -503,9 +811,18 @@ def main():
             batch[prec] = run_batch(args, prec)
     if ws == 1 and not args.skip_serving:
         serve = run_serving(args)
+    c0 = c2 = None
+    if errors_on:
+        c0 = run_c0(args)
+        errors["c0"] = {k: v for k, v in c0.items() if k.endswith("_vs_oracle") or k == "workload"}
+    if ws == 1 and not args.skip_c2:
+        c2 = run_c2(args, dist)
+        errors["c2"] = dict(c2["mixed_vs_fp64_all"], workload=c2["workload"])
     cb = None
     if rank == 0 and ws == 1 and not args.skip_cpu:
         cb = cpu_baseline(case, args.cpu_seconds)
+        if c0 is not None:
+            cb["configs0"] = c0["cpu"]
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
@@ -555,11 +872,21 @@ def main():
         line["mixed_over_fp64"] = value / fv
     if e2e:
         ev = 0.5 * (e2e["n0"] + e2e["n1"]) * args.steps / e2e["seconds"] * ws
+        se = e2e["serial"]
         line["e2e"] = {"value": ev, "unit": "droplet-updates/s", "h2d_bytes_per_step": e2e["h2d"],
-                       "d2h_bytes_per_step": e2e["d2h"],
-                       "note": "fields uploaded from pinned host memory and sources downloaded every step"}
+                       "d2h_bytes_per_step": e2e["d2h"], "ms_per_step": e2e["seconds"] / args.steps * 1e3,
+                       "note": ("through the C ABI: each step uploads the five fields (flow layout) from pinned "
+                                "host memory and downloads the six source arrays into pinned host memory, on "
+                                "the context's copy streams, overlapping the device's work"),
+                       "serial": {"value": 0.5 * (se["n0"] + se["n1"]) * args.steps / se["seconds"] * ws,
+                                  "ms_per_step": se["seconds"] / args.steps * 1e3,
+                                  "note": "the same copies, upload-step-download in sequence on one stream"}}
     if cb:
         line["cpu_baseline"] = cb
+    if errors:
+        line["errors"] = errors
+    if c2:
+        line["c2"] = {k: v for k, v in c2.items() if k != "mixed_vs_fp64_all"}
     if batch:
         line["batch"] = batch
         if "fp64" in batch:

@@ -155,6 +155,28 @@ int ntlp_step_rk3(ntlp_ctx *ctx, int32_t istage, double dt, int32_t it,
  * the reference's list order, so FP64 results are bit-reproducible.        */
 int ntlp_coupling(ntlp_ctx *ctx, double dt, int32_t layout, double *partsrc,
                   double *partTsrc, double *partHsrc, double *partTEsrc);
+/* ---- overlapped host copies ----------------------------------------------
+ * No counterpart in the reference (its fields and sources live in host
+ * memory).  The two calls below return once their copies are queued on the
+ * context's own copy streams (one per direction), so the host-to-device
+ * copy of the next step's fields and the device-to-host copy of the last
+ * step's sources run while the device computes.  With pinned host memory the
+ * copies are asynchronous; the host arrays must not be changed (upload) or
+ * read (download) before ntlp_copies_wait or ntlp_sync returns.
+ *
+ * ntlp_fields_upload_async: the five fields of box 0 in the flow layout of
+ * ntlp_fields_upload, copied to a device area; the next step (on the
+ * context's stream) waits for the copies, then fills the halo and the FP32
+ * copies from that area.  A later upload, synchronous or not, replaces it.
+ * ntlp_coupling_async: ntlp_coupling in the column layout, its six arrays
+ * copied back on the download stream after the deposition; the next
+ * deposition waits until that copy has read the device arrays.            */
+int ntlp_fields_upload_async(ntlp_ctx *ctx, const double *u, const double *v, const double *w,
+                             const double *t, const double *q);
+int ntlp_coupling_async(ntlp_ctx *ctx, double dt, double *partsrc, double *partTsrc, double *partHsrc,
+                        double *partTEsrc);
+/* Wait for both copy streams (ntlp_sync waits for them too).              */
+int ntlp_copies_wait(ntlp_ctx *ctx);
 /* Vertical droplet flux tallies of the last BE step, pflux(0:nnz),
  * pmassflux(0:nnz), penegflux(0:nnz) (particles.f90:3209-3238).           */
 int ntlp_flux(ntlp_ctx *ctx, double *pflux, double *pmassflux, double *penegflux);
@@ -168,6 +190,14 @@ void *ntlp_stream(ntlp_ctx *ctx);
  * context's own stream.  Waits for the current stream first.  The caller
  * keeps the stream alive until the context is destroyed or switched back. */
 int ntlp_use_stream(ntlp_ctx *ctx, void *stream);
+/* Mixed precision, 6th order: the interpolation stages each block of cells'
+ * field window in shared memory (TMA tile loads) and contracts every
+ * droplet's stencil from there.  enable = 0 switches to the per-droplet
+ * kernel (stencil from global memory; the same results, bit for bit), 1
+ * back to the staged one, -1 only queries.  Returns the block height in
+ * cells (0: per-droplet kernel) or an error code (< 0).  No counterpart in
+ * the reference.                                                          */
+int ntlp_interp_staging(ntlp_ctx *ctx, int32_t enable);
 
 /* ---- instrumentation (phase timers; measurement.f90's named phases) ----- */
 /* When enabled, every step records CUDA events around its kernels on the

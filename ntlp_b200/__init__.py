@@ -62,6 +62,10 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.ntlp_stream.argtypes = [C.c_void_p]
     L.ntlp_stream.restype = C.c_void_p
     L.ntlp_use_stream.argtypes = [C.c_void_p, C.c_void_p]
+    L.ntlp_interp_staging.argtypes = [C.c_void_p, C.c_int32]
+    L.ntlp_fields_upload_async.argtypes = [C.c_void_p] + [dp] * 5
+    L.ntlp_coupling_async.argtypes = [C.c_void_p, C.c_double, dp, dp, dp, dp]
+    L.ntlp_copies_wait.argtypes = [C.c_void_p]
     L.ntlp_stats.argtypes = [C.c_void_p, C.c_int32, P(abi.NtlpStats0), C.c_int32, dp, dp]
     L.ntlp_sub_create.argtypes = [P(abi.NtlpGrid), P(abi.NtlpSubdomain), P(abi.NtlpParams), C.c_int64,
                                   P(C.c_void_p)]
@@ -220,6 +224,15 @@ class DropletStep:
         """Issue this context's work on an external cudaStream_t (None: its own)."""
         self._check(self.L.ntlp_use_stream(self.h, C.c_void_p(stream_handle or None)), "ntlp_use_stream")
 
+    def interp_staging(self, enable: int = -1) -> int:
+        """Mixed 6th-order interpolation over staged cell blocks (1) or per
+        droplet from global memory (0); -1 queries.  Returns the block
+        height in cells (0: per droplet)."""
+        r = int(self.L.ntlp_interp_staging(self.h, int(enable)))
+        if r < 0:
+            self._check(r, "ntlp_interp_staging")
+        return r
+
     def profile(self, enable: bool = True):
         self._check(self.L.ntlp_profile_enable(self.h, 1 if enable else 0), "ntlp_profile_enable")
 
@@ -244,6 +257,28 @@ class DropletStep:
         self._check(self.L.ntlp_fields_upload(self.h, *(abi.as_dptr(a) for a in arrs)), "ntlp_fields_upload")
         self.sync()
 
+    def fill_ext_async(self, flow: dict):
+        """Flow-layout fields, copied on the context's upload stream while
+        the device computes; the next step fills the halo from them.  The
+        arrays (pinned host memory for an asynchronous copy) must stay
+        unchanged until copies_wait() or sync()."""
+        arrs = [_field(flow[k]) for k in ("u", "v", "w", "T", "q")]
+        self._async_keep = arrs
+        self._check(self.L.ntlp_fields_upload_async(self.h, *(abi.as_dptr(a) for a in arrs)),
+                    "ntlp_fields_upload_async")
+
+    def particle_coupling_update_async(self, dt: float, out: list):
+        """The deposition, its six column-layout source arrays copied into
+        `out` ([partsrc (3, nnx, nny, nnz+2), partTsrc, partHsrc,
+        partTEsrc]) on the download stream; valid after copies_wait() or
+        sync()."""
+        mom, rest = out[0], out[1:]
+        self._check(self.L.ntlp_coupling_async(self.h, float(dt), abi.as_dptr(mom.reshape(-1)),
+                                               *(abi.as_dptr(a.reshape(-1)) for a in rest)), "ntlp_coupling_async")
+
+    def copies_wait(self):
+        self._check(self.L.ntlp_copies_wait(self.h), "ntlp_copies_wait")
+
     # -- droplets --
     def set_droplets(self, d: dict):
         s = abi.make_droplets_struct(d)
@@ -259,6 +294,27 @@ class DropletStep:
         for k, v in d.items():
             out[k] = np.ascontiguousarray(v[..., :n] if v.ndim == 2 else v[:n])
         return out
+
+    def get_droplets_device(self, keys=("xp", "vp", "uf", "Tp", "Tf", "radius", "qinf", "qstar", "lid")) -> dict:
+        """The named fields of the droplets, in list order, as tensors on the
+        context's device (no host copy; for comparisons at full size)."""
+        import torch
+        n = self.numpart
+        dev = torch.device("cuda", torch.cuda.current_device())
+        d = {}
+        for k in keys:
+            if k in abi.VEC3_FIELDS:
+                d[k] = torch.empty((3, max(n, 1)), dtype=torch.float64, device=dev)
+            elif k == "mult":
+                d[k] = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
+            elif k == "lid":
+                d[k] = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
+            else:
+                d[k] = torch.empty(max(n, 1), dtype=torch.float64, device=dev)
+        s = abi.make_droplets_struct(d, n=n)
+        self._check(self.L.ntlp_droplets_download(self.h, C.byref(s)), "ntlp_droplets_download")
+        n = int(s.n)
+        return {k: (v[..., :n] if v.dim() == 2 else v[:n]) for k, v in d.items()}
 
     # -- the step --
     def particle_update_BE(self, dt: float, it: int, counters: bool = True) -> dict:

@@ -17,6 +17,7 @@
 // device's stream-ordered memory pool (cudaMallocAsync), which keeps freed
 // blocks for reuse, so creating and destroying contexts (the serving loop
 // does so per job) does not go back to the driver each time.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -105,11 +106,26 @@ struct ntlp_ctx {
     SortPlan plan{};
     int dep_variant = 0, nt_variant = 0;
     long long *counters_h = nullptr;   // pinned [nbox][kNumCounters]
+    int *err_h = nullptr;              // pinned [nbox] device error words
+    // overlapped host copies (ntlp_fields_upload_async, ntlp_coupling_async):
+    // a copy stream each way, the flow-layout fields of box 0 staged in
+    // up_area until the next step fills the halo from them
+    cudaStream_t up_stream = nullptr, down_stream = nullptr;
+    cudaEvent_t ev_up = nullptr, ev_fill = nullptr, ev_dep = nullptr, ev_down = nullptr;
+    double *up_area = nullptr;
+    bool up_pending = false, fill_recorded = false, down_pending = false;
     // CUDA graph of nsteps (update + sort + finish + deposit)
     cudaGraphExec_t gexec = nullptr;
     double g_dt = 0.0;
     int g_nsteps = 0, g_dep = -1, g_nt = -1;
+    bool g_blk = false;
     bool tex_all = true;   // every box's FP32 fields have a texture (mixed)
+    // staged cell-block interpolation (mixed, 6th order): block height and
+    // tiles; blk_kb = 0 when the tensor maps could not be made
+    int blk_kb = 0;
+    bool blk_on = true;
+    Tile *blk_tiles_d = nullptr;
+    int n_blk_tiles = 0;
     bool tex_all64 = true;   // every box's FP64 fields have textures (FP64)
     bool any_dense = false;   // some box deposits through per-cell sums (mixed)
     int64_t g_launches = 0;
@@ -203,6 +219,49 @@ unsigned long long f64_texture(const double *base, size_t count) {
         return 0;
     }
     return (unsigned long long)t;
+}
+
+// cuTensorMapEncodeTiled, looked up through the runtime (no link against
+// the driver library)
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    });
+    return fn;
+}
+
+// TMA descriptor of a mixed box's packed FP32 copy f4 for cell blocks kb
+// cells high: the copy viewed as floats (4*nz2, ny5, nx5), box
+// (4*(kb+9), kBlkWinY, kBlkWinX) -- kb+8 levels used, one more so that the
+// columns' stride in shared memory is an odd number of float4 --, zero fill
+// outside the array
+bool encode_f4_map(DevBox &B, int kb) {
+    EncodeTiledFn fn = encode_tiled();
+    if (!fn || !B.f4) return false;
+    const DevGrid &g = B.g;
+    CUtensorMap m;
+    const cuuint64_t dims[3] = {4ull * (cuuint64_t)g.nz2, (cuuint64_t)g.ny5, (cuuint64_t)g.nx5};
+    const cuuint64_t strides[2] = {16ull * (cuuint64_t)g.nz2, 16ull * (cuuint64_t)g.nz2 * (cuuint64_t)g.ny5};
+    const cuuint32_t box[3] = {4u * (cuuint32_t)(kb + 9), (cuuint32_t)kBlkWinY, (cuuint32_t)kBlkWinX};
+    const cuuint32_t es[3] = {1, 1, 1};
+    if (box[0] > 256) return false;
+    CUresult r = fn(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)B.f4, dims, strides, box, es,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return false;
+    static_assert(sizeof(CUtensorMap) == sizeof(B.tmap_f4), "tensor map size");
+    memcpy(B.tmap_f4, &m, sizeof m);
+    return true;
 }
 
 void carve_state(Carver &cv, DevState &s, size_t n) {
@@ -534,6 +593,8 @@ bool box_ok(ntlp_ctx *c, int b) { return c && b >= 0 && b < c->nbox; }
 
 extern "C" void ntlp_ctx_destroy(ntlp_ctx *c) {
     if (!c) return;
+    if (c->up_stream) cudaStreamSynchronize(c->up_stream);
+    if (c->down_stream) cudaStreamSynchronize(c->down_stream);
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->gexec) cudaGraphExecDestroy(c->gexec);
     for (auto &r : c->recs) {
@@ -552,8 +613,14 @@ extern "C" void ntlp_ctx_destroy(ntlp_ctx *c) {
         if (h.arena_stats) cudaFreeAsync(h.arena_stats, c->stream);
     }
     if (c->small_arena) cudaFreeAsync(c->small_arena, c->stream);
+    if (c->up_area) cudaFreeAsync(c->up_area, c->stream);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    for (cudaEvent_t e : {c->ev_up, c->ev_fill, c->ev_dep, c->ev_down})
+        if (e) cudaEventDestroy(e);
+    if (c->up_stream) cudaStreamDestroy(c->up_stream);
+    if (c->down_stream) cudaStreamDestroy(c->down_stream);
     if (c->counters_h) cudaFreeHost(c->counters_h);
+    if (c->err_h) cudaFreeHost(c->err_h);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
 }
@@ -707,8 +774,22 @@ int create(int nbox, const ntlp_grid *grids, const ntlp_params *params, const in
             cudaMemsetAsync(B.counters, 0, sizeof(long long) * kNumCounters, c->stream))
             return bail(fail(c, NTLP_ERR_CUDA, "initialising box %d failed", b));
     }
-    // tiles: droplets (128 and 256 per tile), cells (scan tiles), deposition (3 shapes)
-    std::vector<Tile> dt[kNtVariants], ct, dpt[kDepVariants];
+    // staged interpolation (mixed, 6th order): one block height for the
+    // context, from its droplets per cell
+    if (mixed && params->ilin == 0) {
+        double caps_sum = 0.0, cells = 0.0;
+        for (int b = 0; b < nbox; ++b) {
+            caps_sum += (double)c->bh[b].cap;
+            cells += (double)c->box[b].g.ncells;
+        }
+        c->blk_kb = interp_block_kb(caps_sum / cells);
+        for (int b = 0; b < nbox && c->blk_kb; ++b)
+            if (!encode_f4_map(c->box[b], c->blk_kb)) c->blk_kb = 0;
+        for (int b = 0; b < nbox; ++b) c->box[b].blk_kb = c->blk_kb;
+    }
+    // tiles: droplets (128 and 256 per tile), cells (scan tiles), deposition
+    // (3 shapes), interpolation cell blocks
+    std::vector<Tile> dt[kNtVariants], ct, dpt[kDepVariants], bt;
     std::vector<int> bft;
     for (int b = 0; b < nbox; ++b) {
         const DevGrid &g = c->box[b].g;
@@ -719,6 +800,11 @@ int create(int nbox, const ntlp_grid *grids, const ntlp_params *params, const in
         for (int v = 0; v < kDepVariants; ++v) {
             long long nt = deposit_tile_count(v, g.dnx, g.dny, g.nnz);
             for (long long s = 0; s < nt; ++s) dpt[v].push_back(Tile{b, (int)s});
+        }
+        if (c->blk_kb) {
+            const long long nb = interp_block_count(c->blk_kb, g.nnx, g.nny, g.nnz);
+            for (long long s = 0; s < nb; ++s) bt.push_back(Tile{b, (int)s});
+            for (int r = 0; r < kOobBlockTiles; ++r) bt.push_back(Tile{b, -1 - r});
         }
     }
     bft.push_back((int)ct.size());
@@ -737,6 +823,7 @@ int create(int nbox, const ntlp_grid *grids, const ntlp_params *params, const in
             }
             k.take(&c->dp_d, 1);
             k.take(&c->box_d, (size_t)nbox);
+            if (!bt.empty()) k.take(&c->blk_tiles_d, bt.size());
         };
         Carver cv;
         lay(cv);
@@ -764,6 +851,10 @@ int create(int nbox, const ntlp_grid *grids, const ntlp_params *params, const in
     }
     bad |= cudaMemcpyAsync(c->box_first_tile_d, bft.data(), bft.size() * sizeof(int), cudaMemcpyHostToDevice,
                            c->stream) != cudaSuccess;
+    c->n_blk_tiles = (int)bt.size();
+    if (!bt.empty())
+        bad |= cudaMemcpyAsync(c->blk_tiles_d, bt.data(), bt.size() * sizeof(Tile), cudaMemcpyHostToDevice,
+                               c->stream) != cudaSuccess;
     bad |= cudaMemcpyAsync(c->dp_d, &c->dp, sizeof(DevParams), cudaMemcpyHostToDevice, c->stream) != cudaSuccess;
     if (bad) return bail(fail(c, NTLP_ERR_CUDA, "uploading the tile tables failed"));
     c->plan.drop_tiles = c->drop_tiles_d[0];
@@ -774,10 +865,12 @@ int create(int nbox, const ntlp_grid *grids, const ntlp_params *params, const in
     c->plan.box_first_tile = c->box_first_tile_d;
     c->plan.nbox = nbox;
     c->plan.any_big = c->any_big_d;
-    if (cudaMallocHost((void **)&c->counters_h, sizeof(long long) * kNumCounters * nbox) != cudaSuccess)
+    if (cudaMallocHost((void **)&c->counters_h, sizeof(long long) * kNumCounters * nbox) != cudaSuccess ||
+        cudaMallocHost((void **)&c->err_h, sizeof(int) * nbox) != cudaSuccess)
         return bail(fail(c, NTLP_ERR_NOMEM, "pinned counter buffer refused"));
     if (push_boxes(c)) return bail(NTLP_ERR_CUDA);
     if (mixed) prepare_kernels_mixed(); else prepare_kernels64();
+    if (c->blk_kb) prepare_interp_block();
     // the host vectors above are copied from: wait before they go out of scope
     if (cudaStreamSynchronize(c->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess)
         return bail(fail(c, NTLP_ERR_CUDA, "context set-up failed"));
@@ -820,6 +913,7 @@ int fields_ext(ntlp_ctx *c, int b, const double *const h[5]) {
     if (B.f4) launch_pack_f32(&B, (float4 *)B.f4, (float *)B.fw, c->stream);
     CK(cudaGetLastError());
     c->bh[b].have_fields = true;
+    if (b == 0) c->up_pending = false;
     return NTLP_OK;
 }
 
@@ -839,6 +933,51 @@ int fields_flow(ntlp_ctx *c, int b, const double *const h[5]) {
     if (B.f4) launch_pack_f32(&B, (float4 *)B.f4, (float *)B.fw, c->stream);
     CK(cudaGetLastError());
     c->bh[b].have_fields = true;
+    if (b == 0) c->up_pending = false;
+    return NTLP_OK;
+}
+
+// copy streams, events and the upload area, on first use
+int async_setup(ntlp_ctx *c) {
+    if (!c->up_stream) {
+        CK(cudaStreamCreateWithFlags(&c->up_stream, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&c->down_stream, cudaStreamNonBlocking));
+        for (cudaEvent_t *e : {&c->ev_up, &c->ev_fill, &c->ev_dep, &c->ev_down})
+            CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    }
+    if (!c->up_area) {
+        const DevGrid &g = c->box[0].g;
+        const size_t nflow = (size_t)g.nnx * g.nny * g.nz2;
+        if (pool_alloc(c, (void **)&c->up_area, 5 * nflow * sizeof(double)) != cudaSuccess) {
+            c->up_area = nullptr;
+            return fail(c, NTLP_ERR_NOMEM, "device allocation of the field upload area refused");
+        }
+        c->bytes += (int64_t)(5 * nflow * sizeof(double));
+    }
+    return NTLP_OK;
+}
+
+// a pending asynchronous field upload: the compute stream waits for its
+// copies, then fills the halo and the FP32 copies from the upload area
+int consume_upload(ntlp_ctx *c) {
+    if (!c->up_pending) return NTLP_OK;
+    const DevBox &B = c->box[0];
+    const size_t nflow = (size_t)B.g.nnx * B.g.nny * B.g.nz2;
+    CK(cudaStreamWaitEvent(c->stream, c->ev_up, 0));
+    for (int k = 0; k < 5; ++k) launch_fill_ext(c->up_area + k * nflow, (double *)B.f[k], B.g, c->stream);
+    if (B.f4) launch_pack_f32(&B, (float4 *)B.f4, (float *)B.fw, c->stream);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(c->ev_fill, c->stream));
+    c->launches += B.f4 ? 6 : 5;
+    c->fill_recorded = true;
+    c->up_pending = false;
+    return NTLP_OK;
+}
+
+// the previous asynchronous source download reads the source arrays: the
+// next deposition waits for it
+int wait_download(ntlp_ctx *c) {
+    if (c->down_pending) CK(cudaStreamWaitEvent(c->stream, c->ev_down, 0));
     return NTLP_OK;
 }
 
@@ -983,7 +1122,8 @@ int launch_step(ntlp_ctx *c, int kind, int istage, double dt, int32_t it, bool w
         if (c->params.precision == NTLP_PREC_MIXED)
             launch_update_be_mixed(c->params.ilin, nt, c->box_d, c->drop_tiles_d[c->nt_variant],
                                    c->n_drop_tiles[c->nt_variant], c->drop_tiles_d[0], c->n_drop_tiles[0], c->nbox,
-                                   c->dp, in, c->stream, c->tex_all);
+                                   c->dp, in, c->stream, c->tex_all, c->blk_on ? c->blk_kb : 0, c->blk_tiles_d,
+                                   c->n_blk_tiles);
         else
             launch_update_be64(c->params.ilin, nt, c->box_d, c->drop_tiles_d[c->nt_variant],
                                c->n_drop_tiles[c->nt_variant], c->nbox, c->dp, in, c->stream, c->tex_all64);
@@ -1036,11 +1176,19 @@ int check_ready(ntlp_ctx *c, double dt) {
     return NTLP_OK;
 }
 
+// the step's counters, and its device error words: a kernel that gave up
+// a bounded wait reports it here
 int read_counters(ntlp_ctx *c) {
-    for (int b = 0; b < c->nbox; ++b)
+    for (int b = 0; b < c->nbox; ++b) {
         CK(cudaMemcpyAsync(c->counters_h + (size_t)b * kNumCounters, c->box[b].counters,
                            sizeof(long long) * kNumCounters, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(c->err_h + b, c->box[b].err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    }
     CK(cudaStreamSynchronize(c->stream));
+    for (int b = 0; b < c->nbox; ++b)
+        if (c->err_h[b] & ERR_STAGE_WAIT)
+            return fail(c, NTLP_ERR_CUDA, "box %d: a staged field tile did not arrive within the wait limit "
+                                          "(results of the step are from global memory)", b);
     return NTLP_OK;
 }
 
@@ -1060,6 +1208,7 @@ int do_step(ntlp_ctx *c, int kind, int istage, double dt, int32_t it, ntlp_count
     int rc = check_ready(c, dt);
     if (rc) return rc;
     if (kind == 2 && (rc = alloc_rk3(c))) return rc;
+    if ((rc = consume_upload(c))) return rc;
     if ((rc = launch_step(c, kind, istage, dt, it, false))) return rc;
     mirror_flip(c, 1);
     const bool payload = (kind == 1 || istage == 3);
@@ -1154,6 +1303,44 @@ int stats_run(ntlp_ctx *c, int b, bool radius_hist) {
     return NTLP_OK;
 }
 
+// the deposition of particle_coupling_update on the context's stream
+int launch_coupling(ntlp_ctx *c, double dt) {
+    int rc = wait_download(c);
+    if (rc) return rc;
+    if (!c->payload_valid || c->last_dt != dt) {
+        cudaEvent_t ep = phase_begin(c);
+        if (c->params.precision == NTLP_PREC_MIXED)
+            launch_payload_mixed(c->box_d, c->drop_tiles_d[0], c->n_drop_tiles[0], c->dp, dt, c->stream);
+        else
+            launch_payload64(c->box_d, c->drop_tiles_d[0], c->n_drop_tiles[0], c->dp, dt, c->stream);
+        phase_end(c, PH_OTHER, ep);
+        c->launches += 1;
+        c->payload_valid = true;
+        c->last_dt = dt;
+    }
+    cudaEvent_t e0 = phase_begin(c);
+    const int v = c->dep_variant;
+    if (c->params.precision == NTLP_PREC_MIXED)
+        launch_deposit_mixed(v, c->box_d, c->dep_tiles_d[v], c->n_dep_tiles[v], c->dp, c->stream, c->nbox,
+                             c->any_dense, c->overflow_list_d);
+    else
+        launch_deposit64(v, c->box_d, c->dep_tiles_d[v], c->n_dep_tiles[v], c->dp, c->stream);
+    phase_end(c, PH_DEPOSIT, e0);
+    c->launches += deposit_launches(c);
+    CK(cudaGetLastError());
+    return NTLP_OK;
+}
+
+int coupling_checks(ntlp_ctx *c, double dt, int32_t layout) {
+    bool any = false;
+    for (auto &h : c->bh) any = any || h.have_droplets;
+    if (!any) return fail(c, NTLP_ERR_STATE, "droplets not uploaded");
+    if (layout != NTLP_LAYOUT_COLUMN && layout != NTLP_LAYOUT_FLOW)
+        return fail(c, NTLP_ERR_ARG, "unknown layout %d", layout);
+    if (!(dt > 0.0)) return fail(c, NTLP_ERR_ARG, "dt must be positive");
+    return NTLP_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1211,7 +1398,7 @@ int64_t ntlp_numpart(const ntlp_ctx *cc) { return ntlp_box_numpart(const_cast<nt
 int ntlp_sync(ntlp_ctx *c) {
     if (!c) return NTLP_ERR_ARG;
     CK(cudaStreamSynchronize(c->stream));
-    return NTLP_OK;
+    return ntlp_copies_wait(c);
 }
 
 void *ntlp_stream(ntlp_ctx *c) { return c ? (void *)c->stream : nullptr; }
@@ -1221,6 +1408,14 @@ int ntlp_use_stream(ntlp_ctx *c, void *stream) {
     CK(cudaStreamSynchronize(c->stream));
     c->stream = stream ? (cudaStream_t)stream : c->own_stream;
     return NTLP_OK;
+}
+
+int ntlp_interp_staging(ntlp_ctx *c, int32_t enable) {
+    if (!c) return NTLP_ERR_ARG;
+    if (enable == 0 || enable == 1) {
+        c->blk_on = enable == 1;
+    }
+    return c->blk_on ? c->blk_kb : 0;
 }
 
 int ntlp_profile_enable(ntlp_ctx *c, int enable) {
@@ -1307,33 +1502,8 @@ int ntlp_box_counters(ntlp_ctx *c, int32_t box, ntlp_counters *out) {
 int ntlp_coupling(ntlp_ctx *c, double dt, int32_t layout, double *partsrc, double *partTsrc, double *partHsrc,
                   double *partTEsrc) {
     if (!c) return NTLP_ERR_ARG;
-    bool any = false;
-    for (auto &h : c->bh) any = any || h.have_droplets;
-    if (!any) return fail(c, NTLP_ERR_STATE, "droplets not uploaded");
-    if (layout != NTLP_LAYOUT_COLUMN && layout != NTLP_LAYOUT_FLOW)
-        return fail(c, NTLP_ERR_ARG, "unknown layout %d", layout);
-    if (!(dt > 0.0)) return fail(c, NTLP_ERR_ARG, "dt must be positive");
-    if (!c->payload_valid || c->last_dt != dt) {
-        cudaEvent_t ep = phase_begin(c);
-        if (c->params.precision == NTLP_PREC_MIXED)
-            launch_payload_mixed(c->box_d, c->drop_tiles_d[0], c->n_drop_tiles[0], c->dp, dt, c->stream);
-        else
-            launch_payload64(c->box_d, c->drop_tiles_d[0], c->n_drop_tiles[0], c->dp, dt, c->stream);
-        phase_end(c, PH_OTHER, ep);
-        c->launches += 1;
-        c->payload_valid = true;
-        c->last_dt = dt;
-    }
-    cudaEvent_t e0 = phase_begin(c);
-    const int v = c->dep_variant;
-    if (c->params.precision == NTLP_PREC_MIXED)
-        launch_deposit_mixed(v, c->box_d, c->dep_tiles_d[v], c->n_dep_tiles[v], c->dp, c->stream, c->nbox,
-                             c->any_dense, c->overflow_list_d);
-    else
-        launch_deposit64(v, c->box_d, c->dep_tiles_d[v], c->n_dep_tiles[v], c->dp, c->stream);
-    phase_end(c, PH_DEPOSIT, e0);
-    c->launches += deposit_launches(c);
-    CK(cudaGetLastError());
+    int rc = coupling_checks(c, dt, layout);
+    if (rc || (rc = launch_coupling(c, dt))) return rc;
     double *host[6] = {partsrc, nullptr, nullptr, partTsrc, partHsrc, partTEsrc};
     if (partsrc) {
         const size_t nn = (size_t)c->box[0].g.nnodes;
@@ -1341,6 +1511,57 @@ int ntlp_coupling(ntlp_ctx *c, double dt, int32_t layout, double *partsrc, doubl
         host[2] = partsrc + 2 * nn;
     }
     return sources_out(c, 0, layout, host);
+}
+
+int ntlp_fields_upload_async(ntlp_ctx *c, const double *u, const double *v, const double *w, const double *t,
+                             const double *q) {
+    if (!c) return NTLP_ERR_ARG;
+    const double *h[5] = {u, v, w, t, q};
+    for (int k = 0; k < 5; ++k)
+        if (!h[k]) return fail(c, NTLP_ERR_ARG, "field %d is NULL", k);
+    if (!c->box[0].g.periodic)
+        return fail(c, NTLP_ERR_STATE, "a subdomain takes its fields with halos (ntlp_fields_upload_ext)");
+    int rc = async_setup(c);
+    if (rc) return rc;
+    const DevGrid &g = c->box[0].g;
+    const size_t nflow = (size_t)g.nnx * g.nny * g.nz2;
+    // the area is free once the previous upload's halo fill has read it
+    if (c->fill_recorded) CK(cudaStreamWaitEvent(c->up_stream, c->ev_fill, 0));
+    for (int k = 0; k < 5; ++k)
+        CK(cudaMemcpyAsync(c->up_area + k * nflow, h[k], nflow * sizeof(double), cudaMemcpyDefault,
+                           c->up_stream));
+    CK(cudaEventRecord(c->ev_up, c->up_stream));
+    c->up_pending = true;
+    c->bh[0].have_fields = true;
+    return NTLP_OK;
+}
+
+int ntlp_coupling_async(ntlp_ctx *c, double dt, double *partsrc, double *partTsrc, double *partHsrc,
+                        double *partTEsrc) {
+    if (!c) return NTLP_ERR_ARG;
+    if (!c->box[0].g.periodic) return fail(c, NTLP_ERR_STATE, "a subdomain returns its sources with ntlp_coupling");
+    int rc = coupling_checks(c, dt, NTLP_LAYOUT_COLUMN);
+    if (rc || (rc = async_setup(c)) || (rc = launch_coupling(c, dt))) return rc;
+    const DevBox &B = c->box[0];
+    const size_t nn = (size_t)B.g.nnodes;
+    double *host[6] = {partsrc, partsrc ? partsrc + nn : nullptr, partsrc ? partsrc + 2 * nn : nullptr, partTsrc,
+                       partHsrc, partTEsrc};
+    CK(cudaEventRecord(c->ev_dep, c->stream));
+    CK(cudaStreamWaitEvent(c->down_stream, c->ev_dep, 0));
+    for (int q = 0; q < 6; ++q)
+        if (host[q]) CK(cudaMemcpyAsync(host[q], B.src[q], nn * sizeof(double), cudaMemcpyDefault, c->down_stream));
+    CK(cudaEventRecord(c->ev_down, c->down_stream));
+    c->down_pending = true;
+    return NTLP_OK;
+}
+
+int ntlp_copies_wait(ntlp_ctx *c) {
+    if (!c) return NTLP_ERR_ARG;
+    if (c->up_stream) {
+        CK(cudaStreamSynchronize(c->up_stream));
+        CK(cudaStreamSynchronize(c->down_stream));
+    }
+    return NTLP_OK;
 }
 
 int ntlp_box_sources(ntlp_ctx *c, int32_t box, int32_t layout, double *partsrc, double *partTsrc,
@@ -1390,8 +1611,9 @@ int ntlp_advance_graph(ntlp_ctx *c, double dt, int32_t it, int32_t nsteps) {
     if (nsteps < 1 || nsteps > 1000) return fail(c, NTLP_ERR_ARG, "nsteps must be in 1..1000");
     int rc = check_ready(c, dt);
     if (rc) return rc;
+    if ((rc = consume_upload(c)) || (rc = wait_download(c))) return rc;
     if (!c->gexec || c->g_dt != dt || c->g_nsteps != nsteps || c->g_dep != c->dep_variant ||
-        c->g_nt != c->nt_variant) {
+        c->g_nt != c->nt_variant || c->g_blk != c->blk_on) {
         if (c->gexec) {
             cudaGraphExecDestroy(c->gexec);
             c->gexec = nullptr;
@@ -1422,6 +1644,7 @@ int ntlp_advance_graph(ntlp_ctx *c, double dt, int32_t it, int32_t nsteps) {
         c->g_nsteps = nsteps;
         c->g_dep = c->dep_variant;
         c->g_nt = c->nt_variant;
+        c->g_blk = c->blk_on;
     }
     cudaEvent_t e0 = phase_begin(c);
     CK(cudaGraphLaunch(c->gexec, c->stream));
@@ -1438,6 +1661,7 @@ int ntlp_autotune(ntlp_ctx *c, double dt, int32_t it, int32_t steps, int32_t cho
     if (!c) return NTLP_ERR_ARG;
     int rc = check_ready(c, dt);
     if (rc) return rc;
+    if ((rc = consume_upload(c)) || (rc = wait_download(c))) return rc;
     if (steps < 1) steps = 1;
     if (it < 2) it = 2;
     cudaEvent_t a, b;

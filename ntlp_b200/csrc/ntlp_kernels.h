@@ -45,9 +45,27 @@ void launch_deposit64(int variant, DevBox *boxes, const Tile *tiles, int ntiles,
                       cudaStream_t st);
 
 // mixed precision (ntlp_mixed.cu)
+// blk_kb > 0 (6th order): the interpolation runs over cell blocks of
+// kBlkX x kBlkY x blk_kb cells (blk_tiles: per box, the blocks in the order
+// (ipt block, jpt block, kpt block), then kOobBlockTiles tiles with
+// start = -1 - r for the out-of-range bucket)
 void launch_update_be_mixed(int ilin, int nt, DevBox *boxes, const Tile *tiles, int ntiles, const Tile *tiles128,
-                            int ntiles128, int nbox, const DevParams &P, StepIn in, cudaStream_t st,
-                            bool tex);
+                            int ntiles128, int nbox, const DevParams &P, StepIn in, cudaStream_t st, bool tex,
+                            int blk_kb, const Tile *blk_tiles, int n_blk_tiles);
+constexpr int kBlockThreads = 160;   // threads of a cell-block interpolation CTA
+constexpr int kOobBlockTiles = 8;    // tiles per box over the out-of-range bucket
+int interp_block_smem(int kb);       // dynamic shared memory of a cell-block CTA
+void prepare_interp_block();         // kernel attributes, once per device
+// cells per block in z for a droplet density (droplets per cell): about 128
+// droplets per block, a multiple of 4 in 4..32
+inline int interp_block_kb(double density) {
+    const double want = 128.0 / (kBlkX * kBlkY * (density > 1e-9 ? density : 1e-9));
+    int kb = 4 * (int)(want / 4.0 + 0.5);
+    return kb < 4 ? 4 : (kb > 32 ? 32 : (kb > 16 ? 32 : (kb > 8 ? 16 : kb)));
+}
+inline long long interp_block_count(int kb, int nnx, int nny, int nnz) {
+    return (long long)((nnx + kBlkX) / kBlkX) * ((nny + kBlkY) / kBlkY) * ((nnz + kb) / kb);
+}
 void launch_payload_mixed(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams &P, double dt,
                           cudaStream_t st);
 // dense: some box has per-cell sums (cellsum), deposited by the cell-sum

@@ -225,6 +225,255 @@ k_interp_mixed(DevBox *boxes, const Tile *tiles) {
     B.key[t] = bad | (I.kw << 1);
 }
 
+// ---------------------------------------------------------------------------
+// Staged 6th-order interpolation over cell blocks.
+//
+// One CTA takes one block of kBlkX x kBlkY x KB cells.  The droplets of the
+// block are the 16 runs of the sorted order given by the cell offsets of
+// its columns.  The CTA stages the block's node window once: the packed
+// (u, v, T, q) copy by one TMA tile load (cp.async.bulk.tensor, completion
+// on an mbarrier), the w copy by 4-byte asynchronous copies; then every
+// droplet contracts its 6x6x6 stencil from shared memory, in the same
+// order and with the same FMAs as interp6_mixed, so the results are the
+// same bits.  Droplets whose stencil leaves the window (cells at x = xl or
+// y = yl, whose stencil wraps) or whose indices are out of range take
+// interp6_mixed from global memory.  Extra CTAs (tile.start < 0) take the
+// droplets of the out-of-range bucket.
+//
+// The tensor map covers this GPU's own field copy only, and no load is
+// multicast.
+// ---------------------------------------------------------------------------
+constexpr int kOobCtas = kOobBlockTiles;   // CTAs per box over the out-of-range bucket
+constexpr long long kStageSpin = 1 << 22; // mbarrier polls before the wait is given up
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void stage_f4(float4 *dst, const void *tmap, unsigned long long *bar, int c0, int c1,
+                                         int c2, unsigned bytes) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(tmap) : "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], "
+        "[%2];" ::"r"(smem_u32(dst)),
+        "l"(tmap), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
+        : "memory");
+}
+
+__device__ __forceinline__ bool stage_arrived(unsigned long long *bar) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar))
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ void copy4_async(float *dst, const float *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+
+__device__ __noinline__ void interp6_mixed_global(const DevBox &B, double x1, double x2, double x3, Interp &o,
+                                                  int &bad) {
+    interp6_mixed<false>(B, x1, x2, x3, o, bad);
+}
+
+// interp6_mixed from the staged window of the block at cells (i0, j0, k0);
+// false (nothing written) when the droplet's stencil is not inside it
+template <int KB>
+__device__ __forceinline__ bool interp6_staged(const DevBox &B, const float4 *s4, const float *sw, int i0, int j0,
+                                               int k0, double x1, double x2, double x3, Interp &o) {
+    constexpr int ZS = KB + 9;      // column stride (KB + 8 levels used; odd, to spread the banks)
+    const DevGrid &g = B.g;
+    const int nnz = g.nnz;
+    const int ip3g = ijpt(x1, g.dx), jp3g = ijpt(x2, g.dy);
+    const int ip3 = ip3g - g.ioff, jp3 = jp3g - g.joff;
+    const int ku2 = minloc_zz(g, x3) - 2;
+    const int kw2 = minloc_z(g, x3) - 2;
+    const int xo = ip3 - i0, yo = jp3 - j0, zu = ku2 - k0 + 2, zw = kw2 - k0 + 2;
+    if (ku2 < 0 || ku2 > nnz || kw2 < 0 || kw2 > nnz || g.rden_zz == nullptr || ip3 > g.nnx || jp3 > g.nny ||
+        (unsigned)xo >= (unsigned)kBlkX || (unsigned)yo >= (unsigned)kBlkY || zu < 0 || zu + 6 > KB + 8 || zw < 0 ||
+        zw + 6 > KB + 8)
+        return false;
+    o.kw = kw2 + 2;
+    float wx[6], wy[6], wz[6], wzw[6];
+    lagrange6_unif((float)(x1 / g.dx - (double)(ip3g - 3)), wx);
+    lagrange6_unif((float)(x2 / g.dy - (double)(jp3g - 3)), wy);
+    lagrange6_win(x3, g.zz, ku2, g.nz2, g.rden_zz + (ku2 + 2) * 6, wz);
+    lagrange6_win(x3, g.z, kw2, g.nz2, g.rden_z + (kw2 + 2) * 6, wzw);
+    float su = 0.f, sv = 0.f, sw_ = 0.f, sT = 0.f, sq = 0.f;
+#pragma unroll 1
+    for (int i = 0; i < 6; ++i) {
+        const int col = ((xo + i) * kBlkWinY + yo) * ZS;
+        float cu_ = 0.f, cv = 0.f, cw_ = 0.f, cT = 0.f, cq = 0.f;
+#pragma unroll
+        for (int j = 0; j < 6; ++j) {
+            const float4 *p4 = s4 + col + j * ZS + zu;
+            const float *pw = sw + col + j * ZS + zw;
+            float au = 0.f, av = 0.f, aT = 0.f, aq = 0.f, aw = 0.f;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                const float4 val = p4[k];
+                au = fmaf(val.x, wz[k], au);
+                av = fmaf(val.y, wz[k], av);
+                aT = fmaf(val.z, wz[k], aT);
+                aq = fmaf(val.w, wz[k], aq);
+                aw = fmaf(pw[k], wzw[k], aw);
+            }
+            cu_ = fmaf(au, wy[j], cu_);
+            cv = fmaf(av, wy[j], cv);
+            cw_ = fmaf(aw, wy[j], cw_);
+            cT = fmaf(aT, wy[j], cT);
+            cq = fmaf(aq, wy[j], cq);
+        }
+        su = fmaf(cu_, wx[0], su);
+        sv = fmaf(cv, wx[0], sv);
+        sw_ = fmaf(cw_, wx[0], sw_);
+        sT = fmaf(cT, wx[0], sT);
+        sq = fmaf(cq, wx[0], sq);
+#pragma unroll
+        for (int r = 0; r < 5; ++r) wx[r] = wx[r + 1];
+    }
+    const long long ridx = f32_ref_index(g);
+    o.uf[0] = B.f[0][ridx] + (double)su;
+    o.uf[1] = B.f[1][ridx] + (double)sv;
+    o.uf[2] = B.f[2][ridx] + (double)sw_;
+    o.Tf = B.f[3][ridx] + (double)sT;
+    o.qinf = B.f[4][ridx] + (double)sq;
+    return true;
+}
+
+__device__ __forceinline__ void interp_out(const DevBox &B, int t, const Interp &I, int bad) {
+    const DevState &O = B.st[1 - B.cur];
+    O.uf[0][t] = I.uf[0];
+    O.uf[1][t] = I.uf[1];
+    O.uf[2][t] = I.uf[2];
+    O.Tf[t] = I.Tf;
+    O.qinf[t] = I.qinf;
+    B.key[t] = bad | (I.kw << 1);
+}
+
+template <int KB>
+__global__ void __launch_bounds__(kBlockThreads, 4) k_interp_block(DevBox *boxes, const Tile *tiles) {
+    constexpr int ZS = KB + 9;      // staged levels per column (KB + 8 used, + 1 for an odd stride)
+    constexpr int NT = kBlockThreads;
+    constexpr int NCOL = kBlkWinX * kBlkWinY;
+    extern __shared__ unsigned char smem_raw[];
+    __shared__ __align__(8) unsigned long long bar;
+    __shared__ int s_lo[kBlkX * kBlkY], s_off[kBlkX * kBlkY + 1];
+    const Tile tl = tiles[blockIdx.x];
+    const DevBox &B = boxes[tl.box];
+    const DevGrid &g = B.g;
+    const DevState &S = B.st[B.cur];
+    if (tl.start < 0) {
+        // the out-of-range bucket (interp6_mixed flags the droplet)
+        const int a = B.cell_start[g.ncells], e = B.cell_start[g.ncells + 1];
+        for (int t = a + (-1 - tl.start) * NT + (int)threadIdx.x; t < e; t += kOobCtas * NT) {
+            const int s = B.perm[t];
+            Interp I;
+            int bad = 0;
+            interp6_mixed_global(B, S.x[0][s], S.x[1][s], S.x[2][s], I, bad);
+            interp_out(B, t, I, bad);
+        }
+        return;
+    }
+    const int nbj = (g.nny + kBlkY) / kBlkY;    // ceil((nny+1)/kBlkY)
+    const int nbk = (g.nnz + KB) / KB;          // ceil((nnz+1)/KB)
+    const int bk = tl.start % nbk;
+    const int bij = tl.start / nbk;
+    const int i0 = 1 + kBlkX * (bij / nbj), j0 = 1 + kBlkY * (bij % nbj), k0 = KB * bk;
+    if (threadIdx.x < kBlkX * kBlkY) {
+        const int ipt = i0 + (int)threadIdx.x / kBlkY, jpt = j0 + (int)threadIdx.x % kBlkY;
+        int lo = 0, cnt = 0;
+        if (ipt <= g.nnx + 1 && jpt <= g.nny + 1) {
+            const int k1 = min(k0 + KB, g.nnz + 1);
+            const long long key0 = k0 + (long long)(g.nnz + 1) * ((jpt - 1) + (long long)(g.nny + 1) * (ipt - 1));
+            lo = B.cell_start[key0];
+            cnt = B.cell_start[key0 + (k1 - k0)] - lo;
+        }
+        int x = cnt;
+#pragma unroll
+        for (int o = 1; o < kBlkX * kBlkY; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffu, x, o);
+            if ((int)threadIdx.x >= o) x += y;
+        }
+        s_lo[threadIdx.x] = lo;
+        s_off[threadIdx.x + 1] = x;
+        if (threadIdx.x == 0) s_off[0] = 0;
+    }
+    __syncthreads();
+    const int total = s_off[kBlkX * kBlkY];
+    if (total == 0) return;
+
+    float4 *s4 = reinterpret_cast<float4 *>(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+    float *swin = reinterpret_cast<float *>(s4 + NCOL * ZS);
+    if (threadIdx.x == 0)
+        stage_f4(s4, B.tmap_f4, &bar, 4 * (k0 - 4), j0 - 1, i0 - 1, (unsigned)(NCOL * ZS * sizeof(float4)));
+    for (int e = threadIdx.x; e < NCOL * ZS; e += NT) {
+        const int zi = e % ZS, c = e / ZS;
+        const int k = k0 - 4 + zi, ya = j0 - 1 + c % kBlkWinY, xa = i0 - 1 + c / kBlkWinY;
+        if (k >= 0 && k < g.nz2 && ya < g.ny5 && xa < g.nx5)
+            copy4_async(swin + e, B.fw + k + (long long)g.nz2 * (ya + (long long)g.ny5 * xa));
+        else
+            swin[e] = 0.f;
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncthreads();
+    bool ok = false;
+    for (long long n = 0; n < kStageSpin && !ok; ++n) ok = stage_arrived(&bar);
+    ok = __syncthreads_and(ok) != 0;
+    if (!ok && threadIdx.x == 0) atomicOr(B.err, ERR_STAGE_WAIT);
+
+    for (int q = threadIdx.x; q < total; q += NT) {
+        int c = 0;
+#pragma unroll
+        for (int h = kBlkX * kBlkY / 2; h > 0; h >>= 1)
+            if (s_off[c + h] <= q) c += h;
+        const int t = s_lo[c] + (q - s_off[c]);
+        const int s = B.perm[t];
+        const double x1 = S.x[0][s], x2 = S.x[1][s], x3 = S.x[2][s];
+        Interp I;
+        int bad = 0;
+        if (!ok || !interp6_staged<KB>(B, s4, swin, i0, j0, k0, x1, x2, x3, I))
+            interp6_mixed_global(B, x1, x2, x3, I, bad);
+        interp_out(B, t, I, bad);
+    }
+    if (!ok) {
+        // the tile may still land: wait (bounded) before the shared memory
+        // goes to another CTA
+        bool late = false;
+        for (long long n = 0; n < kStageSpin && !late; ++n) late = stage_arrived(&bar);
+    }
+}
+
+int interp_block_smem(int kb) {
+    return kBlkWinX * kBlkWinY * (kb + 9) * (int)(sizeof(float4) + sizeof(float)) + 128;
+}
+
+template <int KB>
+static void blk_attr() {
+    cudaFuncSetAttribute(k_interp_block<KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, interp_block_smem(KB));
+}
+
+void prepare_interp_block() {
+    if (!first_on_device(ONCE_INTERP_BLOCK)) return;
+    blk_attr<4>();
+    blk_attr<8>();
+    blk_attr<16>();
+    blk_attr<32>();
+}
+
+static void launch_interp_block(int kb, DevBox *boxes, const Tile *tiles, int ntiles, cudaStream_t st) {
+    const int sm = interp_block_smem(kb);
+    if (kb == 4) k_interp_block<4><<<ntiles, kBlockThreads, sm, st>>>(boxes, tiles);
+    else if (kb == 16) k_interp_block<16><<<ntiles, kBlockThreads, sm, st>>>(boxes, tiles);
+    else if (kb == 32) k_interp_block<32><<<ntiles, kBlockThreads, sm, st>>>(boxes, tiles);
+    else k_interp_block<8><<<ntiles, kBlockThreads, sm, st>>>(boxes, tiles);
+}
+
 // 7 resident blocks of 128: 72 registers, 28 warps per SM (spills, to L1).
 // Measured at 16.8 M droplets: faster than 5 blocks (94 registers, no
 // spills) and 6 (80); 8 blocks (64 registers) is no faster.
@@ -257,9 +506,12 @@ k_be_defer_mixed(DevBox *boxes, const __grid_constant__ DevParams P, StepIn in) 
 // arithmetic may be contracted by the code generator, and one register
 // budget for every tuning choice keeps the results identical across them.
 void launch_update_be_mixed(int ilin, int nt, DevBox *boxes, const Tile *tiles, int ntiles, const Tile *tiles128,
-                            int ntiles128, int nbox, const DevParams &P, StepIn in, cudaStream_t st, bool tex) {
+                            int ntiles128, int nbox, const DevParams &P, StepIn in, cudaStream_t st, bool tex,
+                            int blk_kb, const Tile *blk_tiles, int n_blk_tiles) {
     if (ntiles <= 0) return;
-    if (nt == 256) {
+    if (ilin == 0 && blk_kb > 0 && n_blk_tiles > 0) {
+        launch_interp_block(blk_kb, boxes, blk_tiles, n_blk_tiles, st);
+    } else if (nt == 256) {
         if (ilin == 1) k_interp_mixed<1, 256, false><<<ntiles, 256, 0, st>>>(boxes, tiles);
         else if (tex) k_interp_mixed<0, 256, true><<<ntiles, 256, 0, st>>>(boxes, tiles);
         else k_interp_mixed<0, 256, false><<<ntiles, 256, 0, st>>>(boxes, tiles);

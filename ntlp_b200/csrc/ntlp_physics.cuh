@@ -688,10 +688,15 @@ __device__ __forceinline__ double be_drag(const DevParams &p, double radius, dou
         const float taup_if = 18.0f * (float)rhoa * (float)p.nuf / rhopf / ((2.0f * rr) * (2.0f * rr));
         const float dtf = (float)dt;
         const float den = 1.0f + dtf * taup_if;
-        float d0 = (float)(v[0] - uf[0]), d1 = (float)(v[1] - uf[1]), d2 = (float)(v[2] - uf[2]);
-        const double Rep = (double)(2.0f * rr * sqrtf(d0 * d0 + d1 * d1 + d2 * d2) / (float)p.nuf);
+        float d[3] = {(float)(v[0] - uf[0]), (float)(v[1] - uf[1]), (float)(v[2] - uf[2])};
+        const double Rep = (double)(2.0f * rr * sqrtf(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) / (float)p.nuf);
+        // the reference's update rearranged as an increment,
+        // v_new - v = (dt taup_i (uf - v) + dt g) / (1 + dt taup_i), formed in
+        // FP32 and added to v in FP64: the increment keeps FP32's relative
+        // precision, which the momentum source (v_new - v)/dt needs when |v|
+        // (a mean wind) is far larger than the change over one step
         for (int a = 0; a < 3; ++a)
-            v[a] = (double)(((float)v[a] + taup_if * dtf * (float)uf[a] + dtf * (float)p.g[a]) / den);
+            v[a] = v[a] + (double)((dtf * (float)p.g[a] - taup_if * dtf * d[a]) / den);
         return Rep;
     } else {
         const double Volp = p.pi2 * 2.0 / 3.0 * cube(radius);

@@ -53,27 +53,44 @@ def _spectral_velocity(shape, g, rms: float, device):
 
 def make_box(edge: int | tuple, n: int, seed: int, params: dict, device, *, length: float = 2.0,
              rms: float = 0.5, T0: float = 293.0, sigT: float = 0.3, q0: float = 0.015,
-             sigq: float = 2e-4, median: float = 1e-6, sigma_g: float = 1.5, kappa: float = 1.2) -> dict:
+             sigq: float = 2e-4, median: float = 1e-6, sigma_g: float = 1.5, kappa: float = 1.2,
+             extent: tuple | None = None, stretch: float | None = None, lapse_per_m: float = 0.0,
+             loglaw_top: float | None = None, z0: float = 0.002844, bimodal: tuple | None = None,
+             zfrac: float = 1.0) -> dict:
     """One periodic box: returns dict(grid=host grid dict, flow=dict of
-    device tensors (nnz+2, nny, nnx), droplets=dict of device tensors)."""
+    device tensors (nnz+2, nny, nnx), droplets=dict of device tensors).
+
+    extent (xl, yl, zl) overrides the cube of side `length`; stretch,
+    lapse_per_m, loglaw_top, bimodal and zfrac have the meaning they have in
+    ``generator.make_fields`` / ``generator.make_droplets``."""
     torch = _torch()
     nnx, nny, nnz = (edge, edge, edge) if isinstance(edge, int) else edge
-    grid = gen.make_grid(nnx, nny, nnz, length, length, length, None)
+    xl, yl, zl = extent if extent is not None else (length, length, length)
+    grid = gen.make_grid(nnx, nny, nnz, xl, yl, zl, stretch)
     g = torch.Generator(device=device)
     g.manual_seed(int(seed))
     shape = (nnx, nny, nnz + 2)
+    f64 = dict(device=device, dtype=torch.float64)
     u, v, w = _spectral_velocity(shape, g, rms, device)
-    T = T0 + sigT * torch.randn(shape, generator=g, device=device, dtype=torch.float64)
-    q = q0 + sigq * torch.randn(shape, generator=g, device=device, dtype=torch.float64)
+    zz = torch.as_tensor(grid["zz"], **f64)
+    if loglaw_top is not None:
+        zc = torch.clamp(zz, min=z0 * 1.0001)
+        u = u + (torch.log(zc / z0) / math.log(zl / z0) * loglaw_top)[None, None, :]
+    T = T0 - lapse_per_m * zz[None, None, :] + sigT * torch.randn(shape, generator=g, **f64)
+    q = q0 + sigq * torch.randn(shape, generator=g, **f64)
     fields = dict(u=u, v=v, w=w, T=T, q=q)
     flow = {k: f.permute(2, 1, 0).contiguous() for k, f in fields.items()}
 
-    xl, yl, zl = grid["xl"], grid["yl"], grid["zl"]
-    f64 = dict(device=device, dtype=torch.float64)
     x = torch.rand(n, generator=g, **f64) * xl
     y = torch.rand(n, generator=g, **f64) * yl
-    zp = torch.rand(n, generator=g, **f64) * zl
-    r = median * torch.exp(math.log(sigma_g) * torch.randn(n, generator=g, **f64))
+    zp = torch.rand(n, generator=g, **f64) * (zl * zfrac)
+    if bimodal is None:
+        r = median * torch.exp(math.log(sigma_g) * torch.randn(n, generator=g, **f64))
+    else:
+        (m1, s1, w1), (m2, s2, _w2) = bimodal
+        pick = torch.rand(n, generator=g, **f64) < w1
+        gs = torch.randn(n, generator=g, **f64)
+        r = torch.where(pick, m1 * torch.exp(math.log(s1) * gs), m2 * torch.exp(math.log(s2) * gs))
     r = r.clamp(2e-8, 5e-4)
     top = float(grid["z"][nnz]) - r
     zp = torch.minimum(zp.clamp_min(0.0), top * (1.0 - 1e-12))
@@ -83,7 +100,6 @@ def make_box(edge: int | tuple, n: int, seed: int, params: dict, device, *, leng
     dx, dy = xl / nnx, yl / nny
     ix = torch.clamp((x / dx + 0.5).long(), max=nnx) % nnx
     iy = torch.clamp((y / dy + 0.5).long(), max=nny) % nny
-    zz = torch.as_tensor(grid["zz"], **f64)
     iz = torch.searchsorted(zz, zp).clamp(0, nnz + 1)
     Tp = T[ix, iy, iz].contiguous()
     vp = torch.stack([u[ix, iy, iz], v[ix, iy, iz], w[ix, iy, iz]]).contiguous()
@@ -98,6 +114,43 @@ def make_box(edge: int | tuple, n: int, seed: int, params: dict, device, *, leng
     }
     d["rc"] = crit_radius(params, m_s, kappa_s, Tp) if params.get("ievap", 1) == 1 else zeros
     return dict(grid=grid, flow=flow, droplets=d)
+
+
+def make_config_box(name: str, params: dict, device, n: int | None = None, seed: int | None = None) -> dict:
+    """A benchmark configuration of ``generator.CONFIGS`` ("c0", "c1", "c2")
+    generated in device memory: its grid, field statistics, droplet count
+    and radius distribution (the values differ from the host generator's:
+    another random stream)."""
+    cfg = gen.CONFIGS[name]
+    nnx, nny, nnz, xl, yl, zl, stretch = cfg["grid"]
+    return make_box((nnx, nny, nnz), cfg["n"] if n is None else n, cfg["seed"] if seed is None else seed, params,
+                    device, extent=(xl, yl, zl), stretch=stretch, rms=cfg["rms"], T0=cfg["T0"], sigT=cfg["sigT"],
+                    q0=cfg["q0"], sigq=cfg["sigq"], lapse_per_m=cfg.get("lapse", 0.0),
+                    loglaw_top=cfg.get("loglaw"), median=cfg.get("median", 1e-6),
+                    sigma_g=cfg.get("sigma_g", 1.5), bimodal=cfg.get("bimodal"), zfrac=cfg.get("zfrac", 1.0))
+
+
+def flow_to_ext(grid: dict, flow: dict) -> dict:
+    """Flow-layout device fields -> host arrays in the halo-padded reference
+    layout (``generator.to_ext``), for the oracle."""
+    out = {}
+    for k, f in flow.items():
+        core = f.permute(2, 1, 0).contiguous().cpu().numpy()     # (nnx, nny, nnz+2)
+        out[k] = gen.to_ext(grid, core)
+    return out
+
+
+def droplets_to_host(d: dict) -> dict:
+    """Device droplet dict -> host numpy dict in list order, with lid and
+    the RK3 fields the host layout carries."""
+    n = d["radius"].shape[0]
+    out = {k: v.cpu().numpy() for k, v in d.items()}
+    out["lid"] = np.arange(n, dtype=np.int32)
+    for k in ("xrhs", "vrhs"):
+        out[k] = np.zeros((3, n))
+    for k in ("Tprhs_s", "Tprhs_L", "radrhs"):
+        out[k] = np.zeros(n)
+    return {k: np.ascontiguousarray(v) for k, v in out.items()}
 
 
 _RADVAL = np.array([math.pow(10.0, -8.0 - i * ((-8.0 - (-3.0)) / 1024)) for i in range(1024)])

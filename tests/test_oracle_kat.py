@@ -23,7 +23,7 @@ import pytest
 
 from ntlp_b200 import abi
 from ntlp_b200 import generator as gen
-from helpers import clone, small_case
+from helpers import LIBM_BOUNDS, LIBM_EXACT, LIBM_SOURCE_BOUND, clone, small_case
 
 
 def _ulps(a, b):
@@ -277,23 +277,44 @@ def test_crit_radius_table_search_matches_full_scan():
     assert np.max(np.abs(full2 - fast) / fast) <= 2.3e-16
 
 
-def test_libm_and_shared_math_restatements_agree():
-    """The two oracle builds differ only in which libm they call; after two
-    steps the droplet states agree far below the 1e-9 level, which bounds how
-    much the choice of elementary-function library matters."""
+def libm_differences(case, steps=3):
+    """Per-quantity max relative difference of the two oracle builds after
+    `steps` BE steps, and the sources' differences relative to the largest
+    |contribution|."""
     import pyoracle
-    case = small_case(n=800)
     ext = case.ext()
     a = pyoracle.Oracle(case.grid, case.params, ext, "ntlp")
     b = pyoracle.Oracle(case.grid, case.params, ext, "libm")
     da, db = clone(case.droplets), clone(case.droplets)
-    for it in (1, 2):
-        a.step_be(da, case.dt, it)
-        b.step_be(db, case.dt, it)
-    assert np.array_equal(da["lid"], db["lid"])
-    for k in ("radius", "Tp", "vp", "xp", "qstar"):
-        rel = np.max(np.abs(da[k] - db[k]) / np.abs(db[k]))
-        assert rel < 1e-9, (k, rel)
+    counters_equal = True
+    for it in range(1, steps + 1):
+        ca, _ = a.step_be(da, case.dt, it)
+        cb, _ = b.step_be(db, case.dt, it)
+        counters_equal = counters_equal and ca == cb
+    rel = {}
+    for k in tuple(LIBM_BOUNDS) + LIBM_EXACT:
+        den = np.abs(db[k])
+        rel[k] = float(np.max(np.abs(da[k] - db[k]) / np.where(den > 0, den, 1.0)))
+    sa, aabs = a.coupling(da, case.dt, with_abs=True)
+    sb, _ = b.coupling(db, case.dt, with_abs=True)
+    src = [float(np.max(np.abs(sa[q] - sb[q])) / max(float(np.max(np.abs(aabs[q]))), 1e-300)) for q in range(6)]
+    return counters_equal, np.array_equal(da["lid"], db["lid"]), rel, src
+
+
+@pytest.mark.parametrize("ilin", [0, 1])
+def test_libm_and_shared_math_restatements_agree(ilin):
+    """The two oracle builds differ only in which libm they call.  Counters,
+    list order, interpolated fields and positions agree; radius, Tp, vp and
+    qstar differ at the 1e-11 level (the reference's solve amplifies one-ulp
+    differences of exp/pow), within the stated bounds."""
+    case = small_case(n=5000, params=gen.default_params(ilin=ilin))
+    counters_equal, lid_equal, rel, src = libm_differences(case)
+    assert counters_equal and lid_equal
+    for k in LIBM_EXACT:
+        assert rel[k] == 0.0, (k, rel[k])
+    for k, bound in LIBM_BOUNDS.items():
+        assert rel[k] <= bound, (k, rel[k])
+    assert max(src) <= LIBM_SOURCE_BOUND, src
 
 
 @pytest.mark.parametrize("icase", [0, 1])
@@ -333,3 +354,35 @@ def test_flux_counts_crossings():
     assert pflux[5] == 1.0 and pflux[7] == -1.0
     assert np.count_nonzero(pflux) == 2
     assert pmass[5] > 0 and pmass[7] < 0 and peneg[5] > 0
+
+
+def test_levenberg_marquardt_fallback_solves_the_residual():
+    """A droplet that Gauss-Newton gives up on from the start (1, 1) (solute
+    mass cut by 1e6, q = 0.010, dt = 0.02 s) goes to LV_solver, which
+    returns flag 0 with the cost far below its value at the start."""
+    import pyoracle
+    p = gen.default_params()
+    L = pyoracle.lib("ntlp")
+    ps = abi.make_params_struct(p)
+    r0 = 2e-6
+    m_s = (2.0 / 3.0) * gen.PI2 * (0.5 * r0) ** 3 * 2000.0 * 1e-6
+    Tf, Tp, qinf, rhoa = 293.0, 293.0, 0.010, 1.0
+    uf = (C.c_double * 3)(0.0, 0.0, 0.0)
+    ri = p["radius_init"]      # taup0 of ie_vrt_nd, particles.f90:4279
+    taup0 = ((m_s / ((2.0 / 3.0) * gen.PI2 * ri ** 3) + p["rhow"]) * (ri * 2) ** 2) / (18 * rhoa * p["nuf"])
+    h = 0.02 / taup0
+    start = (C.c_double * 2)(1.0, 1.0)
+    out = (C.c_double * 2)()
+    gn, lm = C.c_int(), C.c_int()
+    flag = L.oracle_newton(C.byref(ps), rhoa, uf, Tf, qinf, m_s, 1.2, r0, Tp, h, start, out, C.byref(gn),
+                           C.byref(lm))
+    assert flag == 0 and lm.value > 0
+    res0, res = (C.c_double * 2)(), (C.c_double * 2)()
+    L.oracle_ie_vrt_nd(C.byref(ps), rhoa, uf, Tf, qinf, m_s, 1.2, r0, Tp, 1.0, 1.0, h, res0)
+    L.oracle_ie_vrt_nd(C.byref(ps), rhoa, uf, Tf, qinf, m_s, 1.2, r0, Tp, out[0], out[1], h, res)
+    # LV_solver accepts a step only when it lowers the cost sum(0.5 f^2)
+    # and stops on a correction below 1e-8, which can come with lambda
+    # grown large before the residual is zero: the cost falls, by orders of
+    # magnitude here, but the returned point is not a root
+    cost = lambda f: math.hypot(0.5 * f[0] * f[0], 0.5 * f[1] * f[1])  # noqa: E731
+    assert cost(res) < 1e-3 * cost(res0)
