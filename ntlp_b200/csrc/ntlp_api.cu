@@ -242,9 +242,7 @@ EncodeTiledFn encode_tiled() {
 
 // TMA descriptor of a mixed box's packed FP32 copy f4 for cell blocks kb
 // cells high: the copy viewed as floats (4*nz2, ny5, nx5), box
-// (4*(kb+9), kBlkWinY, kBlkWinX) -- kb+8 levels used, one more so that the
-// columns' stride in shared memory is an odd number of float4 --, zero fill
-// outside the array
+// (4*(kb+8), kBlkWinY, kBlkWinX), zero fill outside the array
 bool encode_f4_map(DevBox &B, int kb) {
     EncodeTiledFn fn = encode_tiled();
     if (!fn || !B.f4) return false;
@@ -252,7 +250,7 @@ bool encode_f4_map(DevBox &B, int kb) {
     CUtensorMap m;
     const cuuint64_t dims[3] = {4ull * (cuuint64_t)g.nz2, (cuuint64_t)g.ny5, (cuuint64_t)g.nx5};
     const cuuint64_t strides[2] = {16ull * (cuuint64_t)g.nz2, 16ull * (cuuint64_t)g.nz2 * (cuuint64_t)g.ny5};
-    const cuuint32_t box[3] = {4u * (cuuint32_t)(kb + 9), (cuuint32_t)kBlkWinY, (cuuint32_t)kBlkWinX};
+    const cuuint32_t box[3] = {4u * (cuuint32_t)(kb + 8), (cuuint32_t)kBlkWinY, (cuuint32_t)kBlkWinX};
     const cuuint32_t es[3] = {1, 1, 1};
     if (box[0] > 256) return false;
     CUresult r = fn(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)B.f4, dims, strides, box, es,

@@ -112,7 +112,7 @@ constexpr int kF32GuardDev = 8;   // guard elements before the FP32 field copies
 // Cell blocks of the staged 6th-order interpolation (mixed path): kBlkX x
 // kBlkY cell columns, kb cells high (kb from the context's droplet density,
 // a multiple of 4).  The staged node window is (kBlkX+5) x (kBlkY+5) columns
-// of kb+8 levels, starting 4 levels below the block (stored kb+9 apart).
+// of kb+8 levels, starting 4 levels below the block.
 constexpr int kBlkX = 4, kBlkY = 4;
 constexpr int kBlkWinX = kBlkX + 5, kBlkWinY = kBlkY + 5;
 
@@ -121,7 +121,7 @@ enum { ERR_STAGE_WAIT = 1 };   // a staged tile did not arrive within the wait l
 
 struct DevBox {
     // TMA descriptor (CUtensorMap, 128 bytes) of the packed (u, v, T, q)
-    // FP32 copy f4, viewed as floats (4*nz2, ny5, nx5), box (4*(kb+9), 9, 9);
+    // FP32 copy f4, viewed as floats (4*nz2, ny5, nx5), box (4*(kb+8), 9, 9);
     // written by the host when the context is created (mixed boxes)
     alignas(64) unsigned char tmap_f4[128];
     int blk_kb;            // z cells per interpolation block; 0: no staged interpolation

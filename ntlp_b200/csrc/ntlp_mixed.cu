@@ -276,43 +276,95 @@ __device__ __forceinline__ void copy4_async(float *dst, const float *src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
 
-__device__ __noinline__ void interp6_mixed_global(const DevBox &B, double x1, double x2, double x3, Interp &o,
-                                                  int &bad) {
-    interp6_mixed<false>(B, x1, x2, x3, o, bad);
+__device__ __forceinline__ void interp_out(const DevBox &B, int t, const Interp &I, int bad) {
+    const DevState &O = B.st[1 - B.cur];
+    O.uf[0][t] = I.uf[0];
+    O.uf[1][t] = I.uf[1];
+    O.uf[2][t] = I.uf[2];
+    O.Tf[t] = I.Tf;
+    O.qinf[t] = I.qinf;
+    B.key[t] = bad | (I.kw << 1);
 }
 
-// interp6_mixed from the staged window of the block at cells (i0, j0, k0);
-// false (nothing written) when the droplet's stencil is not inside it
+// interp6_mixed from global memory, outputs written (out of line: its
+// locals stay off the staged path)
+__device__ __noinline__ void interp_global_out(const DevBox &B, int t, double x1, double x2, double x3) {
+    Interp I;
+    int bad = 0;
+    interp6_mixed<false>(B, x1, x2, x3, I, bad);
+    interp_out(B, t, I, bad);
+}
+
+// The box fields the staged path reads, copied once per CTA into shared
+// memory (no reloads of the descriptor between the output stores).
+struct StageCtx {
+    double dx, dy, lut_scale;
+    double ref[5];                 // the fields' values at (1, 1, 1), added back in FP64
+    const double *zz, *z;
+    const int *lut_zz, *lut_z;
+    const double *xp[3];
+    const int *perm;
+    double *out[5];                // uf(1:3), Tf, qinf of the output buffer
+    int *key;
+    int ioff, joff, nnx, nny, nnz, nz2, nlut, tables;
+};
+
+// Shared-memory layout of a staged block (KB cells high): the (u, v, T, q)
+// columns KB + 8 float4 apart (the TMA box), the w columns ZSW floats
+// apart.  A warp's lanes are droplets of the block columns yo = 0..3 at one
+// xo, each column's droplets in ascending z; with ZSW = 8 or 24 (mod 32)
+// their w loads of one stencil point fall on different banks.  Measured at
+// 16.8 M droplets on 256^3 (update phase): column strides KB+8 / 24 give
+// 6.22 ms; KB+9 / 24, 6.42; KB+12 / 24, 6.60; KB+16 / 24, 6.29; KB+8 / 40,
+// 6.29; the per-droplet kernel from global memory, 6.34.
+template <int KB> struct StageDims {
+    static constexpr int ZS = KB + 8;
+    static constexpr int ZSW = KB <= 16 ? 24 : 40;
+    static constexpr int NCOL = kBlkWinX * kBlkWinY;
+    static constexpr int NLEV = KB + 8;              // levels k0-4 .. k0+KB+3
+    // vertical tables: zz, z of the levels (clamped to the grid as the
+    // stencil reads them), reciprocal denominators of the windows with
+    // base ku2 in [k0, k0+KB) and kw2 in [k0-1, k0+KB)
+    static constexpr int TAB_BYTES = 2 * NLEV * 8 + (2 * KB + 1) * 6 * 4;
+    static constexpr int BYTES = NCOL * ZS * 16 + NCOL * ZSW * 4 + TAB_BYTES + 128;
+    static_assert((NCOL * ZSW * 4) % 8 == 0, "the FP64 level tables follow the w columns");
+};
+
+// interp6_mixed from the staged window of the block at cells (i0, j0, k0):
+// the contraction's FP32 sums (deviations of u, v, w, T, q) and
+// minloc(z > x3); false (nothing computed) when the droplet's stencil is not
+// inside the window
 template <int KB>
-__device__ __forceinline__ bool interp6_staged(const DevBox &B, const float4 *s4, const float *sw, int i0, int j0,
-                                               int k0, double x1, double x2, double x3, Interp &o) {
-    constexpr int ZS = KB + 9;      // column stride (KB + 8 levels used; odd, to spread the banks)
-    const DevGrid &g = B.g;
-    const int nnz = g.nnz;
-    const int ip3g = ijpt(x1, g.dx), jp3g = ijpt(x2, g.dy);
-    const int ip3 = ip3g - g.ioff, jp3 = jp3g - g.joff;
-    const int ku2 = minloc_zz(g, x3) - 2;
-    const int kw2 = minloc_z(g, x3) - 2;
+__device__ __forceinline__ bool interp6_staged(const StageCtx &C, const float4 *s4, const float *sw,
+                                               const double *s_zz, const double *s_z, const float *s_rzz,
+                                               const float *s_rz, int i0, int j0, int k0, double x1, double x2,
+                                               double x3, float dev[5], int &kw) {
+    constexpr int ZS = StageDims<KB>::ZS, ZSW = StageDims<KB>::ZSW;
+    const int ip3g = ijpt(x1, C.dx), jp3g = ijpt(x2, C.dy);
+    const int ip3 = ip3g - C.ioff, jp3 = jp3g - C.joff;
+    const int ku2 = minloc_lut(C.zz, C.nz2, C.lut_zz, C.nlut, C.lut_scale, x3) - 2;
+    const int kw2 = minloc_lut(C.z, C.nz2, C.lut_z, C.nlut, C.lut_scale, x3) - 2;
     const int xo = ip3 - i0, yo = jp3 - j0, zu = ku2 - k0 + 2, zw = kw2 - k0 + 2;
-    if (ku2 < 0 || ku2 > nnz || kw2 < 0 || kw2 > nnz || g.rden_zz == nullptr || ip3 > g.nnx || jp3 > g.nny ||
-        (unsigned)xo >= (unsigned)kBlkX || (unsigned)yo >= (unsigned)kBlkY || zu < 0 || zu + 6 > KB + 8 || zw < 0 ||
-        zw + 6 > KB + 8)
+    if (kw2 < 0 || ku2 > C.nnz || !C.tables || ip3 > C.nnx || jp3 > C.nny || (unsigned)xo >= (unsigned)kBlkX ||
+        (unsigned)yo >= (unsigned)kBlkY || (unsigned)(ku2 - k0) >= (unsigned)KB || kw2 < k0 - 1 || kw2 >= k0 + KB)
         return false;
-    o.kw = kw2 + 2;
+    kw = kw2 + 2;
     float wx[6], wy[6], wz[6], wzw[6];
-    lagrange6_unif((float)(x1 / g.dx - (double)(ip3g - 3)), wx);
-    lagrange6_unif((float)(x2 / g.dy - (double)(jp3g - 3)), wy);
-    lagrange6_win(x3, g.zz, ku2, g.nz2, g.rden_zz + (ku2 + 2) * 6, wz);
-    lagrange6_win(x3, g.z, kw2, g.nz2, g.rden_z + (kw2 + 2) * 6, wzw);
+    lagrange6_unif((float)(x1 / C.dx - (double)(ip3g - 3)), wx);
+    lagrange6_unif((float)(x2 / C.dy - (double)(jp3g - 3)), wy);
+    // the levels and denominators from the block's tables: the values
+    // lagrange6_win reads from global memory (s_zz[i] = zz(clamped k0-4+i))
+    lagrange6_win(x3, s_zz - (k0 - 4), ku2, 0x40000000, s_rzz + (ku2 - k0) * 6, wz);
+    lagrange6_win(x3, s_z - (k0 - 4), kw2, 0x40000000, s_rz + (kw2 - k0 + 1) * 6, wzw);
     float su = 0.f, sv = 0.f, sw_ = 0.f, sT = 0.f, sq = 0.f;
 #pragma unroll 1
     for (int i = 0; i < 6; ++i) {
-        const int col = ((xo + i) * kBlkWinY + yo) * ZS;
+        const int col = (xo + i) * kBlkWinY + yo;
         float cu_ = 0.f, cv = 0.f, cw_ = 0.f, cT = 0.f, cq = 0.f;
 #pragma unroll
         for (int j = 0; j < 6; ++j) {
-            const float4 *p4 = s4 + col + j * ZS + zu;
-            const float *pw = sw + col + j * ZS + zw;
+            const float4 *p4 = s4 + (col + j) * ZS + zu;
+            const float *pw = sw + (col + j) * ZSW + zw;
             float au = 0.f, av = 0.f, aT = 0.f, aq = 0.f, aw = 0.f;
 #pragma unroll
             for (int k = 0; k < 6; ++k) {
@@ -337,30 +389,20 @@ __device__ __forceinline__ bool interp6_staged(const DevBox &B, const float4 *s4
 #pragma unroll
         for (int r = 0; r < 5; ++r) wx[r] = wx[r + 1];
     }
-    const long long ridx = f32_ref_index(g);
-    o.uf[0] = B.f[0][ridx] + (double)su;
-    o.uf[1] = B.f[1][ridx] + (double)sv;
-    o.uf[2] = B.f[2][ridx] + (double)sw_;
-    o.Tf = B.f[3][ridx] + (double)sT;
-    o.qinf = B.f[4][ridx] + (double)sq;
+    dev[0] = su;
+    dev[1] = sv;
+    dev[2] = sw_;
+    dev[3] = sT;
+    dev[4] = sq;
     return true;
-}
-
-__device__ __forceinline__ void interp_out(const DevBox &B, int t, const Interp &I, int bad) {
-    const DevState &O = B.st[1 - B.cur];
-    O.uf[0][t] = I.uf[0];
-    O.uf[1][t] = I.uf[1];
-    O.uf[2][t] = I.uf[2];
-    O.Tf[t] = I.Tf;
-    O.qinf[t] = I.qinf;
-    B.key[t] = bad | (I.kw << 1);
 }
 
 template <int KB>
 __global__ void __launch_bounds__(kBlockThreads, 4) k_interp_block(DevBox *boxes, const Tile *tiles) {
-    constexpr int ZS = KB + 9;      // staged levels per column (KB + 8 used, + 1 for an odd stride)
+    using D = StageDims<KB>;
+    constexpr int ZS = D::ZS, ZSW = D::ZSW, NLEV = D::NLEV;
     constexpr int NT = kBlockThreads;
-    constexpr int NCOL = kBlkWinX * kBlkWinY;
+    constexpr int NCOL = D::NCOL;
     extern __shared__ unsigned char smem_raw[];
     __shared__ __align__(8) unsigned long long bar;
     __shared__ int s_lo[kBlkX * kBlkY], s_off[kBlkX * kBlkY + 1];
@@ -373,10 +415,7 @@ __global__ void __launch_bounds__(kBlockThreads, 4) k_interp_block(DevBox *boxes
         const int a = B.cell_start[g.ncells], e = B.cell_start[g.ncells + 1];
         for (int t = a + (-1 - tl.start) * NT + (int)threadIdx.x; t < e; t += kOobCtas * NT) {
             const int s = B.perm[t];
-            Interp I;
-            int bad = 0;
-            interp6_mixed_global(B, S.x[0][s], S.x[1][s], S.x[2][s], I, bad);
-            interp_out(B, t, I, bad);
+            interp_global_out(B, t, S.x[0][s], S.x[1][s], S.x[2][s]);
         }
         return;
     }
@@ -410,15 +449,51 @@ __global__ void __launch_bounds__(kBlockThreads, 4) k_interp_block(DevBox *boxes
 
     float4 *s4 = reinterpret_cast<float4 *>(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
     float *swin = reinterpret_cast<float *>(s4 + NCOL * ZS);
+    double *s_zz = reinterpret_cast<double *>(swin + NCOL * ZSW);
+    double *s_z = s_zz + NLEV;
+    float *s_rzz = reinterpret_cast<float *>(s_z + NLEV);   // [KB][6]
+    float *s_rz = s_rzz + KB * 6;                            // [KB+1][6]
     if (threadIdx.x == 0)
         stage_f4(s4, B.tmap_f4, &bar, 4 * (k0 - 4), j0 - 1, i0 - 1, (unsigned)(NCOL * ZS * sizeof(float4)));
-    for (int e = threadIdx.x; e < NCOL * ZS; e += NT) {
-        const int zi = e % ZS, c = e / ZS;
+    for (int e = threadIdx.x; e < NCOL * NLEV; e += NT) {
+        const int zi = e % NLEV, c = e / NLEV;
         const int k = k0 - 4 + zi, ya = j0 - 1 + c % kBlkWinY, xa = i0 - 1 + c / kBlkWinY;
+        float *dst = swin + c * ZSW + zi;
         if (k >= 0 && k < g.nz2 && ya < g.ny5 && xa < g.nx5)
-            copy4_async(swin + e, B.fw + k + (long long)g.nz2 * (ya + (long long)g.ny5 * xa));
+            copy4_async(dst, B.fw + k + (long long)g.nz2 * (ya + (long long)g.ny5 * xa));
         else
-            swin[e] = 0.f;
+            *dst = 0.f;
+    }
+    for (int e = threadIdx.x; e < 2 * NLEV + (2 * KB + 1) * 6; e += NT) {
+        if (e < 2 * NLEV) {
+            const int zi = e % NLEV;
+            const int k = min(max(k0 - 4 + zi, 0), g.nz2 - 1);
+            (e < NLEV ? s_zz : s_z)[zi] = (e < NLEV ? g.zz : g.z)[k];
+        } else if (g.rden_zz != nullptr) {
+            const int r = e - 2 * NLEV;
+            if (r < KB * 6) {
+                const int kb2 = k0 + r / 6;          // window base ku2
+                s_rzz[r] = kb2 <= g.nnz ? g.rden_zz[(kb2 + 2) * 6 + r % 6] : 0.f;
+            } else {
+                const int r2 = r - KB * 6;
+                const int kb2 = k0 - 1 + r2 / 6;     // window base kw2
+                s_rz[r2] = (kb2 >= -2 && kb2 <= g.nnz) ? g.rden_z[(kb2 + 2) * 6 + r2 % 6] : 0.f;
+            }
+        }
+    }
+    __shared__ StageCtx sc;
+    if (threadIdx.x == 0) {
+        const DevState &O = B.st[1 - B.cur];
+        const long long ridx = f32_ref_index(g);
+        sc.dx = g.dx; sc.dy = g.dy; sc.lut_scale = g.lut_scale;
+        for (int q = 0; q < 5; ++q) sc.ref[q] = B.f[q][ridx];
+        sc.zz = g.zz; sc.z = g.z; sc.lut_zz = g.lut_zz; sc.lut_z = g.lut_z;
+        for (int a = 0; a < 3; ++a) sc.xp[a] = S.x[a];
+        sc.perm = B.perm;
+        sc.out[0] = O.uf[0]; sc.out[1] = O.uf[1]; sc.out[2] = O.uf[2]; sc.out[3] = O.Tf; sc.out[4] = O.qinf;
+        sc.key = B.key;
+        sc.ioff = g.ioff; sc.joff = g.joff; sc.nnx = g.nnx; sc.nny = g.nny; sc.nnz = g.nnz; sc.nz2 = g.nz2;
+        sc.nlut = g.nlut; sc.tables = g.rden_zz != nullptr;
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
     __syncthreads();
@@ -427,19 +502,23 @@ __global__ void __launch_bounds__(kBlockThreads, 4) k_interp_block(DevBox *boxes
     ok = __syncthreads_and(ok) != 0;
     if (!ok && threadIdx.x == 0) atomicOr(B.err, ERR_STAGE_WAIT);
 
+    const StageCtx &C = sc;
     for (int q = threadIdx.x; q < total; q += NT) {
         int c = 0;
 #pragma unroll
         for (int h = kBlkX * kBlkY / 2; h > 0; h >>= 1)
             if (s_off[c + h] <= q) c += h;
         const int t = s_lo[c] + (q - s_off[c]);
-        const int s = B.perm[t];
-        const double x1 = S.x[0][s], x2 = S.x[1][s], x3 = S.x[2][s];
-        Interp I;
-        int bad = 0;
-        if (!ok || !interp6_staged<KB>(B, s4, swin, i0, j0, k0, x1, x2, x3, I))
-            interp6_mixed_global(B, x1, x2, x3, I, bad);
-        interp_out(B, t, I, bad);
+        const int s = C.perm[t];
+        const double x1 = C.xp[0][s], x2 = C.xp[1][s], x3 = C.xp[2][s];
+        float dev[5];
+        int kw;
+        if (ok && interp6_staged<KB>(C, s4, swin, s_zz, s_z, s_rzz, s_rz, i0, j0, k0, x1, x2, x3, dev, kw)) {
+            for (int v = 0; v < 5; ++v) C.out[v][t] = C.ref[v] + (double)dev[v];
+            C.key[t] = kw << 1;
+        } else {
+            interp_global_out(B, t, x1, x2, x3);
+        }
     }
     if (!ok) {
         // the tile may still land: wait (bounded) before the shared memory
@@ -450,7 +529,8 @@ __global__ void __launch_bounds__(kBlockThreads, 4) k_interp_block(DevBox *boxes
 }
 
 int interp_block_smem(int kb) {
-    return kBlkWinX * kBlkWinY * (kb + 9) * (int)(sizeof(float4) + sizeof(float)) + 128;
+    return kb == 4 ? StageDims<4>::BYTES
+                   : kb == 16 ? StageDims<16>::BYTES : kb == 32 ? StageDims<32>::BYTES : StageDims<8>::BYTES;
 }
 
 template <int KB>
