@@ -81,14 +81,18 @@ def parse():
     ap.add_argument("--batch-boxes", type=int, default=48)
     ap.add_argument("--batch-steps", type=int, default=50)
     ap.add_argument("--tune-steps", type=int, default=2)
-    ap.add_argument("--serve-jobs", type=int, default=120)
+    ap.add_argument("--serve-jobs", type=int, default=1000)
+    ap.add_argument("--serve-bank", type=int, default=32, help="request-payload bank entries (pinned host)")
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-work-cap", type=float, default=2e7)
     ap.add_argument("--hbm-budget", type=float, default=150e9)
     ap.add_argument("--serve-depth", type=int, default=2)
     ap.add_argument("--serve-priorities", type=int, default=1)
     ap.add_argument("--serve-max-large", type=int, default=1)
-    ap.add_argument("--serve-max-active", type=int, default=4)
+    ap.add_argument("--serve-max-active", type=int, default=2)
+    ap.add_argument("--serve-classes", type=float, nargs="*", default=[2e5, 2e6],
+                    help="droplet counts splitting jobs into size classes that share the device only "
+                         "within a class (empty: no classes)")
     ap.add_argument("--serve-ingest-priority", choices=["job", "high"], default="high")
     ap.add_argument("--skip-errors", action="store_true", help="no error tables (configs[0], [1] and [2])")
     ap.add_argument("--skip-c2", action="store_true", help="no configs[2] section")
@@ -663,18 +667,21 @@ def run_serving(args):
     from ntlp_b200 import serving
     eng = serving.CudaEngine(dt=1e-3, priorities=bool(args.serve_priorities),
                              ingest_priority=args.serve_ingest_priority)
-    jobs = serving.draw_jobs(args.serve_jobs, rate=args.serve_rate, seed=4)
+    jobs = serving.draw_jobs(args.serve_jobs, rate=args.serve_rate, seed=4, bank_size=args.serve_bank)
+    t_stage = time.perf_counter()
     eng.stage(jobs)
+    t_stage = time.perf_counter() - t_stage
+    payload_host_bytes = eng.payload_bytes()
     server = serving.Server(eng, hbm_budget=args.hbm_budget, max_active_droplets=args.serve_work_cap,
                             depth=args.serve_depth, max_active=args.serve_max_active,
-                            max_large=args.serve_max_large if args.serve_max_large > 0 else None)
+                            max_large=args.serve_max_large if args.serve_max_large > 0 else None,
+                            class_bounds=args.serve_classes or None)
     clk = ClockSampler()
     clk.start()
     rep = server.run(jobs, realtime=True, time_limit=600)
     clocks = clk.stop()
     torch.cuda.empty_cache()
     # the same jobs one at a time: per-step slowdowns and result equality
-    eng.stage(jobs)
     cmp = serving.compare_alone(rep, eng.replay_alone(jobs))
     torch.cuda.empty_cache()
     spots = [r["result"]["spot_check"] for r in rep["records"] if "spot_check" in r["result"]]
@@ -693,7 +700,13 @@ def run_serving(args):
             "results_equal_alone_and_mix": cmp["results_equal_alone_and_mix"],
             "peak_admitted_bytes": rep["peak_bytes"], "hbm_budget": args.hbm_budget,
             "peak_active_jobs": rep["peak_active"], "work_cap_droplets": args.serve_work_cap,
-            "spot_checks": spots, "clocks": clocks}
+            "max_active_jobs": args.serve_max_active, "size_classes": args.serve_classes,
+            "spot_checks": spots, "spot_check_jobs": len(spots),
+            "ingest": ("at admission, inside the stream: context creation, the request payload (flow-layout "
+                       "fields and droplet arrays) copied from pinned host memory, the one-step graph recorded"),
+            "payload_bank": {"entries": args.serve_bank, "host_bytes": payload_host_bytes,
+                             "staging_s": t_stage},
+            "clocks": clocks}
 
 
 def cpu_baseline(case, seconds: float, dist=None):

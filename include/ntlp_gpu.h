@@ -190,6 +190,12 @@ void *ntlp_stream(ntlp_ctx *ctx);
  * context's own stream.  Waits for the current stream first.  The caller
  * keeps the stream alive until the context is destroyed or switched back. */
 int ntlp_use_stream(ntlp_ctx *ctx, void *stream);
+/* Replace the context's own stream by a new one of the given scheduling
+ * priority (cudaDeviceGetStreamPriorityRange), after the current work on
+ * it has finished; work issued on a caller's stream (ntlp_use_stream) is
+ * not affected until the context returns to its own.  No counterpart in
+ * the reference.                                                          */
+int ntlp_stream_priority(ntlp_ctx *ctx, int32_t priority);
 /* Mixed precision, 6th order: the interpolation stages each block of cells'
  * field window in shared memory (TMA tile loads) and contracts every
  * droplet's stencil from there.  enable = 0 switches to the per-droplet
@@ -239,6 +245,23 @@ int ntlp_box_sources(ntlp_ctx *ctx, int32_t box, int32_t layout, double *partsrc
  * it is the step counter of the first of them and must be >= 2 (the it <= 1
  * rule vp = uf belongs to an eagerly run first step).  Returns when queued. */
 int ntlp_advance_graph(ntlp_ctx *ctx, double dt, int32_t it, int32_t nsteps);
+/* Record and instantiate the graph that ntlp_advance_graph(ctx, dt, it,
+ * nsteps) replays, without launching it, so that a caller can move the
+ * capture out of a latency-sensitive path (a serving loop builds it at
+ * admission).  No counterpart in the reference.                           */
+int ntlp_graph_build(ntlp_ctx *ctx, double dt, int32_t nsteps);
+/* One particle_update_BE + particle_coupling_update step of every box,
+ * timed on the device: events recorded on the context's stream right
+ * before and after the step's work, inside this call (no host time between
+ * them).  it <= 1 runs eagerly; later steps are one launch of the one-step
+ * graph (built here if ntlp_graph_build has not).  Returns when queued.
+ * ntlp_step_time gives the step's milliseconds once it has completed
+ * (return 0), or returns 1 while it has not.  A slot (0 ..
+ * NTLP_TIMED_SLOTS-1) holds one step until it is reused.  No counterpart in
+ * the reference.                                                          */
+#define NTLP_TIMED_SLOTS 16
+int ntlp_step_timed(ntlp_ctx *ctx, double dt, int32_t it, int32_t slot);
+int ntlp_step_time(ntlp_ctx *ctx, int32_t slot, double *ms);
 /* Autotuner: times each deposition tile shape (NTLP_TUNE_VARIANTS of them:
  * 2x4x32, 4x4x16, 2x2x64 nodes) and each interpolation block size (128, 256) on
  * this context's boxes over `steps` steps (state advances), keeps the

@@ -62,6 +62,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.ntlp_stream.argtypes = [C.c_void_p]
     L.ntlp_stream.restype = C.c_void_p
     L.ntlp_use_stream.argtypes = [C.c_void_p, C.c_void_p]
+    L.ntlp_stream_priority.argtypes = [C.c_void_p, C.c_int32]
     L.ntlp_interp_staging.argtypes = [C.c_void_p, C.c_int32]
     L.ntlp_fields_upload_async.argtypes = [C.c_void_p] + [dp] * 5
     L.ntlp_coupling_async.argtypes = [C.c_void_p, C.c_double, dp, dp, dp, dp]
@@ -97,6 +98,9 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.ntlp_box_counters.argtypes = [C.c_void_p, C.c_int32, P(abi.NtlpCounters)]
     L.ntlp_box_sources.argtypes = [C.c_void_p, C.c_int32, C.c_int32, dp, dp, dp, dp]
     L.ntlp_advance_graph.argtypes = [C.c_void_p, C.c_double, C.c_int32, C.c_int32]
+    L.ntlp_graph_build.argtypes = [C.c_void_p, C.c_double, C.c_int32]
+    L.ntlp_step_timed.argtypes = [C.c_void_p, C.c_double, C.c_int32, C.c_int32]
+    L.ntlp_step_time.argtypes = [C.c_void_p, C.c_int32, P(C.c_double)]
     L.ntlp_autotune.argtypes = [C.c_void_p, C.c_double, C.c_int32, C.c_int32, P(C.c_int32), dp]
     _lib = L
     return L
@@ -219,6 +223,10 @@ class DropletStep:
     def stream_handle(self) -> int:
         """cudaStream_t of the context (for events on the launching stream)."""
         return int(self.L.ntlp_stream(self.h) or 0)
+
+    def stream_priority(self, priority: int):
+        """Give the context a new own stream of this scheduling priority."""
+        self._check(self.L.ntlp_stream_priority(self.h, int(priority)), "ntlp_stream_priority")
 
     def use_stream(self, stream_handle: int | None):
         """Issue this context's work on an external cudaStream_t (None: its own)."""
@@ -476,6 +484,24 @@ class DropletBatch(DropletStep):
         self._check(self.L.ntlp_box_sources(self.h, int(b), int(layout), abi.as_dptr(mom.reshape(-1)),
                                             *(abi.as_dptr(a.reshape(-1)) for a in rest)), "ntlp_box_sources")
         return [mom[0], mom[1], mom[2], rest[0], rest[1], rest[2]]
+
+    def graph_build(self, dt: float, nsteps: int = 1):
+        """Record the nsteps graph of advance_graph without launching it."""
+        self._check(self.L.ntlp_graph_build(self.h, float(dt), int(nsteps)), "ntlp_graph_build")
+
+    def step_timed(self, dt: float, it: int, slot: int):
+        """One BE step + coupling of every box with device events around it
+        (recorded inside the call); read with step_time(slot)."""
+        self._check(self.L.ntlp_step_timed(self.h, float(dt), int(it), int(slot)), "ntlp_step_timed")
+
+    def step_time(self, slot: int):
+        """Milliseconds of the timed step in `slot`, or None while it runs."""
+        ms = C.c_double()
+        r = int(self.L.ntlp_step_time(self.h, int(slot), C.byref(ms)))
+        if r == 1:
+            return None
+        self._check(r, "ntlp_step_time")
+        return ms.value
 
     def advance_graph(self, dt: float, it: int, nsteps: int):
         """nsteps of particle_update_BE + particle_coupling_update for every

@@ -107,6 +107,8 @@ struct ntlp_ctx {
     int dep_variant = 0, nt_variant = 0;
     long long *counters_h = nullptr;   // pinned [nbox][kNumCounters]
     int *err_h = nullptr;              // pinned [nbox] device error words
+    // device-timed steps (ntlp_step_timed): an event pair per slot
+    std::vector<cudaEvent_t> tev;
     // overlapped host copies (ntlp_fields_upload_async, ntlp_coupling_async):
     // a copy stream each way, the flow-layout fields of box 0 staged in
     // up_area until the next step fills the halo from them
@@ -600,6 +602,7 @@ extern "C" void ntlp_ctx_destroy(ntlp_ctx *c) {
         cudaEventDestroy(r.b);
     }
     for (cudaEvent_t e : c->pool) cudaEventDestroy(e);
+    for (cudaEvent_t e : c->tev) cudaEventDestroy(e);
     for (const DevBox &B : c->box) {
         if (B.tex_f4) cudaDestroyTextureObject((cudaTextureObject_t)B.tex_f4);
         for (int q = 0; q < 5; ++q)
@@ -1401,6 +1404,17 @@ int ntlp_sync(ntlp_ctx *c) {
 
 void *ntlp_stream(ntlp_ctx *c) { return c ? (void *)c->stream : nullptr; }
 
+int ntlp_stream_priority(ntlp_ctx *c, int32_t priority) {
+    if (!c) return NTLP_ERR_ARG;
+    CK(cudaStreamSynchronize(c->stream));
+    cudaStream_t s = nullptr;
+    CK(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, priority));
+    if (c->stream == c->own_stream) c->stream = s;
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    c->own_stream = s;
+    return NTLP_OK;
+}
+
 int ntlp_use_stream(ntlp_ctx *c, void *stream) {
     if (!c) return NTLP_ERR_ARG;
     CK(cudaStreamSynchronize(c->stream));
@@ -1603,6 +1617,54 @@ int ntlp_flux(ntlp_ctx *c, double *pflux, double *pmassflux, double *penegflux) 
     return NTLP_OK;
 }
 
+// record the n-step graph (update, sort, finish, deposition per step) and
+// instantiate it, unless the one held matches dt, nsteps and the variants
+static int build_graph(ntlp_ctx *c, double dt, int32_t it, int32_t nsteps) {
+    if (c->gexec && c->g_dt == dt && c->g_nsteps == nsteps && c->g_dep == c->dep_variant &&
+        c->g_nt == c->nt_variant && c->g_blk == c->blk_on)
+        return NTLP_OK;
+    if (c->gexec) {
+        cudaGraphExecDestroy(c->gexec);
+        c->gexec = nullptr;
+    }
+    const bool prof = c->prof;
+    c->prof = false;   // no events inside the capture
+    const int64_t launches = c->launches;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int lrc = NTLP_OK;
+    for (int s = 0; s < nsteps && !lrc; ++s) lrc = launch_step(c, 1, 0, dt, it, true);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+    c->prof = prof;
+    c->g_launches = c->launches - launches;   // kernels in the graph
+    c->launches = launches;
+    if (lrc) {
+        if (graph) cudaGraphDestroy(graph);
+        return lrc;
+    }
+    if (e != cudaSuccess) return fail(c, NTLP_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&c->gexec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        c->gexec = nullptr;
+        return fail(c, NTLP_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(e));
+    }
+    c->g_dt = dt;
+    c->g_nsteps = nsteps;
+    c->g_dep = c->dep_variant;
+    c->g_nt = c->nt_variant;
+    c->g_blk = c->blk_on;
+    return NTLP_OK;
+}
+
+int ntlp_graph_build(ntlp_ctx *c, double dt, int32_t nsteps) {
+    if (!c) return NTLP_ERR_ARG;
+    if (nsteps < 1 || nsteps > 1000) return fail(c, NTLP_ERR_ARG, "nsteps must be in 1..1000");
+    int rc = check_ready(c, dt);
+    if (rc) return rc;
+    return build_graph(c, dt, 2, nsteps);
+}
+
 int ntlp_advance_graph(ntlp_ctx *c, double dt, int32_t it, int32_t nsteps) {
     if (!c) return NTLP_ERR_ARG;
     if (it < 2) return fail(c, NTLP_ERR_ARG, "graph steps need it >= 2 (run the first step eagerly)");
@@ -1610,40 +1672,7 @@ int ntlp_advance_graph(ntlp_ctx *c, double dt, int32_t it, int32_t nsteps) {
     int rc = check_ready(c, dt);
     if (rc) return rc;
     if ((rc = consume_upload(c)) || (rc = wait_download(c))) return rc;
-    if (!c->gexec || c->g_dt != dt || c->g_nsteps != nsteps || c->g_dep != c->dep_variant ||
-        c->g_nt != c->nt_variant || c->g_blk != c->blk_on) {
-        if (c->gexec) {
-            cudaGraphExecDestroy(c->gexec);
-            c->gexec = nullptr;
-        }
-        const bool prof = c->prof;
-        c->prof = false;   // no events inside the capture
-        const int64_t launches = c->launches;
-        CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-        int lrc = NTLP_OK;
-        for (int s = 0; s < nsteps && !lrc; ++s) lrc = launch_step(c, 1, 0, dt, it, true);
-        cudaGraph_t graph = nullptr;
-        cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
-        c->prof = prof;
-        c->g_launches = c->launches - launches;   // kernels in the graph
-        c->launches = launches;
-        if (lrc) {
-            if (graph) cudaGraphDestroy(graph);
-            return lrc;
-        }
-        if (e != cudaSuccess) return fail(c, NTLP_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
-        e = cudaGraphInstantiate(&c->gexec, graph, 0);
-        cudaGraphDestroy(graph);
-        if (e != cudaSuccess) {
-            c->gexec = nullptr;
-            return fail(c, NTLP_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(e));
-        }
-        c->g_dt = dt;
-        c->g_nsteps = nsteps;
-        c->g_dep = c->dep_variant;
-        c->g_nt = c->nt_variant;
-        c->g_blk = c->blk_on;
-    }
+    if ((rc = build_graph(c, dt, it, nsteps))) return rc;
     cudaEvent_t e0 = phase_begin(c);
     CK(cudaGraphLaunch(c->gexec, c->stream));
     phase_end(c, PH_OTHER, e0);
@@ -1651,6 +1680,39 @@ int ntlp_advance_graph(ntlp_ctx *c, double dt, int32_t it, int32_t nsteps) {
     mirror_flip(c, nsteps);
     c->payload_valid = true;
     c->last_dt = dt;
+    return NTLP_OK;
+}
+
+int ntlp_step_timed(ntlp_ctx *c, double dt, int32_t it, int32_t slot) {
+    if (!c) return NTLP_ERR_ARG;
+    if (slot < 0 || slot >= NTLP_TIMED_SLOTS) return fail(c, NTLP_ERR_ARG, "slot %d out of range", slot);
+    int rc = check_ready(c, dt);
+    if (rc) return rc;
+    if (c->tev.empty()) {
+        c->tev.assign(2 * NTLP_TIMED_SLOTS, nullptr);
+        for (auto &e : c->tev) CK(cudaEventCreate(&e));
+    }
+    if ((rc = consume_upload(c))) return rc;
+    CK(cudaEventRecord(c->tev[2 * slot], c->stream));
+    if (it <= 1) {
+        if ((rc = do_step(c, 1, 0, dt, it, nullptr)) || (rc = launch_coupling(c, dt))) return rc;
+    } else if ((rc = ntlp_advance_graph(c, dt, it, 1))) {
+        return rc;
+    }
+    CK(cudaEventRecord(c->tev[2 * slot + 1], c->stream));
+    return NTLP_OK;
+}
+
+int ntlp_step_time(ntlp_ctx *c, int32_t slot, double *ms) {
+    if (!c || !ms) return NTLP_ERR_ARG;
+    if (slot < 0 || slot >= NTLP_TIMED_SLOTS || c->tev.empty())
+        return fail(c, NTLP_ERR_ARG, "no timed step in slot %d", slot);
+    cudaError_t q = cudaEventQuery(c->tev[2 * slot + 1]);
+    if (q == cudaErrorNotReady) return 1;
+    CK(q);
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, c->tev[2 * slot], c->tev[2 * slot + 1]));
+    *ms = t;
     return NTLP_OK;
 }
 

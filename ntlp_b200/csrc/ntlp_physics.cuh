@@ -319,24 +319,30 @@ __device__ __forceinline__ int gauss_newton32(const DevParams &p, const Drop &d,
     k.sc6 = (float)(0.6 * p.Sc13);
     k.pr6 = (float)(0.6 * p.Pra13);
     float va = (float)a, vb = (float)b;
+    // the lanes of the warp that solve iterate together until a vote finds
+    // every one of them finished (converged, or given up); a finished lane
+    // idles through the others' iterations, its result unchanged
+    const unsigned solving = __activemask();
+    int state = 0;   // 0 iterating, 1 converged, -1 given up
     for (int it = 0; it < 10; ++it) {
+        if (!__any_sync(solving, state == 0)) break;
+        if (state != 0) continue;
         float f[2], J[4];
         resid_jac_ad32(k, va, vb, f, J);
         const float det = J[0] * J[3] - J[2] * J[1];
-        if (!(fabsf(det) >= 1.0e-5f)) return 0;   // singular, or NaN
+        if (!(fabsf(det) >= 1.0e-5f)) { state = -1; continue; }   // singular, or NaN
         const float rd = __frcp_rn(det);
         const float c1 = (J[3] * f[0] - J[2] * f[1]) * rd;
         const float c2 = (J[0] * f[1] - J[1] * f[0]) * rd;
         va -= c1;
         vb -= c2;
-        if (!(va >= 0.01f && vb >= 0.01f)) return 0;   // out of range, or NaN
-        if (c1 * c1 + c2 * c2 < 1.0e-10f) {
-            a = (double)va;
-            b = (double)vb;
-            return 1;
-        }
+        if (!(va >= 0.01f && vb >= 0.01f)) { state = -1; continue; }   // out of range, or NaN
+        if (c1 * c1 + c2 * c2 < 1.0e-10f) state = 1;
     }
-    return 0;
+    if (state != 1) return 0;
+    a = (double)va;
+    b = (double)vb;
+    return 1;
 }
 
 // tol: the stopping tolerance on |correction| (1e-8 in gauss_newton_2d).
@@ -346,12 +352,17 @@ __device__ int gauss_newton_ad(const DevParams &p, const Drop &d, const AdConst 
     double v1a = vec1[0], v1b = vec1[1];
     vec2[0] = 0.0;
     vec2[1] = 0.0;
-    while (iterations < 50) {
+    // iterations in step across the warp's solving lanes, ended by a vote
+    // (as in gauss_newton32); each lane's arithmetic and exit rule are its own
+    const unsigned solving = __activemask();
+    bool going = true;
+    while (__any_sync(solving, going && iterations < 50)) {
+        if (!going || iterations >= 50) continue;
         iterations++;
         double fv[2], J[4];
         resid_jac_ad(p, d, k, v1a, v1b, fv, J);
         const double det = J[0] * J[3] - J[2] * J[1];
-        if (fabs(det) < 1.0e-5) { flag = 1; break; }
+        if (fabs(det) < 1.0e-5) { flag = 1; going = false; continue; }
         const double rd = 1.0 / det;
         const double c1 = (J[3] * fv[0] - J[2] * fv[1]) * rd;
         const double c2 = (J[0] * fv[1] - J[1] * fv[0]) * rd;
@@ -366,8 +377,12 @@ __device__ int gauss_newton_ad(const DevParams &p, const Drop &d, const AdConst 
             vec2[1] = v1b - c2 * relax;
             if (counts > 10) break;
         }
-        if (vec2[0] < 0.01 || vec2[1] < 0.01 || ntlp_isnan(vec2[0]) || ntlp_isnan(vec2[1])) { flag = 1; break; }
-        if (sqrt(c1 * c1 + c2 * c2) < tol) break;
+        if (vec2[0] < 0.01 || vec2[1] < 0.01 || ntlp_isnan(vec2[0]) || ntlp_isnan(vec2[1])) {
+            flag = 1;
+            going = false;
+            continue;
+        }
+        if (sqrt(c1 * c1 + c2 * c2) < tol) { going = false; continue; }
         v1a = vec2[0];
         v1b = vec2[1];
     }

@@ -9,15 +9,21 @@ Poisson stream; the server
   contexts (``ntlp_bytes_required``, exact) stay within an HBM budget and
   the droplets in flight stay within a work cap, so that requests arriving
   while others run join as memory and slots free up;
-* builds each admitted job's box on the device on an ingest thread and
-  keeps its fields and droplets resident in its own context for all of its
-  steps (no host round trip between steps);
+* ingests each admitted job on an ingest thread: creates its context,
+  copies the request payload (fields in the flow layout and the droplet
+  arrays, held in pinned host memory like a client's buffers) to the
+  device, and records the job's one-step CUDA graph; the fields and
+  droplets then stay resident in that context for all of the job's steps
+  (no host round trip between steps);
 * lets at most `max_large` large jobs run at once, so that the long kernels
   of large jobs do not fill the GPU while small jobs wait;
 * keeps up to ``depth`` steps of every active job queued on that job's own
   CUDA stream, so steps of different jobs overlap on the device; smaller
   jobs get higher stream priority, so their short steps are not queued
   behind the long ones of large jobs;
+* issues a job's first step eagerly (its it = 1 rule) and every later step
+  as one graph launch, so a step reaches the device whole, without host
+  gaps between its kernels;
 * times every step on the device (events on the job's stream around the
   step) and every job from arrival to completion on the host clock.
 
@@ -52,14 +58,29 @@ class JobSpec:
     steps: int
     seed: int
     spot_check: bool = False
+    payload: int | None = None    # entry of the request-payload bank (None: the job's own)
 
 
 def draw_jobs(n_jobs: int, rate: float = 200.0, edge=(32, 192), droplets=(1e4, 1e7),
-              median=(1e-6, 10e-6), steps=(1, 20), spot_frac: float = 0.01, seed: int = 0) -> list:
+              median=(1e-6, 10e-6), steps=(1, 20), spot_frac: float = 0.01, seed: int = 0,
+              bank_size: int | None = None) -> list:
     """Seeded job stream: exponential inter-arrival times (Poisson process of
     the given rate, first arrival at 0), grid edge and droplet count
     log-uniform over their ranges, radius median uniform, steps uniform;
-    round(spot_frac * n_jobs) jobs (at least one) carry the FP64 spot check."""
+    round(spot_frac * n_jobs) jobs (at least one) carry the FP64 spot check.
+
+    With bank_size, the request payloads (box, droplet count, radius
+    median, seed) are drawn once into a bank of that many entries, with the
+    same distributions, and each job takes an entry uniformly at random, so
+    that the payloads of a long stream fit in host memory."""
+    if bank_size:
+        bank = draw_jobs(bank_size, rate, edge, droplets, median, steps, 0.0, seed + 7919)
+        jobs = draw_jobs(n_jobs, rate, edge, droplets, median, steps, spot_frac, seed)
+        pick = np.random.Generator(np.random.Philox(seed + 104729)).integers(0, bank_size, n_jobs)
+        for j, b in zip(jobs, pick):
+            e = bank[int(b)]
+            j.edge, j.n, j.median, j.seed, j.payload = e.edge, e.n, e.median, e.seed, int(b)
+        return jobs
     rng = np.random.Generator(np.random.Philox(seed))
     gaps = rng.exponential(1.0 / rate, n_jobs)
     arrivals = np.concatenate([[0.0], np.cumsum(gaps[1:])])
@@ -97,8 +118,11 @@ class Server:
 
     def __init__(self, engine, hbm_budget: float = 150e9, max_active: int = 64,
                  max_active_droplets: float = 2e7, depth: int = 2, ingest_workers: int = 3,
-                 max_large: int | None = 1, large: int = 2_000_000):
+                 max_large: int | None = 1, large: int = 2_000_000, class_bounds: tuple | None = None):
         self.max_large = max_large      # cap on concurrently admitted jobs of >= `large` droplets
+        # with class_bounds (droplet counts splitting the jobs into size
+        # classes), jobs share the device only with jobs of their own class
+        self.class_bounds = tuple(class_bounds) if class_bounds else None
         self.large = int(large)
         self.engine = engine
         self.budget = float(hbm_budget)
@@ -142,6 +166,11 @@ class Server:
                     fits_work = used_drops + job.n <= self.max_drops or (used_drops == 0)
                     if self.max_large is not None and job.n >= self.large and n_large >= self.max_large:
                         fits_work = False
+                    if self.class_bounds and (active or ingesting):
+                        cls = self._size_class(job.n)
+                        others = [a.spec.n for a in active] + [j.n for j, _, _ in ingesting.values()]
+                        if any(self._size_class(n) != cls for n in others):
+                            fits_work = False
                     if not (fits_mem and fits_work):
                         if b > self.budget:
                             queue.popleft()
@@ -207,6 +236,9 @@ class Server:
             pool.shutdown(wait=True)
         t_end = time.perf_counter() - t0
         return self._report(records, rejected, admit_order, first_arrival, t_end, peak_bytes, peak_active)
+
+    def _size_class(self, n: int) -> int:
+        return sum(n >= b for b in self.class_bounds)
 
     def _report(self, records, rejected, admit_order, first_arrival, t_end, peak_bytes, peak_active) -> dict:
         steps = [ms for r in records for ms in r["step_ms"]]
@@ -301,21 +333,24 @@ class CudaEngine:
         return s
 
     def _context(self, box, params, prio):
-        # with ingest_priority "high" the upload runs on the ingest thread's
-        # high-priority stream (set-up is not queued behind running steps);
-        # with "job" it runs at the job's own priority (a large job's set-up
-        # does not hold back the steps of small ones).  The steps go to a
-        # stream of the job's priority.
-        stream = self.torch.cuda.Stream(device=self.device, priority=prio)
+        # Each context works on a stream of its own (the library's), never
+        # one from torch's stream pool, which hands the same few streams to
+        # many users: a job's steps then never wait behind another job's
+        # work on a shared stream, and the graph recorded at ingest is
+        # captured on a stream that no other thread uses.  With
+        # ingest_priority "high" the set-up runs at the highest priority
+        # (not queued behind running steps), with "job" at the job's own;
+        # the steps run at the job's priority (small jobs higher).
         ctx = self.ntlp.DropletBatch([box["grid"]], params, [max(box["n"], 1)])
-        if self.ingest_priority == "high":
-            ctx.use_stream(self._ingest_stream().cuda_stream)
-        else:
-            ctx.use_stream(stream.cuda_stream)
+        ctx.stream_priority(self._prio[1] if self.ingest_priority == "high" else prio)
         ctx.box_fill_ext(0, box["flow"], sync=False)
         ctx.set_box_droplets(0, box["droplets"])
-        ctx.use_stream(stream.cuda_stream)      # waits for the upload
-        return ctx, stream
+        ctx.graph_build(self.dt, 1)             # the later steps' graph, recorded at ingest
+        if self.ingest_priority == "high":
+            ctx.stream_priority(prio)           # waits for the set-up
+        else:
+            ctx.sync()
+        return ctx, self.torch.cuda.ExternalStream(ctx.stream_handle, device=self.device)
 
     def _generate(self, job: JobSpec) -> dict:
         from . import devgen
@@ -324,20 +359,45 @@ class CudaEngine:
         box["n"] = job.n
         return box
 
+    @staticmethod
+    def _key(job: JobSpec):
+        return ("bank", job.payload) if job.payload is not None else ("job", job.jid)
+
     def stage(self, jobs: list):
-        """Build the jobs' input boxes in device memory ahead of the stream
-        (the request payloads), so that a job's ingest is its context set-up
-        and upload only."""
+        """The request payloads of the jobs, in pinned host memory, before the
+        stream starts (a client's buffers): generated on the device, copied
+        to pinned host arrays, device copies released.  Jobs that share a
+        payload-bank entry share its arrays.  A job's ingest then copies its
+        payload to the device inside the stream."""
+        torch = self.torch
         for job in jobs:
-            self._payload[job.jid] = self._generate(job)
-        self.torch.cuda.synchronize()
+            key = self._key(job)
+            if key in self._payload:
+                continue
+            box = self._generate(job)
+
+            def pin(t):
+                h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+                h.copy_(t)
+                return h.numpy()
+            host = dict(grid=box["grid"], n=box["n"], flow={k: pin(v) for k, v in box["flow"].items()},
+                        droplets={k: pin(v) for k, v in box["droplets"].items()})
+            del box
+            self._payload[key] = host
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+
+    def payload_bytes(self) -> int:
+        """Host bytes of the staged request payloads."""
+        return int(sum(a.nbytes for h in self._payload.values()
+                       for part in (h["flow"], h["droplets"]) for a in part.values()))
 
     def prepare(self, job: JobSpec):
         torch = self.torch
         # runs on an ingest thread: the contexts are created on the current
         # device, which is per thread
         torch.cuda.set_device(self.device)
-        box = self._payload.pop(job.jid, None)
+        box = self._payload.get(self._key(job))
         if box is None:
             ist = self._ingest_stream()
             with torch.cuda.stream(ist):
@@ -347,33 +407,37 @@ class CudaEngine:
         ctx, stream = self._context(box, self.p_mixed, prio)
         twin = None
         if job.spot_check:
-            twin = self._context(box, self.p_fp64, prio)
+            tctx, _ = self._context(box, self.p_fp64, prio)
+            tctx.use_stream(stream.cuda_stream)
+            twin = (tctx, stream)
         del box
         return dict(job=job, ctx=ctx, stream=stream, twin=twin)
 
     # -- steps --
     def issue_step(self, st: dict, k: int):
-        torch = self.torch
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(st["stream"])
-        st["ctx"].particle_update_BE(self.dt, k + 1, counters=False)
-        st["ctx"].particle_coupling_update(self.dt, download=False)
-        e1.record(st["stream"])
+        """Queue step k + 1 of a job (the first eagerly, for its it = 1
+        rule, later ones as one graph launch), timed by events that the
+        library records around it inside one call (no host time in the
+        window)."""
+        slot = k % 16
+        st["ctx"].step_timed(self.dt, k + 1, slot)
         if st["twin"] is not None:
-            tctx, tstream = st["twin"]
-            tctx.particle_update_BE(self.dt, k + 1, counters=False)
-            tctx.particle_coupling_update(self.dt, download=False)
-            t1 = torch.cuda.Event()
-            t1.record(tstream)
-            return (e0, e1, t1)
-        return (e0, e1, None)
+            # the FP64 twin works on the job's stream after the timed step,
+            # so that its work is not counted in the job's step latency
+            st["twin"][0].step_timed(self.dt, k + 1, slot)
+        return (st, slot)
 
     def done(self, ev) -> bool:
-        return ev[1].query() and (ev[2] is None or ev[2].query())
+        st, slot = ev
+        ms = st["ctx"].step_time(slot)
+        if ms is None or (st["twin"] is not None and st["twin"][0].step_time(slot) is None):
+            return False
+        st.setdefault("_ms", {})[slot] = ms
+        return True
 
     def step_ms(self, ev) -> float:
-        return float(ev[0].elapsed_time(ev[1]))
+        st, slot = ev
+        return float(st["_ms"][slot])
 
     def finish(self, st: dict) -> dict:
         ctx = st["ctx"]
@@ -424,7 +488,8 @@ class CudaEngine:
             ms = []
             for k in range(solo.steps):
                 ev = self.issue_step(st, k)
-                ev[1].synchronize()
+                while not self.done(ev):
+                    time.sleep(0.00005)
                 ms.append(self.step_ms(ev))
             out[job.jid] = (ms, self.finish(st))
         return out
