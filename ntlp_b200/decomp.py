@@ -323,28 +323,31 @@ def owner_of(layout: Layout, x: np.ndarray, y: np.ndarray, dx: float, dy: float)
     return coord(ci, bx, rx) * layout.py + coord(cj, by, ry)
 
 
-def make_ranks(layout: Layout, grid: dict, params: dict, flow_core: dict, droplets: dict, capacity_factor=2.0):
-    """Subdomain contexts of every rank on the current GPU (for runs that
-    emulate the ranks in one process): fields cut with their halos,
-    droplets given to the rank that owns their column (strictly inside its
-    bounds, as read_part_res keeps them)."""
+def make_rank(layout: Layout, rank: int, grid: dict, params: dict, flow_core: dict, droplets: dict,
+              capacity_factor=2.0) -> "Rank":
+    """One rank's subdomain context on the current GPU: its fields cut with
+    their halos, the droplets of its columns (strictly inside its bounds, as
+    read_part_res keeps them), in list order."""
     from . import SubdomainStep
     dx, dy = grid["xl"] / layout.nnx, grid["yl"] / layout.nny
     own = owner_of(layout, droplets["xp"][0], droplets["xp"][1], dx, dy)
-    ranks = []
-    for r in range(layout.size):
-        i0, nx, j0, ny = layout.columns(r)
-        g = dict(grid, nnx=nx, nny=ny)
-        sel = np.nonzero(own == r)[0]
-        d = {k: (np.ascontiguousarray(v[..., sel]) if isinstance(v, np.ndarray) else v) for k, v in droplets.items()}
-        if "lid" in d:
-            d["lid"] = np.arange(sel.size, dtype=np.int32)
-        cap = max(16, int(capacity_factor * max(sel.size, droplets["radius"].shape[0] / layout.size)))
-        st = SubdomainStep(g, params, cap, layout.nnx, layout.nny, i0, j0)
-        st.set_fields_ext(local_ext(flow_core, layout, r))
-        st.set_droplets(d)
-        ranks.append(Rank(layout, r, st))
-    return ranks
+    i0, nx, j0, ny = layout.columns(rank)
+    g = dict(grid, nnx=nx, nny=ny)
+    sel = np.nonzero(own == rank)[0]
+    d = {k: (np.ascontiguousarray(v[..., sel]) if isinstance(v, np.ndarray) else v) for k, v in droplets.items()}
+    if "lid" in d:
+        d["lid"] = np.arange(sel.size, dtype=np.int32)
+    cap = max(16, int(capacity_factor * max(sel.size, droplets["radius"].shape[0] / layout.size)))
+    st = SubdomainStep(g, params, cap, layout.nnx, layout.nny, i0, j0)
+    st.set_fields_ext(local_ext(flow_core, layout, rank))
+    st.set_droplets(d)
+    return Rank(layout, rank, st)
+
+
+def make_ranks(layout: Layout, grid: dict, params: dict, flow_core: dict, droplets: dict, capacity_factor=2.0):
+    """Subdomain contexts of every rank on the current GPU (for runs that
+    emulate the ranks in one process)."""
+    return [make_rank(layout, r, grid, params, flow_core, droplets, capacity_factor) for r in range(layout.size)]
 
 
 def step_local(ranks: list, dt: float, it: int, comm: LocalComm | None = None) -> dict:
@@ -364,6 +367,19 @@ def step_local(ranks: list, dt: float, it: int, comm: LocalComm | None = None) -
     total["numpart"] = sum(r.step.numpart for r in ranks)
     total["emigrants"] = sum(r.last_emigrants for r in ranks)
     return total
+
+
+def step_dist(r: Rank, comm: DistComm, dt: float, it: int) -> dict:
+    """One particle_update_BE + particle_exchange + particle_coupling_update
+    + particle_coupling_exchange of this rank, its neighbours in other
+    processes.  Returns this rank's step counters."""
+    c = r.step.particle_update_BE(dt, it)
+    exchange_droplets_dist(r, comm)
+    r.step.particle_coupling_update(dt, download=False)
+    exchange_halos_dist(r, comm)
+    c = dict(c)
+    c["emigrants"] = r.last_emigrants
+    return c
 
 
 def gather_sources(ranks: list) -> list:

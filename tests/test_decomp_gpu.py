@@ -8,10 +8,16 @@ counters, and the assembled sources agree to 1e-12 of the sum of |terms|
 halos afterwards, the single domain in one list order)."""
 from __future__ import annotations
 
+import os
+import socket
+import subprocess
+import sys
+import tempfile
+
 import numpy as np
 import pytest
 
-from conftest import cuda_available
+from conftest import ROOT, cuda_available
 from helpers import STATE_KEYS, bitwise_equal, clone, max_rel, small_case
 from ntlp_b200 import generator as gen
 
@@ -64,3 +70,53 @@ def test_decomposed_steps_match_the_single_domain(px, py):
     for q in range(6):
         err = np.abs(src[q] - osrc[q])
         assert np.all(err <= 1e-12 * oabs[q] + 1e-300), (q, float(np.max(err / (oabs[q] + 1e-300))))
+
+
+@pytest.mark.parametrize("px,py", [(2, 1), (1, 2)])
+def test_ranks_in_separate_processes_match_the_single_domain(px, py):
+    """The same decomposition with each rank in its own process
+    (tests/decomp_subdomain_worker.py under torch.distributed.run): real
+    subdomain contexts, the exchanges through decomp.DistComm (NCCL when
+    every rank has a GPU, gloo through host memory when they share one).
+    The droplets, counters and sources must equal the single domain's as in
+    the one-process test."""
+    import pyoracle
+    from ntlp_b200 import decomp
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import decomp_subdomain_worker as w
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    with tempfile.TemporaryDirectory() as out:
+        env = dict(os.environ, NTLP_DECOMP_PX=str(px), NTLP_DECOMP_PY=str(py), NTLP_DECOMP_OUT=out,
+                   NCCL_NVLS_ENABLE="0")
+        cmd = ["timeout", "-k", "30", "240", sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+               f"--nproc-per-node={px * py}", "--master-addr=127.0.0.1", f"--master-port={port}",
+               os.path.join(ROOT, "tests", "decomp_subdomain_worker.py")]
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=300, cwd=ROOT, env=env)
+        assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+        parts = [np.load(os.path.join(out, f"rank{k}.npz")) for k in range(px * py)]
+        keys = [str(k) for k in parts[0]["counter_keys"]]
+        counters = sum(p["counters"] for p in parts)
+        g = {k[2:]: np.concatenate([p[k] for p in parts], axis=-1) for k in parts[0].files if k.startswith("d_")}
+        src = [np.zeros((12, 10, 18)) for _ in range(6)]
+        lay = decomp.Layout(12, 10, px, py)
+        for k, p in enumerate(parts):
+            i0, nx, j0, ny = lay.columns(k)
+            for q in range(6):
+                src[q][i0:i0 + nx, j0:j0 + ny, :] = p["sources"][q]
+    c, params = w.case()
+    o = pyoracle.Oracle(c.grid, params, c.ext())
+    od = clone(c.droplets)
+    for it in (1, 2, 3):
+        oc, _ = o.step_be(od, 0.05, it)
+        for k in ("num_destroy", "denum", "actnum", "num100", "numimpos", "neg_qinf", "bad_index"):
+            assert counters[it - 1][keys.index(k)] == oc[k], (it, k)
+    assert counters[:, keys.index("emigrants")].sum() > 20
+    gb, rb = _by_position(g), _by_position(od)
+    bad = {k: max_rel(gb[k], rb[k], 1e-300) for k in STATE_KEYS if k != "lid" and not bitwise_equal(gb[k], rb[k])}
+    assert not bad, bad
+    osrc, oabs = o.coupling(od, 0.05, with_abs=True)
+    for q in range(6):
+        err = np.abs(src[q] - osrc[q])
+        assert np.all(err <= 1e-12 * oabs[q] + 1e-300), q
