@@ -56,10 +56,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 B_D = {"fp64": 248, "mixed": 224}       # algorithmic bytes per droplet
-# DRAM bytes per droplet of the update phase (interpolation + droplet body)
-# measured by ncu at 1M droplets / 128^3 (fields subtracted), used to scale
+# DRAM bytes per droplet of the update phase (k_interp_block + k_be_mixed)
+# measured by ncu at 2M droplets / 128^3 (fields subtracted), used to scale
 # the measured traffic to the bench workload
-NCU_BYTES_PER_DROPLET = {"mixed": 440.0}
+NCU_BYTES_PER_DROPLET = {"mixed": 460.0}
 METRIC = "droplet-updates/s (mixed vs FP64 GPU) at 16M; p50/p99 serving step latency"
 
 
@@ -863,12 +863,12 @@ def main():
                       "block": [128, 256][r["tune"]["block_variant"]]}),
         "gpu_launches": int(r["prof"]["launches"]),
         "roofline": {"bound": "hbm",
-                     "kernel": ("update phase: k_interp_mixed + k_be_mixed + k_be_defer_mixed" if head == "mixed"
+                     "kernel": ("update phase: k_interp_block + k_be_mixed + k_be_defer_mixed" if head == "mixed"
                                 else "update phase: k_interp64 + k_be64 + k_be_defer64"),
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_source": src,
                      "traffic": (NCU_BYTES_PER_DROPLET[head] * n + npad * 5 * sf) if head in NCU_BYTES_PER_DROPLET else None,
-                     "traffic_source": "ncu DRAM bytes at 1M droplets/128^3, scaled per droplet (+ fields)",
+                     "traffic_source": "ncu DRAM bytes at 2M droplets/128^3, scaled per droplet (+ fields)",
                      "alg_bytes_per_launch": alg_update,
                      "step_frac": (step_alg / (r["ms"] / args.steps * 1e-3) / 1e9) / hbm},
         "clocks": r["clocks"],
