@@ -34,7 +34,10 @@ namespace ntlp {
 namespace {
 
 constexpr int kDepCap64 = 640;                                    // droplets staged per tile (FP64)
-constexpr int kDepCapMixed = 1024;                                // droplets staged per tile (mixed)
+constexpr int kDepCapMixed = 768;                                 // droplets staged per tile (mixed)
+// mixed stage: the six source factors of a droplet in FP64 (signs applied,
+// converted once per droplet, not once per node), then fx, fy, fz, mult/dV
+constexpr int kStageD = 6, kStageF = 4;
 
 struct DropVals {
     double x1, x2, x3, D[3], V[3], T0, H0, E1, E2, mult;
@@ -320,7 +323,7 @@ __global__ void k_fold32(DevBox *boxes) {
 
 // shared memory of a tile shape (TX x TY x TZ nodes)
 __host__ __device__ constexpr int dep_smem_bytes(bool mixed, int TX, int TY, int TZ) {
-    return (mixed ? kDepCapMixed * 4 + P32_N * kDepCapMixed * 4 : kDepCap64 * 4 + 14 * kDepCap64 * 8) +
+    return (mixed ? kDepCapMixed * 4 + kDepCapMixed * (kStageD * 8 + kStageF * 4) : kDepCap64 * 4 + 14 * kDepCap64 * 8) +
            (TX + 1) * (TY + 1) * (TZ + 2) * 4 + (TX + 1) * (TY + 1) * 4 + 16;
 }
 
@@ -336,9 +339,9 @@ k_deposit_tiled(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevPar
     extern __shared__ __align__(16) unsigned char sm[];
     constexpr int CAP = MIXED ? kDepCapMixed : kDepCap64;
     // stage: values first (8-byte aligned), then lid, cell starts, column offsets
-    double *s_v = (double *)sm;                                         // FP64: [14][CAP]
-    float *s_f = (float *)sm;                                           // mixed: [P32_N][CAP]
-    int *s_lid = (int *)(sm + (MIXED ? P32_N * CAP * 4 : 14 * CAP * 8));
+    double *s_v = (double *)sm;                                         // FP64: [14][CAP]; mixed: [kStageD][CAP]
+    float *s_f = (float *)(sm + kStageD * CAP * 8);                     // mixed: [kStageF][CAP]
+    int *s_lid = (int *)(sm + (MIXED ? CAP * (kStageD * 8 + kStageF * 4) : 14 * CAP * 8));
     int *s_cs = s_lid + CAP;                                            // [cols][TZ+2], absolute
     int *s_off = s_cs + kDepCols * kDepCSW;                             // [cols] stage offset
     __shared__ int s_total;
@@ -405,11 +408,25 @@ k_deposit_tiled(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevPar
                         v0[q] = B.pay32.f[q][t0];
                         v1[q] = B.pay32.f[q][t1];
                     }
+                    // the factors as contribute32 applies them: -DV, -T0, -H0, +E
+                    const double d0[kStageD] = {-(double)v0[P32_DV0], -(double)v0[P32_DV1], -(double)v0[P32_DV2],
+                                                -(double)v0[P32_T0], -(double)v0[P32_H0], (double)v0[P32_E]};
+                    const double d1[kStageD] = {-(double)v1[P32_DV0], -(double)v1[P32_DV1], -(double)v1[P32_DV2],
+                                                -(double)v1[P32_T0], -(double)v1[P32_H0], (double)v1[P32_E]};
 #pragma unroll
-                    for (int q = 0; q < P32_N; ++q) s_f[q * CAP + k0] = v0[q];
-                    if (two)
+                    for (int q = 0; q < kStageD; ++q) s_v[q * CAP + k0] = d0[q];
+                    s_f[0 * CAP + k0] = v0[P32_FX];
+                    s_f[1 * CAP + k0] = v0[P32_FY];
+                    s_f[2 * CAP + k0] = v0[P32_FZ];
+                    s_f[3 * CAP + k0] = v0[P32_FAC];
+                    if (two) {
 #pragma unroll
-                        for (int q = 0; q < P32_N; ++q) s_f[q * CAP + k1] = v1[q];
+                        for (int q = 0; q < kStageD; ++q) s_v[q * CAP + k1] = d1[q];
+                        s_f[0 * CAP + k1] = v1[P32_FX];
+                        s_f[1 * CAP + k1] = v1[P32_FY];
+                        s_f[2 * CAP + k1] = v1[P32_FZ];
+                        s_f[3 * CAP + k1] = v1[P32_FAC];
+                    }
                 }
             }
             if (!MIXED) {
@@ -447,7 +464,9 @@ k_deposit_tiled(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevPar
             if constexpr (MIXED) {
               if (valid) {
                 for (int q = 0; q < 6; ++q) out[q] = 0.0;
-#pragma unroll
+                // the corner loop stays rolled: a smaller kernel (instruction
+                // fetch was a leading stall)
+#pragma unroll 1
                 for (int o = 0; o < 8; ++o) {
                     const int i = o >> 2, j = (o >> 1) & 1, k = o & 1;
                     const int ckk = iz - k;
@@ -460,10 +479,20 @@ k_deposit_tiled(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevPar
                     if (a == b) continue;
                     double S[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
                     for (int at = a; at < b; ++at) {
-                        float v[P32_N];
-#pragma unroll
-                        for (int q = 0; q < P32_N; ++q) v[q] = s_f[q * CAP + at];
-                        contribute32(p, v, i, j, k, S);
+                        // contribute32 with the factors staged in FP64 (the
+                        // same values, so the same bits)
+                        const float fx = s_f[at], fy = s_f[CAP + at], fz = s_f[2 * CAP + at];
+                        const float wx = i ? fx : 1.0f - fx;
+                        const float wy = j ? fy : 1.0f - fy;
+                        const float wz = k ? fz : 1.0f - fz;
+                        const double c = (double)(wx * wy * wz * s_f[3 * CAP + at]);
+                        if (p.icouple == 1)
+                            for (int a3 = 0; a3 < 3; ++a3) S[a3] = fma(s_v[a3 * CAP + at], c, S[a3]);
+                        if (p.iTcouple == 1) S[3] = fma(s_v[3 * CAP + at], c, S[3]);
+                        if (p.iHcouple == 1) {
+                            S[4] = fma(s_v[4 * CAP + at], c, S[4]);
+                            S[5] = fma(s_v[5 * CAP + at], c, S[5]);
+                        }
                     }
                     for (int q = 0; q < 6; ++q) out[q] += S[q];
                 }
