@@ -87,13 +87,19 @@ def parse():
     ap.add_argument("--serve-work-cap", type=float, default=2e7)
     ap.add_argument("--hbm-budget", type=float, default=150e9)
     ap.add_argument("--serve-depth", type=int, default=2)
-    ap.add_argument("--serve-priorities", type=int, default=1)
+    ap.add_argument("--serve-priorities", type=int, default=0)
+    ap.add_argument("--serve-exclusive", type=float, default=1e6,
+                    help="step work at or above which a job runs with no other job (0: never)")
     ap.add_argument("--serve-max-large", type=int, default=1)
     ap.add_argument("--serve-max-active", type=int, default=2)
-    ap.add_argument("--serve-classes", type=float, nargs="*", default=[2e5, 2e6],
-                    help="droplet counts splitting jobs into size classes that share the device only "
-                         "within a class (empty: no classes)")
-    ap.add_argument("--serve-ingest-priority", choices=["job", "high"], default="high")
+    ap.add_argument("--serve-classes", type=float, nargs="*",
+                    default=[2e4, 3.2e4, 5.2e4, 8.4e4, 1.4e5, 2.2e5, 3.5e5, 5.7e5, 9.1e5, 1.5e6, 2.4e6, 3.8e6,
+                             6.2e6, 9.9e6, 1.6e7],
+                    help="step work (droplets + 0.35 x grid nodes) splitting jobs into size classes that "
+                         "share the device only within a class (empty: no classes)")
+    ap.add_argument("--serve-ingest-priority", choices=["job", "high", "low"], default="low")
+    ap.add_argument("--serve-twins", choices=["mix", "replay"], default="replay",
+                    help="where the FP64 spot-check twins run")
     ap.add_argument("--skip-errors", action="store_true", help="no error tables (configs[0], [1] and [2])")
     ap.add_argument("--skip-c2", action="store_true", help="no configs[2] section")
     ap.add_argument("--err-sample", type=int, default=200_000)
@@ -666,7 +672,7 @@ def run_serving(args):
     import torch
     from ntlp_b200 import serving
     eng = serving.CudaEngine(dt=1e-3, priorities=bool(args.serve_priorities),
-                             ingest_priority=args.serve_ingest_priority)
+                             ingest_priority=args.serve_ingest_priority, twins=args.serve_twins)
     jobs = serving.draw_jobs(args.serve_jobs, rate=args.serve_rate, seed=4, bank_size=args.serve_bank)
     t_stage = time.perf_counter()
     eng.stage(jobs)
@@ -675,16 +681,19 @@ def run_serving(args):
     server = serving.Server(eng, hbm_budget=args.hbm_budget, max_active_droplets=args.serve_work_cap,
                             depth=args.serve_depth, max_active=args.serve_max_active,
                             max_large=args.serve_max_large if args.serve_max_large > 0 else None,
-                            class_bounds=args.serve_classes or None)
+                            class_bounds=args.serve_classes or None,
+                            exclusive_above=args.serve_exclusive if args.serve_exclusive > 0 else None)
     clk = ClockSampler()
     clk.start()
     rep = server.run(jobs, realtime=True, time_limit=600)
     clocks = clk.stop()
     torch.cuda.empty_cache()
     # the same jobs one at a time: per-step slowdowns and result equality
-    cmp = serving.compare_alone(rep, eng.replay_alone(jobs))
+    alone = eng.replay_alone(jobs)
+    cmp = serving.compare_alone(rep, alone)
     torch.cuda.empty_cache()
     spots = [r["result"]["spot_check"] for r in rep["records"] if "spot_check" in r["result"]]
+    spots += [res["spot_check"] for _, res in alone.values() if "spot_check" in res]
     offered = sum(j.n * j.steps for j in jobs) / max(jobs[-1].arrival, 1e-9)
     return {"jobs": rep["jobs"], "rejected": len(rep["rejected"]), "arrival_rate_jobs_per_s": args.serve_rate,
             "offered_droplet_updates_per_s": offered,
@@ -701,6 +710,8 @@ def run_serving(args):
             "peak_admitted_bytes": rep["peak_bytes"], "hbm_budget": args.hbm_budget,
             "peak_active_jobs": rep["peak_active"], "work_cap_droplets": args.serve_work_cap,
             "max_active_jobs": args.serve_max_active, "size_classes": args.serve_classes,
+            "ingest_priority": args.serve_ingest_priority, "spot_check_twins": args.serve_twins,
+            "stream_priorities": bool(args.serve_priorities), "exclusive_above_work": args.serve_exclusive,
             "spot_checks": spots, "spot_check_jobs": len(spots),
             "ingest": ("at admission, inside the stream: context creation, the request payload (flow-layout "
                        "fields and droplet arrays) copied from pinned host memory, the one-step graph recorded"),

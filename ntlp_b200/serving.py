@@ -96,6 +96,13 @@ def draw_jobs(n_jobs: int, rate: float = 200.0, edge=(32, 192), droplets=(1e4, 1
                     steps=int(st[i]), seed=int(seeds[i]), spot_check=i in spot) for i in range(n_jobs)]
 
 
+def job_work(job: JobSpec) -> float:
+    """A step's device work in droplet equivalents: the droplet-proportional
+    kernels plus the grid-proportional ones (deposition, sort), a node
+    costing about 0.35 of a droplet."""
+    return float(job.n) + 0.35 * float(job.edge + 1) ** 3
+
+
 def percentile(v, q) -> float | None:
     return float(np.percentile(np.asarray(v, dtype=np.float64), q)) if len(v) else None
 
@@ -118,11 +125,16 @@ class Server:
 
     def __init__(self, engine, hbm_budget: float = 150e9, max_active: int = 64,
                  max_active_droplets: float = 2e7, depth: int = 2, ingest_workers: int = 3,
-                 max_large: int | None = 1, large: int = 2_000_000, class_bounds: tuple | None = None):
+                 max_large: int | None = 1, large: int = 2_000_000, class_bounds: tuple | None = None,
+                 exclusive_above: float | None = None):
         self.max_large = max_large      # cap on concurrently admitted jobs of >= `large` droplets
-        # with class_bounds (droplet counts splitting the jobs into size
-        # classes), jobs share the device only with jobs of their own class
+        # with class_bounds (step work, job_work(), splitting the jobs into
+        # size classes), jobs share the device only with jobs of their own
+        # class
         self.class_bounds = tuple(class_bounds) if class_bounds else None
+        # jobs whose step work is at least exclusive_above fill the device
+        # alone: they run by themselves (overlap would only time-slice them)
+        self.exclusive_above = exclusive_above
         self.large = int(large)
         self.engine = engine
         self.budget = float(hbm_budget)
@@ -166,10 +178,15 @@ class Server:
                     fits_work = used_drops + job.n <= self.max_drops or (used_drops == 0)
                     if self.max_large is not None and job.n >= self.large and n_large >= self.max_large:
                         fits_work = False
+                    if self.exclusive_above is not None and (active or ingesting):
+                        others = [a.spec for a in active] + [j for j, _, _ in ingesting.values()]
+                        if job_work(job) >= self.exclusive_above or \
+                                any(job_work(o) >= self.exclusive_above for o in others):
+                            fits_work = False
                     if self.class_bounds and (active or ingesting):
-                        cls = self._size_class(job.n)
-                        others = [a.spec.n for a in active] + [j.n for j, _, _ in ingesting.values()]
-                        if any(self._size_class(n) != cls for n in others):
+                        cls = self._size_class(job_work(job))
+                        others = [a.spec for a in active] + [j for j, _, _ in ingesting.values()]
+                        if any(self._size_class(job_work(o)) != cls for o in others):
                             fits_work = False
                     if not (fits_mem and fits_work):
                         if b > self.budget:
@@ -237,8 +254,8 @@ class Server:
         t_end = time.perf_counter() - t0
         return self._report(records, rejected, admit_order, first_arrival, t_end, peak_bytes, peak_active)
 
-    def _size_class(self, n: int) -> int:
-        return sum(n >= b for b in self.class_bounds)
+    def _size_class(self, work: float) -> int:
+        return sum(work >= b for b in self.class_bounds)
 
     def _report(self, records, rejected, admit_order, first_arrival, t_end, peak_bytes, peak_active) -> dict:
         steps = [ms for r in records for ms in r["step_ms"]]
@@ -286,7 +303,8 @@ class CudaEngine:
     (one box) per job, mixed precision; spot-check jobs get an FP64 twin."""
 
     def __init__(self, params: dict | None = None, dt: float = 1e-3, keep_state: bool = False,
-                 priorities: bool = True, spot_keys=("radius", "Tp", "vp", "xp"), ingest_priority: str = "high"):
+                 priorities: bool = True, spot_keys=("radius", "Tp", "vp", "xp"), ingest_priority: str = "high",
+                 twins: str = "mix"):
         import torch
         import ntlp_b200
         self.torch = torch
@@ -300,6 +318,10 @@ class CudaEngine:
         self.priorities = priorities
         self.spot_keys = spot_keys
         self.ingest_priority = ingest_priority
+        # where the FP64 twins of spot-check jobs run: "mix" beside their job
+        # in the stream, "replay" in the alone replay (their work then does
+        # not share the device with other jobs' timed steps)
+        self.twins = twins
         lo, hi = torch.cuda.Stream.priority_range()   # (lowest, highest); numerically hi <= lo
         self._prio = (lo, hi)
         self._local = threading.local()
@@ -339,14 +361,15 @@ class CudaEngine:
         # work on a shared stream, and the graph recorded at ingest is
         # captured on a stream that no other thread uses.  With
         # ingest_priority "high" the set-up runs at the highest priority
-        # (not queued behind running steps), with "job" at the job's own;
+        # (not queued behind running steps), with "low" at the lowest (it
+        # does not hold back running steps), with "job" at the job's own;
         # the steps run at the job's priority (small jobs higher).
         ctx = self.ntlp.DropletBatch([box["grid"]], params, [max(box["n"], 1)])
-        ctx.stream_priority(self._prio[1] if self.ingest_priority == "high" else prio)
+        ctx.stream_priority({"high": self._prio[1], "low": self._prio[0]}.get(self.ingest_priority, prio))
         ctx.box_fill_ext(0, box["flow"], sync=False)
         ctx.set_box_droplets(0, box["droplets"])
         ctx.graph_build(self.dt, 1)             # the later steps' graph, recorded at ingest
-        if self.ingest_priority == "high":
+        if self.ingest_priority in ("high", "low"):
             ctx.stream_priority(prio)           # waits for the set-up
         else:
             ctx.sync()
@@ -406,7 +429,7 @@ class CudaEngine:
         prio = self._priority(job.n)
         ctx, stream = self._context(box, self.p_mixed, prio)
         twin = None
-        if job.spot_check:
+        if job.spot_check and (self.twins == "mix" or getattr(self._local, "replaying", False)):
             tctx, _ = self._context(box, self.p_fp64, prio)
             tctx.use_stream(stream.cuda_stream)
             twin = (tctx, stream)
@@ -480,10 +503,12 @@ class CudaEngine:
     def replay_alone(self, jobs: list) -> dict:
         """Run every job by itself (one at a time, each step waited for) on
         the same inputs: {jid: (step ms list, result)}.  Spot-check twins
-        are not run again."""
+        run here only with twins = "replay" (after each timed step, on the
+        job's stream)."""
         out = {}
+        self._local.replaying = True
         for job in jobs:
-            solo = JobSpec(**{**job.__dict__, "spot_check": False})
+            solo = JobSpec(**{**job.__dict__, "spot_check": job.spot_check and self.twins == "replay"})
             st = self.prepare(solo)
             ms = []
             for k in range(solo.steps):
@@ -492,4 +517,5 @@ class CudaEngine:
                     time.sleep(0.00005)
                 ms.append(self.step_ms(ev))
             out[job.jid] = (ms, self.finish(st))
+        self._local.replaying = False
         return out
