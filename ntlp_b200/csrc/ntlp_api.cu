@@ -1799,7 +1799,7 @@ int ntlp_sub_emigrants(ntlp_ctx *c, ntlp_droplets *d, int32_t *direction) {
     BoxHost &h = c->bh[0];
     const DevBox &B = c->box[0];
     const DevState &S = B.st[B.cur];
-    launch_emig_order(c->box_d, 0, m, h.emig_order_slot, h.emig_order_dir, c->stream);
+    CK(launch_emig_order(c->box_d, 0, m, h.emig_order_slot, h.emig_order_dir, c->stream));
     auto get = [&](const void *src, void *dst, int eb) -> int {
         if (!src || !dst) return NTLP_OK;
         launch_gather_slots(src, eb, h.emig_order_slot, h.staging, m, c->stream);

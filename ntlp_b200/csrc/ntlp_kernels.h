@@ -113,7 +113,8 @@ void launch_pack_f32(const DevBox *host_box, float4 *f4, float *fw, cudaStream_t
 void launch_rank_alive(DevBox *boxes, int box, int *rank_by_lid, int nlid, cudaStream_t st);
 
 // x-y column subdomains (ntlp_subdomain.cu)
-void launch_emig_order(const DevBox *boxes, int box, int m, int *slot_out, int *dir_out, cudaStream_t st);
+// emigrants in send order (direction, then lid) by a radix sort
+cudaError_t launch_emig_order(const DevBox *boxes, int box, int m, int *slot_out, int *dir_out, cudaStream_t st);
 void launch_gather_slots(const void *src, int elem_bytes, const int *slot, void *out, int m, cudaStream_t st);
 void launch_gather_slots_i64(const long long *src, const int *slot, long long *out, int m, cudaStream_t st);
 void launch_shift_existing(DevBox *boxes, int box, int n, int m, const int *rank_by_lid, cudaStream_t st);

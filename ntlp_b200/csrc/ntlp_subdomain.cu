@@ -4,6 +4,8 @@
 // belong to the neighbours (particle_coupling_exchange, :1066-1113).
 #include <cuda_runtime.h>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include "ntlp_dev.cuh"
 #include "ntlp_kernels.h"
 
@@ -26,22 +28,26 @@ __device__ __forceinline__ void copy_droplet(const DevState &A, int i, const Dev
     }
 }
 
-// Position of each emigrant in the send order: by direction, then list
-// order (lid), as particle_exchange fills its eight buffers walking the
-// list.  O(m^2) comparisons, m = emigrants of one step.
-__global__ void k_emig_order(const DevBox *boxes, int box, int m, int *slot_out, int *dir_out) {
+// The send order of the emigrants -- by direction, then list order (lid),
+// as particle_exchange fills its eight buffers walking the list -- by a
+// radix sort of the keys (direction << 31 | lid) carrying the slots.
+constexpr int kEmigKeyBits = 35;   // direction 1..8 above 31 bits of lid
+
+__global__ void k_emig_keys(const DevBox *boxes, int box, int m, unsigned long long *keys, int *vals) {
     const DevBox &B = boxes[box];
     const int *lid = B.st[B.cur].lid;
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= m) return;
-    const int de = B.emig_dir[e], le = lid[B.emig_slot[e]];
-    int r = 0;
-    for (int f = 0; f < m; ++f) {
-        const int df = B.emig_dir[f], lf = lid[B.emig_slot[f]];
-        r += (df < de) || (df == de && lf < le);
-    }
-    slot_out[r] = B.emig_slot[e];
-    dir_out[r] = de;
+    const int slot = B.emig_slot[e];
+    keys[e] = ((unsigned long long)B.emig_dir[e] << 31) | (unsigned long long)(unsigned)lid[slot];
+    vals[e] = slot;
+}
+
+__global__ void k_emig_unpack(const unsigned long long *keys, const int *vals, int m, int *slot_out, int *dir_out) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= m) return;
+    slot_out[r] = vals[r];
+    dir_out[r] = (int)(keys[r] >> 31);
 }
 
 __global__ void k_gather_slots_d(const double *__restrict__ src, const int *__restrict__ slot,
@@ -104,9 +110,25 @@ __global__ void k_halo_add_y(DevBox *boxes, int box, const double *in) {
 
 }  // namespace
 
-void launch_emig_order(const DevBox *boxes, int box, int m, int *slot_out, int *dir_out, cudaStream_t st) {
-    if (m <= 0) return;
-    k_emig_order<<<(m + 255) / 256, 256, 0, st>>>(boxes, box, m, slot_out, dir_out);
+cudaError_t launch_emig_order(const DevBox *boxes, int box, int m, int *slot_out, int *dir_out, cudaStream_t st) {
+    if (m <= 0) return cudaSuccess;
+    size_t temp = 0;
+    cudaError_t e = cub::DeviceRadixSort::SortPairs(nullptr, temp, (const unsigned long long *)nullptr,
+                                                    (unsigned long long *)nullptr, (const int *)nullptr,
+                                                    (int *)nullptr, m, 0, kEmigKeyBits, st);
+    if (e != cudaSuccess) return e;
+    // keys and values in and out, then the sort's own scratch
+    const size_t kb = ((size_t)m * 8 + 255) / 256 * 256, vb = ((size_t)m * 4 + 255) / 256 * 256;
+    unsigned char *buf = nullptr;
+    if ((e = cudaMallocAsync((void **)&buf, 2 * kb + 2 * vb + temp, st)) != cudaSuccess) return e;
+    unsigned long long *k_in = (unsigned long long *)buf, *k_out = (unsigned long long *)(buf + kb);
+    int *v_in = (int *)(buf + 2 * kb), *v_out = (int *)(buf + 2 * kb + vb);
+    k_emig_keys<<<(m + 255) / 256, 256, 0, st>>>(boxes, box, m, k_in, v_in);
+    e = cub::DeviceRadixSort::SortPairs(buf + 2 * kb + 2 * vb, temp, k_in, k_out, v_in, v_out, m, 0, kEmigKeyBits,
+                                        st);
+    if (e == cudaSuccess) k_emig_unpack<<<(m + 255) / 256, 256, 0, st>>>(k_out, v_out, m, slot_out, dir_out);
+    const cudaError_t f = cudaFreeAsync(buf, st);
+    return e != cudaSuccess ? e : f;
 }
 
 void launch_gather_slots(const void *src, int elem_bytes, const int *slot, void *out, int m, cudaStream_t st) {
