@@ -165,12 +165,16 @@ int ntlp_coupling(ntlp_ctx *ctx, double dt, int32_t layout, double *partsrc,
  * read (download) before ntlp_copies_wait or ntlp_sync returns.
  *
  * ntlp_fields_upload_async: the five fields of box 0 in the flow layout of
- * ntlp_fields_upload, copied to a device area; the next step (on the
+ * ntlp_fields_upload, copied to one of two device areas, taken in turn
+ * (each allocated on first use, 40 bytes per point), so the upload for the
+ * next step need not wait for this step's halo fill; the next step (on the
  * context's stream) waits for the copies, then fills the halo and the FP32
  * copies from that area.  A later upload, synchronous or not, replaces it.
- * ntlp_coupling_async: ntlp_coupling in the column layout, its six arrays
- * copied back on the download stream after the deposition; the next
- * deposition waits until that copy has read the device arrays.            */
+ * ntlp_coupling_async: ntlp_coupling in the column layout; after the
+ * deposition the download stream copies the six arrays to a device area
+ * (allocated on first use, 48 bytes per node) and from there to the host,
+ * so the next deposition waits only for the device copy, not for the
+ * transfer to the host.                                                    */
 int ntlp_fields_upload_async(ntlp_ctx *ctx, const double *u, const double *v, const double *w,
                              const double *t, const double *q);
 int ntlp_coupling_async(ntlp_ctx *ctx, double dt, double *partsrc, double *partTsrc, double *partHsrc,

@@ -110,12 +110,23 @@ struct ntlp_ctx {
     // device-timed steps (ntlp_step_timed): an event pair per slot
     std::vector<cudaEvent_t> tev;
     // overlapped host copies (ntlp_fields_upload_async, ntlp_coupling_async):
-    // a copy stream each way, the flow-layout fields of box 0 staged in
-    // up_area until the next step fills the halo from them
+    // a copy stream each way; the flow-layout fields of box 0 staged in one
+    // of two upload areas (in turn) until the next step fills the halo from
+    // it, so an upload need not wait for the previous step's fill; the
+    // sources of box 0 in two sets of arrays, the arena's and src_alt,
+    // deposited into in turn, so a deposition waits only for the download
+    // of the step before last (the set it writes), not for the last one
     cudaStream_t up_stream = nullptr, down_stream = nullptr;
-    cudaEvent_t ev_up = nullptr, ev_fill = nullptr, ev_dep = nullptr, ev_down = nullptr;
-    double *up_area = nullptr;
-    bool up_pending = false, fill_recorded = false, down_pending = false;
+    cudaEvent_t ev_up[2] = {}, ev_fill[2] = {};
+    cudaEvent_t ev_dep = nullptr, ev_down[2] = {};
+    double *up_area[2] = {};
+    int up_next = 0;   // the area the next upload takes
+    int up_cur = 0;    // the area of the pending upload
+    bool up_pending = false, fill_recorded[2] = {};
+    double *src_alt = nullptr;
+    double *src_set[2][6] = {};   // the two sets of box 0's source arrays
+    int src_cur = 0;              // the set box 0's src points to
+    bool down_pending[2] = {};    // a download of set i was queued
     // CUDA graph of nsteps (update + sort + finish + deposit)
     cudaGraphExec_t gexec = nullptr;
     double g_dt = 0.0;
@@ -538,6 +549,11 @@ __global__ void k_gather_lid(const int *__restrict__ perm, const int *__restrict
     out[rank[lid[s]]] = lid[s];
 }
 
+// the six source array pointers of a box, by value
+struct Src6 {
+    double *p[6];
+};
+
 __global__ void k_iota(int *a, int n) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t < n) a[t] = t;
@@ -614,9 +630,12 @@ extern "C" void ntlp_ctx_destroy(ntlp_ctx *c) {
         if (h.arena_stats) cudaFreeAsync(h.arena_stats, c->stream);
     }
     if (c->small_arena) cudaFreeAsync(c->small_arena, c->stream);
-    if (c->up_area) cudaFreeAsync(c->up_area, c->stream);
+    for (double *a : c->up_area)
+        if (a) cudaFreeAsync(a, c->stream);
+    if (c->src_alt) cudaFreeAsync(c->src_alt, c->stream);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    for (cudaEvent_t e : {c->ev_up, c->ev_fill, c->ev_dep, c->ev_down})
+    for (cudaEvent_t e : {c->ev_up[0], c->ev_up[1], c->ev_fill[0], c->ev_fill[1], c->ev_dep, c->ev_down[0],
+                          c->ev_down[1]})
         if (e) cudaEventDestroy(e);
     if (c->up_stream) cudaStreamDestroy(c->up_stream);
     if (c->down_stream) cudaStreamDestroy(c->down_stream);
@@ -938,23 +957,63 @@ int fields_flow(ntlp_ctx *c, int b, const double *const h[5]) {
     return NTLP_OK;
 }
 
-// copy streams, events and the upload area, on first use
+// copy streams and events, on first use
 int async_setup(ntlp_ctx *c) {
     if (!c->up_stream) {
         CK(cudaStreamCreateWithFlags(&c->up_stream, cudaStreamNonBlocking));
         CK(cudaStreamCreateWithFlags(&c->down_stream, cudaStreamNonBlocking));
-        for (cudaEvent_t *e : {&c->ev_up, &c->ev_fill, &c->ev_dep, &c->ev_down})
+        for (cudaEvent_t *e : {&c->ev_up[0], &c->ev_up[1], &c->ev_fill[0], &c->ev_fill[1], &c->ev_dep,
+                               &c->ev_down[0], &c->ev_down[1]})
             CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     }
-    if (!c->up_area) {
-        const DevGrid &g = c->box[0].g;
-        const size_t nflow = (size_t)g.nnx * g.nny * g.nz2;
-        if (pool_alloc(c, (void **)&c->up_area, 5 * nflow * sizeof(double)) != cudaSuccess) {
-            c->up_area = nullptr;
-            return fail(c, NTLP_ERR_NOMEM, "device allocation of the field upload area refused");
-        }
-        c->bytes += (int64_t)(5 * nflow * sizeof(double));
+    return NTLP_OK;
+}
+
+// upload area i (40 bytes per flow-layout point), on first use
+int up_setup(ntlp_ctx *c, int i) {
+    if (c->up_area[i]) return NTLP_OK;
+    const DevGrid &g = c->box[0].g;
+    const size_t nflow = (size_t)g.nnx * g.nny * g.nz2;
+    if (pool_alloc(c, (void **)&c->up_area[i], 5 * nflow * sizeof(double)) != cudaSuccess) {
+        c->up_area[i] = nullptr;
+        return fail(c, NTLP_ERR_NOMEM, "device allocation of a field upload area refused");
     }
+    c->bytes += (int64_t)(5 * nflow * sizeof(double));
+    return NTLP_OK;
+}
+
+// the second set of box 0's source arrays, on first use (set 0 is the
+// arena's, which box 0's src points to until then)
+int src_alt_setup(ntlp_ctx *c) {
+    if (c->src_alt) return NTLP_OK;
+    const DevGrid &g = c->box[0].g;
+    const size_t nsrc = (size_t)g.nz2 * g.sny * g.snx;
+    if (pool_alloc(c, (void **)&c->src_alt, 6 * nsrc * sizeof(double)) != cudaSuccess) {
+        c->src_alt = nullptr;
+        return fail(c, NTLP_ERR_NOMEM, "device allocation of the second source set refused");
+    }
+    c->bytes += (int64_t)(6 * nsrc * sizeof(double));
+    for (int q = 0; q < 6; ++q) {
+        c->src_set[0][q] = c->box[0].src[q];
+        c->src_set[1][q] = c->src_alt + q * nsrc;
+    }
+    c->src_cur = 0;
+    return NTLP_OK;
+}
+
+// points box 0's src (host mirror and device copy, in stream order) at set i
+__global__ void k_point_src(DevBox *boxes, Src6 set) {
+    if (threadIdx.x < 6) boxes[0].src[threadIdx.x] = set.p[threadIdx.x];
+}
+int use_src_set(ntlp_ctx *c, int i) {
+    if (c->src_cur == i) return NTLP_OK;
+    Src6 set;
+    for (int q = 0; q < 6; ++q) set.p[q] = c->src_set[i][q];
+    k_point_src<<<1, 32, 0, c->stream>>>(c->box_d, set);
+    CK(cudaGetLastError());
+    c->launches += 1;
+    for (int q = 0; q < 6; ++q) c->box[0].src[q] = c->src_set[i][q];
+    c->src_cur = i;
     return NTLP_OK;
 }
 
@@ -964,21 +1023,22 @@ int consume_upload(ntlp_ctx *c) {
     if (!c->up_pending) return NTLP_OK;
     const DevBox &B = c->box[0];
     const size_t nflow = (size_t)B.g.nnx * B.g.nny * B.g.nz2;
-    CK(cudaStreamWaitEvent(c->stream, c->ev_up, 0));
-    for (int k = 0; k < 5; ++k) launch_fill_ext(c->up_area + k * nflow, (double *)B.f[k], B.g, c->stream);
+    const int a = c->up_cur;
+    CK(cudaStreamWaitEvent(c->stream, c->ev_up[a], 0));
+    for (int k = 0; k < 5; ++k) launch_fill_ext(c->up_area[a] + k * nflow, (double *)B.f[k], B.g, c->stream);
     if (B.f4) launch_pack_f32(&B, (float4 *)B.f4, (float *)B.fw, c->stream);
     CK(cudaGetLastError());
-    CK(cudaEventRecord(c->ev_fill, c->stream));
+    CK(cudaEventRecord(c->ev_fill[a], c->stream));
     c->launches += B.f4 ? 6 : 5;
-    c->fill_recorded = true;
+    c->fill_recorded[a] = true;
     c->up_pending = false;
     return NTLP_OK;
 }
 
-// the previous asynchronous source download reads the source arrays: the
-// next deposition waits for it
+// an asynchronous download reads the source set the last deposition wrote:
+// work that writes the current set waits for the download of that set
 int wait_download(ntlp_ctx *c) {
-    if (c->down_pending) CK(cudaStreamWaitEvent(c->stream, c->ev_down, 0));
+    if (c->down_pending[c->src_cur]) CK(cudaStreamWaitEvent(c->stream, c->ev_down[c->src_cur], 0));
     return NTLP_OK;
 }
 
@@ -1533,16 +1593,22 @@ int ntlp_fields_upload_async(ntlp_ctx *c, const double *u, const double *v, cons
         if (!h[k]) return fail(c, NTLP_ERR_ARG, "field %d is NULL", k);
     if (!c->box[0].g.periodic)
         return fail(c, NTLP_ERR_STATE, "a subdomain takes its fields with halos (ntlp_fields_upload_ext)");
+    // the two areas in turn; an upload that replaces a pending one (no step
+    // in between) takes the other area as well
+    const int a = c->up_next;
     int rc = async_setup(c);
-    if (rc) return rc;
+    if (rc || (rc = up_setup(c, a))) return rc;
     const DevGrid &g = c->box[0].g;
     const size_t nflow = (size_t)g.nnx * g.nny * g.nz2;
-    // the area is free once the previous upload's halo fill has read it
-    if (c->fill_recorded) CK(cudaStreamWaitEvent(c->up_stream, c->ev_fill, 0));
+    // the area is free once the halo fill of the upload before last has
+    // read it
+    if (c->fill_recorded[a]) CK(cudaStreamWaitEvent(c->up_stream, c->ev_fill[a], 0));
     for (int k = 0; k < 5; ++k)
-        CK(cudaMemcpyAsync(c->up_area + k * nflow, h[k], nflow * sizeof(double), cudaMemcpyDefault,
+        CK(cudaMemcpyAsync(c->up_area[a] + k * nflow, h[k], nflow * sizeof(double), cudaMemcpyDefault,
                            c->up_stream));
-    CK(cudaEventRecord(c->ev_up, c->up_stream));
+    CK(cudaEventRecord(c->ev_up[a], c->up_stream));
+    c->up_cur = a;
+    c->up_next = 1 - a;
     c->up_pending = true;
     c->bh[0].have_fields = true;
     return NTLP_OK;
@@ -1553,17 +1619,22 @@ int ntlp_coupling_async(ntlp_ctx *c, double dt, double *partsrc, double *partTsr
     if (!c) return NTLP_ERR_ARG;
     if (!c->box[0].g.periodic) return fail(c, NTLP_ERR_STATE, "a subdomain returns its sources with ntlp_coupling");
     int rc = coupling_checks(c, dt, NTLP_LAYOUT_COLUMN);
-    if (rc || (rc = async_setup(c)) || (rc = launch_coupling(c, dt))) return rc;
+    if (rc || (rc = async_setup(c)) || (rc = src_alt_setup(c))) return rc;
+    // deposit into the set the previous download does not read (the
+    // deposition then waits for the download of the step before last)
+    if (c->down_pending[c->src_cur] && (rc = use_src_set(c, 1 - c->src_cur))) return rc;
+    if ((rc = launch_coupling(c, dt))) return rc;
     const DevBox &B = c->box[0];
     const size_t nn = (size_t)B.g.nnodes;
     double *host[6] = {partsrc, partsrc ? partsrc + nn : nullptr, partsrc ? partsrc + 2 * nn : nullptr, partTsrc,
                        partHsrc, partTEsrc};
+    // on the download stream, after the deposition
     CK(cudaEventRecord(c->ev_dep, c->stream));
     CK(cudaStreamWaitEvent(c->down_stream, c->ev_dep, 0));
     for (int q = 0; q < 6; ++q)
         if (host[q]) CK(cudaMemcpyAsync(host[q], B.src[q], nn * sizeof(double), cudaMemcpyDefault, c->down_stream));
-    CK(cudaEventRecord(c->ev_down, c->down_stream));
-    c->down_pending = true;
+    CK(cudaEventRecord(c->ev_down[c->src_cur], c->down_stream));
+    c->down_pending[c->src_cur] = true;
     return NTLP_OK;
 }
 

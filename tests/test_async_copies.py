@@ -1,7 +1,7 @@
 """Overlapped host copies (ntlp_fields_upload_async / ntlp_coupling_async)
 against the synchronous calls: the same droplets and sources, bit for bit,
 over steps whose fields change from one step to the next (each step must
-see its own upload)."""
+see its own upload, also when an upload replaces one that no step read)."""
 from __future__ import annotations
 
 import numpy as np
@@ -39,6 +39,8 @@ def test_async_copies_match_synchronous(precision):
         a.particle_update_BE(case.dt, k + 1, counters=False)
         src_a.append([np.asarray(x).copy() for x in a.particle_coupling_update(case.dt)])
     da = a.get_droplets()
+    # a synchronous deposition after the steps (the same sources again)
+    last_a = [np.asarray(x).copy() for x in a.particle_coupling_update(case.dt)]
     a.close()
 
     b = ntlp_b200.DropletStep(g, p, capacity=n)
@@ -48,17 +50,28 @@ def test_async_copies_match_synchronous(precision):
     for pf, f in zip(pinned, flows):
         for k in f:
             pf[k][...] = f[k]
+    # a decoy upload that the next one replaces before any step reads it
+    decoy = {k: torch.empty(v.shape, dtype=torch.float64, pin_memory=True).numpy() for k, v in flows[0].items()}
+    for k in flows[0]:
+        decoy[k][...] = flows[0][k] + (100.0 if k == "T" else 0.5)
     outs = []
     for k in range(len(flows)):
         mom = torch.empty((3,) + shape, dtype=torch.float64, pin_memory=True).numpy()
         rest = [torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy() for _ in range(3)]
         outs.append([mom] + rest)
+        if k == 2:
+            b.fill_ext_async(decoy)
         b.fill_ext_async(pinned[k])
         b.particle_update_BE(case.dt, k + 1, counters=False)
         b.particle_coupling_update_async(case.dt, outs[-1])
     b.sync()
     db = b.get_droplets()
+    # after the overlapped ones, a synchronous call reads the source set that
+    # its own deposition writes
+    last_b = [np.asarray(x).copy() for x in b.particle_coupling_update(case.dt)]
     b.close()
+    for q in range(6):
+        assert bitwise_equal(last_a[q], last_b[q]), q
     for k in STATE_KEYS:
         assert bitwise_equal(da[k], db[k]), k
     for step, (sa, ob) in enumerate(zip(src_a, outs)):
