@@ -56,10 +56,13 @@ constexpr int kBlockThreads = 160;   // threads of a cell-block interpolation CT
 constexpr int kOobBlockTiles = 8;    // tiles per box over the out-of-range bucket
 int interp_block_smem(int kb);       // dynamic shared memory of a cell-block CTA
 void prepare_interp_block();         // kernel attributes, once per device
-// cells per block in z for a droplet density (droplets per cell): about 128
-// droplets per block, a multiple of 4 in 4..32
+// cells per block in z for a droplet density (droplets per cell): about 256
+// droplets per block, one of 4, 8, 16, 32.  Measured at one droplet per cell
+// (16.8 M droplets, 256^3, update phase with 160 threads per CTA): 16 cells
+// 6.06 ms, 8 cells 6.30 ms, 32 cells 6.24 ms; 16 cells with 192, 256 or 288
+// threads 6.26, 6.43, 6.12 ms.
 inline int interp_block_kb(double density) {
-    const double want = 128.0 / (kBlkX * kBlkY * (density > 1e-9 ? density : 1e-9));
+    const double want = 256.0 / (kBlkX * kBlkY * (density > 1e-9 ? density : 1e-9));
     int kb = 4 * (int)(want / 4.0 + 0.5);
     return kb < 4 ? 4 : (kb > 32 ? 32 : (kb > 16 ? 32 : (kb > 8 ? 16 : kb)));
 }
