@@ -446,6 +446,25 @@ __global__ void __launch_bounds__(kBlockThreads, 4) k_interp_block(DevBox *boxes
     __syncthreads();
     const int total = s_off[kBlkX * kBlkY];
     if (total == 0) return;
+    // sorted position of the block's q-th droplet
+    auto locate = [&](int q) {
+        int c = 0;
+#pragma unroll
+        for (int h = kBlkX * kBlkY / 2; h > 0; h >>= 1)
+            if (s_off[c + h] <= q) c += h;
+        return s_lo[c] + (q - s_off[c]);
+    };
+    // the thread's first droplet: its index and position loads are in
+    // flight while the window is staged
+    int tn = 0, sn = 0;
+    double xn1 = 0.0, xn2 = 0.0, xn3 = 0.0;
+    if ((int)threadIdx.x < total) {
+        tn = locate(threadIdx.x);
+        sn = B.perm[tn];
+        xn1 = S.x[0][sn];
+        xn2 = S.x[1][sn];
+        xn3 = S.x[2][sn];
+    }
 
     float4 *s4 = reinterpret_cast<float4 *>(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
     float *swin = reinterpret_cast<float *>(s4 + NCOL * ZS);
@@ -504,13 +523,16 @@ __global__ void __launch_bounds__(kBlockThreads, 4) k_interp_block(DevBox *boxes
 
     const StageCtx &C = sc;
     for (int q = threadIdx.x; q < total; q += NT) {
-        int c = 0;
-#pragma unroll
-        for (int h = kBlkX * kBlkY / 2; h > 0; h >>= 1)
-            if (s_off[c + h] <= q) c += h;
-        const int t = s_lo[c] + (q - s_off[c]);
-        const int s = C.perm[t];
-        const double x1 = C.xp[0][s], x2 = C.xp[1][s], x3 = C.xp[2][s];
+        const int t = tn;
+        const double x1 = xn1, x2 = xn2, x3 = xn3;
+        if (q + NT < total) {
+            // the next droplet's loads, in flight during this one's contraction
+            tn = locate(q + NT);
+            sn = C.perm[tn];
+            xn1 = C.xp[0][sn];
+            xn2 = C.xp[1][sn];
+            xn3 = C.xp[2][sn];
+        }
         float dev[5];
         int kw;
         if (ok && interp6_staged<KB>(C, s4, swin, s_zz, s_z, s_rzz, s_rz, i0, j0, k0, x1, x2, x3, dev, kw)) {
