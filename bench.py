@@ -14,8 +14,9 @@ larger than L2, so no explicit flush is needed between steps.
           library's stream), inputs resident in HBM
   fp64    the FP64 path on the same inputs
   e2e     the same metric through the C ABI with host buffers: each step
-          uploads the five halo-padded fields from pinned host memory and
-          downloads the six source arrays
+          uploads the five fields (flow layout) from pinned host memory and
+          downloads the six source arrays, on the context's copy streams;
+          copy_bound is the time of the same copies alone
   roofline  dominant kernel (the droplet update): algorithmic bytes per
           launch (N*B_d + P_pad*5*s_f) / its event-timed duration, against
           the measured HBM copy bandwidth
@@ -562,14 +563,16 @@ def run_e2e(case, args, dist):
     g = case.grid
     shape = (g["nnx"], g["nny"], g["nnz"] + 2)
     flow = case.flow()
-    pflow = {}
+    pflow, pflow_t = {}, []
     for k, v in flow.items():
         t = torch.empty(v.shape, dtype=torch.float64, pin_memory=True)
         t.numpy()[...] = v
         pflow[k] = t.numpy()
+        pflow_t.append(t)
     del flow
-    outs = [[torch.empty((3,) + shape, dtype=torch.float64, pin_memory=True).numpy()] +
-            [torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy() for _ in range(3)] for _ in range(2)]
+    outs_t = [[torch.empty((3,) + shape, dtype=torch.float64, pin_memory=True)] +
+              [torch.empty(shape, dtype=torch.float64, pin_memory=True) for _ in range(3)] for _ in range(2)]
+    outs = [[t.numpy() for t in o] for o in outs_t]
     nflow = g["nnx"] * g["nny"] * (g["nnz"] + 2)
     nsrc = g["nnx"] * g["nny"] * (g["nnz"] + 2)
     res = {}
@@ -607,7 +610,33 @@ def run_e2e(case, args, dist):
         n1 = s.numpart
         s.close()
         res[mode] = dict(seconds=sec, n0=n0, n1=n1)
-    return dict(res["overlapped"], serial=res["serial"], h2d=5 * nflow * 8, d2h=6 * nsrc * 8)
+    # the bound the copies set: the same bytes between the same pinned host
+    # arrays and device memory, both directions at once, no compute
+    dev = torch.device("cuda", torch.cuda.current_device())
+    d_up = [torch.empty(t.shape, dtype=torch.float64, device=dev) for t in pflow_t]
+    d_dn = [torch.empty(t.shape, dtype=torch.float64, device=dev) for t in outs_t[0]]
+    s_up, s_dn = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def copies(k):
+        with torch.cuda.stream(s_up):
+            for d, h in zip(d_up, pflow_t):
+                d.copy_(h, non_blocking=True)
+        with torch.cuda.stream(s_dn):
+            for h, d in zip(outs_t[k % 2], d_dn):
+                h.copy_(d, non_blocking=True)
+
+    for k in range(max(1, args.warmup)):
+        copies(k)
+    torch.cuda.synchronize()
+    barrier(dist)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        copies(k)
+    torch.cuda.synchronize()
+    copy_sec = max_over_ranks(dist, time.perf_counter() - t0)
+    del d_up, d_dn
+    return dict(res["overlapped"], serial=res["serial"], h2d=5 * nflow * 8, d2h=6 * nsrc * 8,
+                copy_seconds=copy_sec)
 
 
 def run_batch(args, precision: str):
@@ -904,7 +933,13 @@ def main():
                                 "the context's copy streams, overlapping the device's work"),
                        "serial": {"value": 0.5 * (se["n0"] + se["n1"]) * args.steps / se["seconds"] * ws,
                                   "ms_per_step": se["seconds"] / args.steps * 1e3,
-                                  "note": "the same copies, upload-step-download in sequence on one stream"}}
+                                  "note": "the same copies, upload-step-download in sequence on one stream"},
+                       "copy_bound": {"ms_per_step": e2e["copy_seconds"] / args.steps * 1e3,
+                                      "frac": e2e["copy_seconds"] / e2e["seconds"],
+                                      "note": ("the same bytes copied alone, both directions at once on two "
+                                               "streams (torch copies between the same pinned host arrays and "
+                                               "device memory), no compute; frac = that time over the e2e "
+                                               "step time")}}
     if cb:
         line["cpu_baseline"] = cb
     if errors:
