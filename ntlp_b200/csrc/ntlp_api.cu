@@ -653,6 +653,8 @@ void box_geometry(const ntlp_grid &grid, int64_t cap, DevBox &B) {
     g.nz2 = grid.nnz + 2; g.ny5 = grid.nny + 5; g.nx5 = grid.nnx + 5;
     g.dx = grid.xl / grid.nnx;   // les.F:5491
     g.dy = grid.yl / grid.nny;   // les.F:5492
+    g.rdx = 1.0 / g.dx;
+    g.rdy = 1.0 / g.dy;
     g.xl = grid.xl; g.yl = grid.yl; g.zl = grid.zl;
     g.ncells = (long long)(grid.nnx + 1) * (grid.nny + 1) * (grid.nnz + 1);
     g.nnodes = (long long)g.nz2 * grid.nny * grid.nnx;
@@ -678,6 +680,8 @@ void subdomain_geometry(const ntlp_grid &grid, const ntlp_subdomain &sd, DevBox 
     DevGrid &g = B.g;
     g.dx = grid.xl / sd.nnx_g;
     g.dy = grid.yl / sd.nny_g;
+    g.rdx = 1.0 / g.dx;
+    g.rdy = 1.0 / g.dy;
     g.periodic = 0;
     g.ioff = sd.i0;
     g.joff = sd.j0;

@@ -37,6 +37,7 @@ struct DevGrid {
     int nnx, nny, nnz;
     int nz2, ny5, nx5;     // nnz+2, nny+5, nnx+5
     double dx, dy, xl, yl, zl;
+    double rdx, rdy;       // 1/dx, 1/dy
     const double *z, *zz, *dzw, *dzu;
     long long ncells;      // (nnx+1)(nny+1)(nnz+1)
     long long nnodes;      // (nnz+2)*nny*nnx

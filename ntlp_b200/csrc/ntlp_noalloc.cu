@@ -14,8 +14,7 @@
 // Host code cannot use g_scratch's name as a device address (in host code it
 // names a host-side stand-in).  The first call on each device, with that
 // device current, asks the runtime for the address with
-// cudaGetSymbolAddress and caches it; that first call should therefore come
-// before any stream capture.  Every call on a device shares the array, which
+// cudaGetSymbolAddress and caches it.  Every call on a device shares the array, which
 // keeps the previous call's contents: the counters that must start at zero
 // are cleared on every call, and calls whose work overlaps on the GPU race
 // with each other.
@@ -155,6 +154,7 @@ extern "C" int ntlp_coupling_noalloc(const ntlp_grid *grid, const ntlp_params *p
     g.nnx = grid->nnx; g.nny = grid->nny; g.nnz = grid->nnz;
     g.nz2 = nz2; g.ny5 = grid->nny + 5; g.nx5 = grid->nnx + 5;
     g.dx = grid->xl / grid->nnx; g.dy = grid->yl / grid->nny;
+    g.rdx = 1.0 / g.dx; g.rdy = 1.0 / g.dy;
     g.xl = grid->xl; g.yl = grid->yl; g.zl = grid->zl;
     g.ncells = ncells; g.nnodes = nnodes;
     g.periodic = 1;

@@ -674,18 +674,21 @@ __device__ __forceinline__ void write_payload_mixed(const DevBox &B, const DevPa
     const double Tprhs_s = (Tp - Tpold) * inv_dt - Tprhs_L;
     const double rhoa =
         (p.iexner == 1) ? func_p_base64(p, p.surf_p, p.tsfcc1, x[2]) / p.Rd / Tf : p.surf_rho;
-    const float rf = (float)r, rhoaf = (float)rhoa, pi2 = (float)p.pi2, rhow = (float)p.rhow;
+    const float rf = (float)r, pi2 = (float)p.pi2, rhow = (float)p.rhow;
+    const float irhoa = 1.0f / (float)rhoa;
     const float volp = (float)(p.pi2 * 2.0 / 3.0) * (rf * rf * rf);
-    const float rhop = ((float)m_s + volp * rhow) / volp;
-    const float partmass = rhop * volp;
-    const float taup_i = 18.0f * rhoaf * (float)p.nuf / rhop / ((2.0f * rf) * (2.0f * rf));
-    const float H0 = rhow / rhoaf * pi2 * 2.0f * (rf * rf) * (float)radrhs;
+    // partmass = rhop*Volp = m_s + Volp*rhow; the reference's heat factor
+    // Tprhs_s*6*rhow/rhop/CpaCpp/taup_i*(pi2/2)*r*nuf with taup_i =
+    // 18*rhoa*nuf/rhop/(2r)^2 is Tprhs_s*Volp*rhow/(CpaCpp*rhoa) (rhop and
+    // nuf cancel): the same quantities without their divides
+    const float partmass = (float)m_s + volp * rhow;
+    const float H0 = rhow * irhoa * pi2 * 2.0f * (rf * rf) * (float)radrhs;
     float *const *f = B.pay32.f;
-    f[P32_FX][t] = (float)((x[0] - g.dx * (double)(ipt + g.ioff - 1)) / g.dx);
-    f[P32_FY][t] = (float)((x[1] - g.dy * (double)(jpt + g.joff - 1)) / g.dy);
-    f[P32_FZ][t] = (float)((x[2] - g.zz[kpt]) / g.dzu[kpt + 1]);
-    for (int a = 0; a < 3; ++a) f[P32_DV0 + a][t] = partmass / rhoaf * (vrhs[a] - (float)p.g[a]) + H0 * (float)v[a];
-    f[P32_T0][t] = (float)Tprhs_s * 6.0f * rhow / rhop / (float)p.CpaCpp / taup_i * (pi2 / 2.0f) * rf * (float)p.nuf;
+    f[P32_FX][t] = (float)((x[0] - g.dx * (double)(ipt + g.ioff - 1)) * g.rdx);
+    f[P32_FY][t] = (float)((x[1] - g.dy * (double)(jpt + g.joff - 1)) * g.rdy);
+    f[P32_FZ][t] = (float)(x[2] - g.zz[kpt]) / (float)g.dzu[kpt + 1];
+    for (int a = 0; a < 3; ++a) f[P32_DV0 + a][t] = partmass * irhoa * (vrhs[a] - (float)p.g[a]) + H0 * (float)v[a];
+    f[P32_T0][t] = (float)Tprhs_s * volp * (float)(p.rhow / p.CpaCpp) * irhoa;
     f[P32_H0][t] = H0;
     f[P32_E][t] = H0 * (float)(p.Cpv / p.Cpa) * (float)(Tf - Tp);
     f[P32_FAC][t] = (float)((double)mult / (g.dx * g.dy * g.dzu[kpt + 1]));
