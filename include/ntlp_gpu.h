@@ -383,8 +383,9 @@ int ntlp_crit_radius(const ntlp_params *params, int64_t n, const double *m_s,
  * allocating routine; its working memory is one static device array of
  * about 24 MB that every GPU loading the library holds until exit, which
  * bounds the sizes below (larger inputs return NTLP_ERR_CAPACITY).  The
- * first call on a device looks up that array's address; all calls share
- * the array, so calls whose work overlaps on the GPU race.  Work is queued on `stream` (a cudaStream_t, NULL for the
+ * first call on a device looks up that array's address (make that first
+ * call before any stream capture); all calls share the array, so calls
+ * whose work overlaps on the GPU race.  Work is queued on `stream` (a cudaStream_t, NULL for the
  * default stream); the outputs are ready when that stream reaches them.    */
 #define NTLP_NOALLOC_MAX_DROPLETS 131072
 #define NTLP_NOALLOC_MAX_CELLS    1048576   /* (nnx+1)*(nny+1)*(nnz+1) */

@@ -14,7 +14,8 @@
 // Host code cannot use g_scratch's name as a device address (in host code it
 // names a host-side stand-in).  The first call on each device, with that
 // device current, asks the runtime for the address with
-// cudaGetSymbolAddress and caches it.  Every call on a device shares the array, which
+// cudaGetSymbolAddress and caches it; that first call should come before
+// any stream capture.  Every call on a device shares the array, which
 // keeps the previous call's contents: the counters that must start at zero
 // are cleared on every call, and calls whose work overlaps on the GPU race
 // with each other.
