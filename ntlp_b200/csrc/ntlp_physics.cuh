@@ -272,7 +272,9 @@ __device__ __forceinline__ void resid_jac_ad32(const AdConst32 &k, float a, floa
     const float E = k.k_e1 * (k.inv_Tf - iTn) + g * iTn - solterm;
     const float E_a = g_a * iTn - solterm_a;
     const float E_b = (g - k.k_e1) * iTn_b;
-    const float qstr = k.k_q * iTn * expf(E);
+    // the FP32 phase only brings the point near the root (the FP64 step
+    // that follows fixes it): the fast exponential suffices
+    const float qstr = k.k_q * iTn * __expf(E);
     const float qstr_a = qstr * E_a;
     const float qstr_b = qstr * (E_b - k.Tp * iTn);
     const float dq = k.qinf - qstr;
@@ -464,25 +466,30 @@ __device__ double rad_solver2_64(const DevParams &p, double Tf, double qinf, dou
 // Mixed path: the same equilibrium guess in FP32.  It only starts the
 // Newton iteration, which then converges to the same root under the same
 // stopping rule; a branch that flips near M = 0 changes the start, not the
-// root.
+// root.  So the constant divides are multiplies by their reciprocals, the
+// two divides by lg one reciprocal, and the cosines the fast hardware
+// approximation (absolute error near 2^-21 over [-pi, pi]).
 __device__ double rad_solver2_32(const DevParams &p, double Tf, double qinf, double rhoa, double m_s,
                                  double kap, double radius, double esa, int &mflag) {
     mflag = 0;
     const float pi2 = (float)p.pi2;
     const float lg = logf((float)Tf * (float)rhoa * (float)qinf / ((float)esa * (float)p.m_q));
-    const float a = -((float)p.m_g / (float)Tf) / lg;
-    const float c = (float)(kap * m_s) / ((float)((2.0 / 3.0) * p.pi2 * p.rhos) * lg);
-    const float Q = (a * a) / 9.0f;
-    const float R = (2.0f * a * a * a + 27.0f * c) / 54.0f;
+    const float ilg = 1.0f / lg;
+    const float a = -((float)p.m_g / (float)Tf) * ilg;
+    const float c = (float)(kap * m_s) * (float)(1.0 / ((2.0 / 3.0) * p.pi2 * p.rhos)) * ilg;
+    const float Q = (a * a) * (1.0f / 9.0f);
+    const float R = (2.0f * a * a * a + 27.0f * c) * (1.0f / 54.0f);
     const float M = R * R - Q * Q * Q;
+    const float a3 = a * (1.0f / 3.0f);
     float guess;
     if (M < 0.0f) {
-        const float theta = acosf(fminf(fmaxf(R / sqrtf(Q * Q * Q), -1.0f), 1.0f));
-        guess = -(2.0f * sqrtf(Q) * cosf((theta - pi2) / 3.0f)) - a / 3.0f;
-        if (guess < 0.0f) guess = -(2.0f * sqrtf(Q) * cosf((theta + pi2) / 3.0f)) - a / 3.0f;
+        const float theta = acosf(fminf(fmaxf(R * rsqrtf(Q * Q * Q), -1.0f), 1.0f));
+        const float sQ2 = 2.0f * sqrtf(Q);
+        guess = -(sQ2 * __cosf((theta - pi2) * (1.0f / 3.0f))) - a3;
+        if (guess < 0.0f) guess = -(sQ2 * __cosf((theta + pi2) * (1.0f / 3.0f))) - a3;
     } else {
         const float S = -copysignf(1.0f, R) * cbrtf(fabsf(R) + sqrtf(M));
-        guess = S + Q / S - a / 3.0f;
+        guess = S + Q / S - a3;
         if (guess < 0.0f) {
             mflag = 1;
             return radius;
