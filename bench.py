@@ -60,7 +60,7 @@ B_D = {"fp64": 248, "mixed": 224}       # algorithmic bytes per droplet
 # DRAM bytes per droplet of the update phase (k_interp_block + k_be_mixed)
 # measured by ncu at 2M droplets / 128^3 (fields subtracted), used to scale
 # the measured traffic to the bench workload
-NCU_BYTES_PER_DROPLET = {"mixed": 460.0}
+NCU_BYTES_PER_DROPLET = {"mixed": 465.0}
 METRIC = "droplet-updates/s (mixed vs FP64 GPU) at 16M; p50/p99 serving step latency"
 
 
