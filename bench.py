@@ -101,10 +101,10 @@ def parse():
     ap.add_argument("--serve-ingest-priority", choices=["job", "high", "low"], default="low")
     ap.add_argument("--serve-twins", choices=["mix", "replay"], default="replay",
                     help="where the FP64 spot-check twins run")
-    ap.add_argument("--skip-errors", action="store_true", help="no error tables (configs[0], [1] and [2])")
-    ap.add_argument("--skip-c2", action="store_true", help="no configs[2] section")
+    ap.add_argument("--skip-errors", action="store_true", help="no error tables (the 1M-droplet 128^3 case, the 16.8M-droplet 256^3 case, the spray case)")
+    ap.add_argument("--skip-c2", action="store_true", help="no section for the spray case (67M droplets, 512x512x128 stretched)")
     ap.add_argument("--err-sample", type=int, default=200_000)
-    ap.add_argument("--c2-n", type=int, default=None, help="droplets of the configs[2] section (default: its 67M)")
+    ap.add_argument("--c2-n", type=int, default=None, help="droplets of the spray-case section (default: 67,108,864)")
     ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
                     help="run one precision only (profiling)")
     return ap.parse_args()
@@ -405,7 +405,7 @@ def gpu_run(grid, params, precision, droplets, dt, steps, ext=None, flow=None):
 
 
 def run_errors_c1(case, ctx_mixed, ctx_fp64, args):
-    """the mixed path against the FP64 path over all droplets
+    """The 16.8M-droplet 256^3 case: the mixed path against the FP64 path over all droplets
     (the two timed contexts, after the same steps), and both against the
     oracle on a sample of the same droplets and fields run from it = 1."""
     import torch
@@ -437,7 +437,7 @@ def ctx_steps(args) -> int:
 
 
 def run_c0(args):
-    """configs[0] in full (1,000,000 droplets, 128^3, dt = 1e-3 s, 10
+    """The 1M-droplet case in full (1,000,000 droplets, 128^3, dt = 1e-3 s, 10
     steps): the FP64 and mixed GPU paths against the oracle, which is also
     timed here on the host cores, update and deposition every step (the
     designated CPU configuration)."""
@@ -460,7 +460,7 @@ def run_c0(args):
     cpu_s = ot["update_s"] + ot["deposit_s"]
     out["cpu"] = {"value": n * case.steps / cpu_s, "unit": "droplet-updates/s", "cores": ot["threads"],
                   "mpi_ranks": 0, "kind": "port",
-                  "sample": (f"configs[0] in full: {case.steps} steps of {n} droplets, BE update on "
+                  "sample": (f"the 1M-droplet 128^3 case in full: {case.steps} steps of {n} droplets, BE update on "
                              f"{ot['threads']} OpenMP threads {ot['update_s']:.2f} s, serial list-order "
                              f"deposition {ot['deposit_s']:.2f} s")}
     out["seconds"] = time.perf_counter() - t0
@@ -468,7 +468,7 @@ def run_c0(args):
 
 
 def run_c2(args, dist):
-    """configs[2], the spray-like case in full: 67,108,864 droplets (bimodal
+    """The spray-like case in full: 67,108,864 droplets (bimodal
     3/40 um, bottom 20%) on the stretched 512x512x128 grid, generated in
     device memory; 3 warm-up and 10 timed steps of the mixed path
     (update + coupling), the FP64 path over the same steps, and the mixed
@@ -539,7 +539,7 @@ def run_c2(args, dist):
     for s in ctxs.values():
         s.close()
     res["mixed_over_fp64"] = res["mixed"]["value"] / res["fp64"]["value"]
-    res["workload"] = (f"configs[2]: {n} droplets (bimodal 3/40 um, bottom 20%), 512x512x128 stretched 1.02, "
+    res["workload"] = (f"spray case: {n} droplets (bimodal 3/40 um, bottom 20%), 512x512x128 stretched 1.02, "
                        f"log-law wind, dt={dt}, {warm} warm-up + {steps} timed steps, ilin={args.ilin}, "
                        "inputs generated in device memory")
     res["seconds"] = time.perf_counter() - t_all

@@ -1,10 +1,10 @@
 """Parity on the benchmark configurations at their own grid sizes.
 
-* configs[0] in full: 1,000,000 droplets on the 128^3 grid, dt = 1e-3 s,
+* The 1M-droplet case in full: 1,000,000 droplets on the 128^3 grid, dt = 1e-3 s,
   10 steps of particle_update_BE with 6th-order interpolation, then the
   coupling; the FP64 path against the oracle, bit for bit (every droplet
   quantity, every counter of every step, the six source arrays).
-* The spray grid of configs[2]: 512x512x128 with the vertical spacing
+* The spray case's grid: 512x512x128 with the vertical spacing
   stretched by 1.02 from the surface, log-law wind, lapse rate, bimodal
   radius, droplets in the bottom 20%: 2,000,000 droplets (of its 67 M) for
   two steps, FP64 bit for bit and mixed within the stated tolerances.  This
