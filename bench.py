@@ -238,9 +238,10 @@ def run_device(case, precision: str, args, dist, rank, keep: bool = False):
     tune = None
     if args.tune_steps > 0:
         # the library's autotuner on this box (deposition tile shape,
-        # interpolation block size); untimed, like the warm-up
+        # droplet block size, interpolation block height); untimed, like the
+        # warm-up
         tune = s.autotune(case.dt, it, steps=args.tune_steps)
-        it += 5 * (args.tune_steps + 1)
+        it += tune["steps_advanced"]
     s.sync()
     n0 = s.numpart
     s.profile(True)
@@ -470,7 +471,7 @@ def run_c0(args):
 def run_c2(args, dist):
     """The spray-like case in full: 67,108,864 droplets (bimodal
     3/40 um, bottom 20%) on the stretched 512x512x128 grid, generated in
-    device memory; 3 warm-up and 10 timed steps of the mixed path
+    device memory; 3 warm-up steps, the autotuner, and 10 timed steps of the mixed path
     (update + coupling), the FP64 path over the same steps, and the mixed
     path's errors against it."""
     import torch
@@ -487,6 +488,7 @@ def run_c2(args, dist):
     dt, steps, warm = cfg["dt"], cfg["steps"], 3
     res = {}
     ctxs = {}
+    extra, tune = 0, None
     for prec in ("mixed", "fp64"):
         p = dict(params, precision=abi.NTLP_PREC_MIXED if prec == "mixed" else abi.NTLP_PREC_FP64)
         s = ntlp_b200.DropletStep(grid, p, capacity=n)
@@ -498,6 +500,18 @@ def run_c2(args, dist):
             s.particle_update_BE(dt, it, counters=False)
             s.particle_coupling_update(dt, download=False)
             it += 1
+        if prec == "mixed" and args.tune_steps > 0:
+            # the mixed path autotuned (untimed); the FP64 path then takes as
+            # many plain steps, so the two compare after the same steps
+            s.sync()
+            tune = s.autotune(dt, it, steps=args.tune_steps)
+            extra = tune["steps_advanced"]
+            it += extra
+        elif extra:
+            for _ in range(extra):
+                s.particle_update_BE(dt, it, counters=False)
+                s.particle_coupling_update(dt, download=False)
+                it += 1
         s.sync()
         n0 = s.numpart
         s.profile(True)
@@ -525,6 +539,9 @@ def run_c2(args, dist):
                      "numpart": [int(n0), int(n1)], "device_bytes": s.device_bytes}
         if clocks:
             res[prec]["clocks"] = clocks
+        if prec == "mixed" and tune:
+            res[prec]["autotune"] = {"deposit_shape": ["2x4x32", "4x4x16", "2x2x64"][tune["deposit_variant"]],
+                                     "interp_block_height": tune["interp_block_height"]}
         ctxs[prec] = s
     del box
     torch.cuda.empty_cache()
@@ -535,12 +552,13 @@ def run_c2(args, dist):
     res["mixed"]["update_hbm_frac"] = alg / (upd * 1e-3) / 1e9 / hbm
     a, asrc = device_state(ctxs["mixed"], dt)
     b, bsrc = device_state(ctxs["fp64"], dt)
-    res["mixed_vs_fp64_all"] = dict(compare(a, asrc, b, bsrc, grid), steps=warm + steps)
+    res["mixed_vs_fp64_all"] = dict(compare(a, asrc, b, bsrc, grid), steps=warm + extra + steps)
     for s in ctxs.values():
         s.close()
     res["mixed_over_fp64"] = res["mixed"]["value"] / res["fp64"]["value"]
     res["workload"] = (f"spray case: {n} droplets (bimodal 3/40 um, bottom 20%), 512x512x128 stretched 1.02, "
-                       f"log-law wind, dt={dt}, {warm} warm-up + {steps} timed steps, ilin={args.ilin}, "
+                       f"log-law wind, dt={dt}, {warm} warm-up + {extra} autotuner + {steps} timed steps, "
+                       f"ilin={args.ilin}, "
                        "inputs generated in device memory")
     res["seconds"] = time.perf_counter() - t_all
     return res
@@ -596,8 +614,7 @@ def run_e2e(case, args, dist):
             it += 1
         if args.tune_steps > 0:
             s.sync()
-            s.autotune(case.dt, it, steps=args.tune_steps)
-            it += 5 * (args.tune_steps + 1)
+            it += s.autotune(case.dt, it, steps=args.tune_steps)["steps_advanced"]
         s.sync()
         n0 = s.numpart
         barrier(dist)
@@ -666,7 +683,7 @@ def run_batch(args, precision: str):
     s.particle_update_BE(dt, 1, counters=False)
     s.particle_coupling_update(dt, download=False)
     tune = s.autotune(dt, 2, steps=args.tune_steps)
-    it = 2 + 5 * (args.tune_steps + 1)
+    it = 2 + tune["steps_advanced"]
     s.advance_graph(dt, it, args.batch_steps)          # records the graph; also a warm-up
     it += args.batch_steps
     s.sync()
@@ -690,6 +707,7 @@ def run_batch(args, precision: str):
             "edges": [sp["edge"] for sp in specs], "graph_launches_timed": 1,
             "autotune": {"deposit_shape": ["2x4x32", "4x4x16", "2x2x64"][tune["deposit_variant"]],
                          "block": [128, 256][tune["block_variant"]],
+                         "interp_block_height": tune["interp_block_height"],
                          "ms_per_step": [round(v, 4) for v in tune["ms"]]},
             "clocks": clocks}
 
@@ -900,7 +918,8 @@ def main():
         "phases_ms_per_step": {k: v / args.steps for k, v in r["prof"].items() if k.endswith("_ms")},
         "autotune": (None if not r.get("tune") else
                      {"deposit_shape": ["2x4x32", "4x4x16", "2x2x64"][r["tune"]["deposit_variant"]],
-                      "block": [128, 256][r["tune"]["block_variant"]]}),
+                      "block": [128, 256][r["tune"]["block_variant"]],
+                      "interp_block_height": r["tune"]["interp_block_height"]}),
         "gpu_launches": int(r["prof"]["launches"]),
         "roofline": {"bound": "hbm",
                      "kernel": ("update phase: k_interp_block + k_be_mixed + k_be_defer_mixed" if head == "mixed"

@@ -204,9 +204,13 @@ int ntlp_stream_priority(ntlp_ctx *ctx, int32_t priority);
  * field window in shared memory (TMA tile loads) and contracts every
  * droplet's stencil from there.  enable = 0 switches to the per-droplet
  * kernel (stencil from global memory; the same results, bit for bit), 1
- * back to the staged one, -1 only queries.  Returns the block height in
- * cells (0: per-droplet kernel) or an error code (< 0).  No counterpart in
- * the reference.                                                          */
+ * back to the staged one, -1 only queries; 4, 8, 16 or 32 sets the block
+ * height in cells (blocks are 4 x 4 x height cells; the context picks one
+ * for about 256 droplets a block, ntlp_autotune tries half and twice that)
+ * and switches staging on.
+ * Returns the block height in cells (0: per-droplet kernel) or an error
+ * code (< 0).  The results do not depend on it.  No counterpart in the
+ * reference.                                                              */
 int ntlp_interp_staging(ntlp_ctx *ctx, int32_t enable);
 
 /* ---- instrumentation (phase timers; measurement.f90's named phases) ----- */
@@ -270,9 +274,14 @@ int ntlp_step_time(ntlp_ctx *ctx, int32_t slot, double *ms);
  * 2x4x32, 4x4x16, 2x2x64 nodes) and each interpolation block size (128, 256) on
  * this context's boxes over `steps` steps (state advances), keeps the
  * fastest, and reports the per-variant milliseconds per step (ms[i] for
- * deposition shape i, ms[3+j] for block size j).                          */
-#define NTLP_TUNE_VARIANTS 5
-int ntlp_autotune(ntlp_ctx *ctx, double dt, int32_t it, int32_t steps, int32_t choice[2],
+ * deposition shape i, ms[3+j] for block size j).  With the staged mixed
+ * interpolation it then times half and twice the context's block height
+ * (ms[5], ms[6]; 0 when not tried, outside 4..32) and keeps the fastest.
+ * choice = {deposition shape, block size, interpolation block height (0:
+ * none)}.  The state advances by steps + 1 steps per variant timed.  No
+ * variant changes a result.                                               */
+#define NTLP_TUNE_VARIANTS 7
+int ntlp_autotune(ntlp_ctx *ctx, double dt, int32_t it, int32_t steps, int32_t choice[3],
                   double ms[NTLP_TUNE_VARIANTS]);
 
 /* ---- x-y column subdomains -------------------------------------------------

@@ -394,13 +394,16 @@ class DropletStep:
         return out
 
     def autotune(self, dt: float, it: int, steps: int = 2) -> dict:
-        """Time the deposition tile shapes and droplet block sizes on this
-        context's boxes (the state advances by 5 * (steps + 1) steps) and keep the
-        fastest."""
-        choice = (C.c_int32 * 2)()
-        ms = (C.c_double * 5)()
+        """Time the deposition tile shapes, the droplet block sizes and (staged
+        mixed interpolation) half and twice the interpolation block height on
+        this context's boxes, and keep the fastest.  The state advances by
+        steps + 1 steps per variant timed: `steps_advanced` in the result."""
+        choice = (C.c_int32 * 3)()
+        ms = (C.c_double * abi.NTLP_TUNE_VARIANTS)()
         self._check(self.L.ntlp_autotune(self.h, float(dt), int(it), int(steps), choice, ms), "ntlp_autotune")
-        return dict(deposit_variant=int(choice[0]), block_variant=int(choice[1]), ms=list(ms))
+        timed = sum(1 for v in ms if v > 0)
+        return dict(deposit_variant=int(choice[0]), block_variant=int(choice[1]), interp_block_height=int(choice[2]),
+                    ms=list(ms), steps_advanced=timed * (int(max(steps, 1)) + 1))
 
 
 class DropletBatch(DropletStep):

@@ -25,6 +25,7 @@ NTLP_PREC_FP64 = 0
 NTLP_PREC_MIXED = 1
 NTLP_LAYOUT_COLUMN = 0
 NTLP_LAYOUT_FLOW = 1
+NTLP_TUNE_VARIANTS = 7   # ntlp_autotune's ms[] entries
 
 _dp = C.POINTER(C.c_double)
 

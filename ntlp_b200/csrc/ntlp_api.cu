@@ -132,6 +132,7 @@ struct ntlp_ctx {
     double g_dt = 0.0;
     int g_nsteps = 0, g_dep = -1, g_nt = -1;
     bool g_blk = false;
+    int g_kb = 0;
     bool tex_all = true;   // every box's FP32 fields have a texture (mixed)
     // staged cell-block interpolation (mixed, 6th order): block height and
     // tiles; blk_kb = 0 when the tensor maps could not be made
@@ -139,6 +140,7 @@ struct ntlp_ctx {
     bool blk_on = true;
     Tile *blk_tiles_d = nullptr;
     int n_blk_tiles = 0;
+    int blk_tile_cap = 0;   // tiles blk_tiles_d holds (the smallest block height the tuner tries)
     bool tex_all64 = true;   // every box's FP64 fields have textures (FP64)
     bool any_dense = false;   // some box deposits through per-cell sums (mixed)
     int64_t g_launches = 0;
@@ -829,6 +831,7 @@ int create(int nbox, const ntlp_grid *grids, const ntlp_params *params, const in
             const long long nb = interp_block_count(c->blk_kb, g.nnx, g.nny, g.nnz);
             for (long long s = 0; s < nb; ++s) bt.push_back(Tile{b, (int)s});
             for (int r = 0; r < kOobBlockTiles; ++r) bt.push_back(Tile{b, -1 - r});
+            c->blk_tile_cap += (int)(interp_block_count(4, g.nnx, g.nny, g.nnz) + kOobBlockTiles);
         }
     }
     bft.push_back((int)ct.size());
@@ -847,7 +850,7 @@ int create(int nbox, const ntlp_grid *grids, const ntlp_params *params, const in
             }
             k.take(&c->dp_d, 1);
             k.take(&c->box_d, (size_t)nbox);
-            if (!bt.empty()) k.take(&c->blk_tiles_d, bt.size());
+            if (!bt.empty()) k.take(&c->blk_tiles_d, (size_t)c->blk_tile_cap);
         };
         Carver cv;
         lay(cv);
@@ -1396,6 +1399,40 @@ int launch_coupling(ntlp_ctx *c, double dt) {
     return NTLP_OK;
 }
 
+// another block height for the staged interpolation: the boxes' tensor
+// maps (box height kb+8 levels) and the block tile table, rebuilt on the
+// context's stream; the results do not depend on it
+int set_blk_kb(ntlp_ctx *c, int kb) {
+    if (kb == c->blk_kb) return NTLP_OK;
+    if (c->blk_kb == 0) return fail(c, NTLP_ERR_STATE, "this context has no staged interpolation");
+    if (kb != 4 && kb != 8 && kb != 16 && kb != 32) return fail(c, NTLP_ERR_ARG, "block height %d is not 4, 8, 16 or 32", kb);
+    std::vector<Tile> bt;
+    for (int b = 0; b < c->nbox; ++b) {
+        const DevGrid &g = c->box[b].g;
+        const long long nb = interp_block_count(kb, g.nnx, g.nny, g.nnz);
+        for (long long s = 0; s < nb; ++s) bt.push_back(Tile{b, (int)s});
+        for (int r = 0; r < kOobBlockTiles; ++r) bt.push_back(Tile{b, -1 - r});
+    }
+    if ((long long)bt.size() > c->blk_tile_cap)
+        return fail(c, NTLP_ERR_ARG, "block height %d needs %zu tiles, the table holds %d", kb, bt.size(),
+                    c->blk_tile_cap);
+    // the host mirror of the boxes, current, then the new maps in it
+    if (pull_boxes(c)) return NTLP_ERR_CUDA;
+    for (int b = 0; b < c->nbox; ++b) {
+        if (!encode_f4_map(c->box[b], kb)) {
+            for (int r = 0; r <= b; ++r) encode_f4_map(c->box[r], c->blk_kb);
+            return fail(c, NTLP_ERR_CUDA, "tensor map for block height %d refused", kb);
+        }
+    }
+    for (int b = 0; b < c->nbox; ++b) c->box[b].blk_kb = kb;
+    CK(cudaMemcpyAsync(c->blk_tiles_d, bt.data(), bt.size() * sizeof(Tile), cudaMemcpyHostToDevice, c->stream));
+    c->n_blk_tiles = (int)bt.size();
+    c->blk_kb = kb;
+    if (push_boxes(c)) return NTLP_ERR_CUDA;
+    CK(cudaStreamSynchronize(c->stream));   // bt is read by the copy
+    return NTLP_OK;
+}
+
 int coupling_checks(ntlp_ctx *c, double dt, int32_t layout) {
     bool any = false;
     for (auto &h : c->bh) any = any || h.have_droplets;
@@ -1490,6 +1527,12 @@ int ntlp_interp_staging(ntlp_ctx *c, int32_t enable) {
     if (!c) return NTLP_ERR_ARG;
     if (enable == 0 || enable == 1) {
         c->blk_on = enable == 1;
+    } else if (enable >= 2) {
+        int rc = set_blk_kb(c, enable);
+        if (rc) return rc;
+        c->blk_on = true;
+    } else if (enable != -1) {
+        return fail(c, NTLP_ERR_ARG, "staging switch %d", enable);
     }
     return c->blk_on ? c->blk_kb : 0;
 }
@@ -1696,7 +1739,7 @@ int ntlp_flux(ntlp_ctx *c, double *pflux, double *pmassflux, double *penegflux) 
 // instantiate it, unless the one held matches dt, nsteps and the variants
 static int build_graph(ntlp_ctx *c, double dt, int32_t it, int32_t nsteps) {
     if (c->gexec && c->g_dt == dt && c->g_nsteps == nsteps && c->g_dep == c->dep_variant &&
-        c->g_nt == c->nt_variant && c->g_blk == c->blk_on)
+        c->g_nt == c->nt_variant && c->g_blk == c->blk_on && c->g_kb == c->blk_kb)
         return NTLP_OK;
     if (c->gexec) {
         cudaGraphExecDestroy(c->gexec);
@@ -1729,6 +1772,7 @@ static int build_graph(ntlp_ctx *c, double dt, int32_t it, int32_t nsteps) {
     c->g_dep = c->dep_variant;
     c->g_nt = c->nt_variant;
     c->g_blk = c->blk_on;
+    c->g_kb = c->blk_kb;
     return NTLP_OK;
 }
 
@@ -1791,7 +1835,7 @@ int ntlp_step_time(ntlp_ctx *c, int32_t slot, double *ms) {
     return NTLP_OK;
 }
 
-int ntlp_autotune(ntlp_ctx *c, double dt, int32_t it, int32_t steps, int32_t choice[2],
+int ntlp_autotune(ntlp_ctx *c, double dt, int32_t it, int32_t steps, int32_t choice[3],
                   double ms[NTLP_TUNE_VARIANTS]) {
     if (!c) return NTLP_ERR_ARG;
     int rc = check_ready(c, dt);
@@ -1818,7 +1862,7 @@ int ntlp_autotune(ntlp_ctx *c, double dt, int32_t it, int32_t steps, int32_t cho
         *out_ms = t / steps;
         return NTLP_OK;
     };
-    double local[NTLP_TUNE_VARIANTS] = {0, 0, 0, 0, 0};
+    double local[NTLP_TUNE_VARIANTS] = {0, 0, 0, 0, 0, 0, 0};
     int best_dep = 0, best_nt = 0;
     for (int v = 0; v < kDepVariants && !rc; ++v) {
         c->dep_variant = v;
@@ -1832,6 +1876,28 @@ int ntlp_autotune(ntlp_ctx *c, double dt, int32_t it, int32_t steps, int32_t cho
         if (!rc && local[kDepVariants + v] < local[kDepVariants + best_nt]) best_nt = v;
     }
     c->nt_variant = best_nt;
+    // the staged interpolation's block height: the context's choice, half of
+    // it and twice it (within 4..32 and the tile table)
+    if (!rc && c->blk_kb > 0 && c->blk_on) {
+        const int kb0 = c->blk_kb;
+        int best_kb = kb0;
+        double best_ms = local[kDepVariants + best_nt];
+        const int cand[2] = {kb0 / 2, kb0 * 2};
+        for (int i = 0; i < 2 && !rc; ++i) {
+            const int kb = cand[i];
+            if (kb < 4 || kb > 32) continue;
+            if (set_blk_kb(c, kb)) {   // no tensor map for it: not a candidate
+                c->err.clear();
+                continue;
+            }
+            rc = time_steps(&local[kDepVariants + kNtVariants + i]);
+            if (!rc && local[kDepVariants + kNtVariants + i] < best_ms) {
+                best_ms = local[kDepVariants + kNtVariants + i];
+                best_kb = kb;
+            }
+        }
+        if (!rc) rc = set_blk_kb(c, best_kb);
+    }
     c->prof = prof;
     cudaEventDestroy(a);
     cudaEventDestroy(b);
@@ -1841,6 +1907,7 @@ int ntlp_autotune(ntlp_ctx *c, double dt, int32_t it, int32_t steps, int32_t cho
     if (choice) {
         choice[0] = best_dep;
         choice[1] = best_nt;
+        choice[2] = c->blk_on ? c->blk_kb : 0;
     }
     if (ms)
         for (int k = 0; k < NTLP_TUNE_VARIANTS; ++k) ms[k] = local[k];

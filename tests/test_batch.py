@@ -146,10 +146,15 @@ def test_autotune_changes_no_result(precision):
     dt = cases[0].dt
     for s in (a, b):
         s.particle_update_BE(dt, 1)
-    r = a.autotune(dt, 2, steps=1)          # 5 variants x 2 steps
+    r = a.autotune(dt, 2, steps=1)          # 5 to 7 variants x 2 steps
     assert 0 <= r["deposit_variant"] < 3 and 0 <= r["block_variant"] < 2
-    assert all(m > 0 for m in r["ms"])
-    for it in range(2, 12):
+    assert all(m > 0 for m in r["ms"][:5])
+    staged = precision == abi.NTLP_PREC_MIXED
+    assert (r["interp_block_height"] in (4, 8, 16, 32)) == staged
+    assert r["interp_block_height"] == a.interp_staging(-1)
+    nsteps = r["steps_advanced"]
+    assert nsteps == 2 * sum(1 for m in r["ms"] if m > 0) and nsteps >= 10
+    for it in range(2, 2 + nsteps):
         b.particle_update_BE(dt, it)
     b.particle_coupling_update(dt, download=False)
     a.particle_coupling_update(dt, download=False)
@@ -157,8 +162,8 @@ def test_autotune_changes_no_result(precision):
         _same_state(a.get_box_droplets(k), b.get_box_droplets(k))
         _same_sources(a.box_sources(k), b.box_sources(k))
     # the chosen variants run in the graph too
-    a.advance_graph(dt, 12, 2)
-    for it in (12, 13):
+    a.advance_graph(dt, 2 + nsteps, 2)
+    for it in (2 + nsteps, 3 + nsteps):
         b.particle_update_BE(dt, it)
         b.particle_coupling_update(dt, download=False)
     a.sync()

@@ -36,11 +36,13 @@ def _edges(case):
     return case
 
 
-def _run(case, params, staged, steps=3):
+def _run(case, params, staged, steps=3, height=None):
     import ntlp_b200
     s = ntlp_b200.DropletStep(case.grid, params, capacity=case.droplets["radius"].shape[0])
     kb = s.interp_staging(1 if staged else 0)
     assert (kb > 0) == staged
+    if height is not None:
+        assert s.interp_staging(height) == height
     s.set_fields_ext(case.ext())
     s.set_droplets(case.droplets)
     counters = [s.particle_update_BE(case.dt, it) for it in range(1, steps + 1)]
@@ -67,6 +69,34 @@ def test_staged_interpolation_matches_per_droplet(name, grid_n, n):
         assert bitwise_equal(d_a[k], d_b[k]), k
     for q in range(6):
         assert bitwise_equal(s_a[q], s_b[q]), q
+
+
+def test_every_block_height_gives_the_same_bits():
+    # blocks 4, 8, 16 and 32 cells high (the autotuner's choices), against
+    # the per-droplet kernel
+    params = dict(gen.default_params(ilin=0), precision=abi.NTLP_PREC_MIXED)
+    case = _edges(gen.make_case("c0", n=12000, grid_n=(13, 9, 40), params=params))
+    c_b, d_b, s_b = _run(case, params, False)
+    for height in (4, 8, 16, 32):
+        c_a, d_a, s_a = _run(case, params, True, height=height)
+        assert c_a == c_b, height
+        for k in STATE_KEYS:
+            assert bitwise_equal(d_a[k], d_b[k]), (height, k)
+        for q in range(6):
+            assert bitwise_equal(s_a[q], s_b[q]), (height, q)
+
+
+def test_block_height_setting_rejects_other_values():
+    import ntlp_b200
+    params = dict(gen.default_params(ilin=0), precision=abi.NTLP_PREC_MIXED)
+    case = small_case(params=params, n=2000, grid_n=(8, 8, 12))
+    s = ntlp_b200.DropletStep(case.grid, params, capacity=2000)
+    kb = s.interp_staging(-1)
+    for bad in (2, 6, 64):
+        with pytest.raises(ntlp_b200.NtlpError):
+            s.interp_staging(bad)
+        assert s.interp_staging(-1) == kb
+    s.close()
 
 
 def test_staged_interpolation_in_a_batch():
