@@ -500,6 +500,22 @@ void fill_devparams(const ntlp_params *p, DevParams &d) {
     d.m_q = p->Mw / p->Ru;
     d.m_vri = 1.0 / ((2.0 / 3.0) * p->pi2 * (p->radius_init * p->radius_init * p->radius_init));
     d.m_t0 = (2.0 * p->radius_init) * (2.0 * p->radius_init) / (18.0 * p->nuf);
+    d.vol = p->pi2 * 2.0 / 3.0;
+    d.f_pi2 = (float)p->pi2;
+    d.f_vol = (float)(p->pi2 * 2.0 / 3.0);
+    d.f_rhow = (float)p->rhow;
+    d.f_nuf = (float)p->nuf;
+    d.f_rhos = (float)p->rhos;
+    for (int a = 0; a < 3; ++a) d.f_g[a] = (float)p->part_grav[a];
+    d.f_m_q = (float)d.m_q;
+    d.f_m_g = (float)d.m_g;
+    d.f_m_e1 = (float)d.m_e1;
+    d.f_m_clat = (float)d.m_clat;
+    d.f_sc6 = (float)(0.6 * d.Sc13);
+    d.f_pr6 = (float)(0.6 * d.Pra13);
+    d.f_isol = (float)(1.0 / ((2.0 / 3.0) * p->pi2 * p->rhos));
+    d.f_rhow_cc = (float)(p->rhow / d.CpaCpp);
+    d.f_cpv_cpa = (float)(p->Cpv / p->Cpa);
     // set_binsdata calls of particles.f90:1909-1921
     d.hb[NTLP_H_ACTRES] = ntlp_hist_log_bins(1.0e-1, 1.0e4);
     d.hb[NTLP_H_RES] = ntlp_hist_log_bins(1.0e-1, 1.0e4);

@@ -314,12 +314,12 @@ __device__ __forceinline__ int gauss_newton32(const DevParams &p, const Drop &d,
     k.k_tpre = (float)c.k_tpre;
     k.k_rep = (float)c.k_rep;
     k.k_solv = (float)c.k_solv;
-    k.k_clat = (float)c.k_clat;
-    k.k_g = (float)c.k_g;
-    k.k_e1 = (float)c.k_e1;
+    k.k_clat = p.f_m_clat;   // c.k_clat, k_g, k_e1 are the run factors
+    k.k_g = p.f_m_g;
+    k.k_e1 = p.f_m_e1;
     k.k_q = (float)c.k_q;
-    k.sc6 = (float)(0.6 * p.Sc13);
-    k.pr6 = (float)(0.6 * p.Pra13);
+    k.sc6 = p.f_sc6;
+    k.pr6 = p.f_pr6;
     float va = (float)a, vb = (float)b;
     // the lanes of the warp that solve iterate together until a vote finds
     // every one of them finished (converged, or given up); a finished lane
@@ -472,11 +472,11 @@ __device__ double rad_solver2_64(const DevParams &p, double Tf, double qinf, dou
 __device__ double rad_solver2_32(const DevParams &p, double Tf, double qinf, double rhoa, double m_s,
                                  double kap, double radius, double esa, int &mflag) {
     mflag = 0;
-    const float pi2 = (float)p.pi2;
-    const float lg = logf((float)Tf * (float)rhoa * (float)qinf / ((float)esa * (float)p.m_q));
+    const float pi2 = p.f_pi2;
+    const float lg = logf((float)Tf * (float)rhoa * (float)qinf / ((float)esa * p.f_m_q));
     const float ilg = 1.0f / lg;
-    const float a = -((float)p.m_g / (float)Tf) * ilg;
-    const float c = (float)(kap * m_s) * (float)(1.0 / ((2.0 / 3.0) * p.pi2 * p.rhos)) * ilg;
+    const float a = -(p.f_m_g / (float)Tf) * ilg;
+    const float c = (float)(kap * m_s) * p.f_isol * ilg;
     const float Q = (a * a) * (1.0f / 9.0f);
     const float R = (2.0f * a * a * a + 27.0f * c) * (1.0f / 54.0f);
     const float M = R * R - Q * Q * Q;
@@ -681,9 +681,9 @@ __device__ __forceinline__ void write_payload_mixed(const DevBox &B, const DevPa
     const double Tprhs_s = (Tp - Tpold) * inv_dt - Tprhs_L;
     const double rhoa =
         (p.iexner == 1) ? func_p_base64(p, p.surf_p, p.tsfcc1, x[2]) / p.Rd / Tf : p.surf_rho;
-    const float rf = (float)r, pi2 = (float)p.pi2, rhow = (float)p.rhow;
+    const float rf = (float)r, pi2 = p.f_pi2, rhow = p.f_rhow;
     const float irhoa = 1.0f / (float)rhoa;
-    const float volp = (float)(p.pi2 * 2.0 / 3.0) * (rf * rf * rf);
+    const float volp = p.f_vol * (rf * rf * rf);
     // partmass = rhop*Volp = m_s + Volp*rhow; the reference's heat factor
     // Tprhs_s*6*rhow/rhop/CpaCpp/taup_i*(pi2/2)*r*nuf with taup_i =
     // 18*rhoa*nuf/rhop/(2r)^2 is Tprhs_s*Volp*rhow/(CpaCpp*rhoa) (rhop and
@@ -694,10 +694,10 @@ __device__ __forceinline__ void write_payload_mixed(const DevBox &B, const DevPa
     f[P32_FX][t] = (float)((x[0] - g.dx * (double)(ipt + g.ioff - 1)) * g.rdx);
     f[P32_FY][t] = (float)((x[1] - g.dy * (double)(jpt + g.joff - 1)) * g.rdy);
     f[P32_FZ][t] = (float)(x[2] - g.zz[kpt]) / (float)g.dzu[kpt + 1];
-    for (int a = 0; a < 3; ++a) f[P32_DV0 + a][t] = partmass * irhoa * (vrhs[a] - (float)p.g[a]) + H0 * (float)v[a];
-    f[P32_T0][t] = (float)Tprhs_s * volp * (float)(p.rhow / p.CpaCpp) * irhoa;
+    for (int a = 0; a < 3; ++a) f[P32_DV0 + a][t] = partmass * irhoa * (vrhs[a] - p.f_g[a]) + H0 * (float)v[a];
+    f[P32_T0][t] = (float)Tprhs_s * volp * p.f_rhow_cc * irhoa;
     f[P32_H0][t] = H0;
-    f[P32_E][t] = H0 * (float)(p.Cpv / p.Cpa) * (float)(Tf - Tp);
+    f[P32_E][t] = H0 * p.f_cpv_cpa * (float)(Tf - Tp);
     f[P32_FAC][t] = (float)((double)mult / (g.dx * g.dy * g.dzu[kpt + 1]));
 }
 
@@ -708,20 +708,20 @@ __device__ __forceinline__ double be_drag(const DevParams &p, double radius, dou
                                           double v[3], const double uf[3]) {
     if (MIXED) {
         const float rr = (float)radius;
-        const float volp = (float)(p.pi2 * 2.0 / 3.0) * (rr * rr * rr);
-        const float rhopf = ((float)m_s + volp * (float)p.rhow) / volp;
-        const float taup_if = 18.0f * (float)rhoa * (float)p.nuf / rhopf / ((2.0f * rr) * (2.0f * rr));
+        const float volp = p.f_vol * (rr * rr * rr);
+        const float rhopf = ((float)m_s + volp * p.f_rhow) / volp;
+        const float taup_if = 18.0f * (float)rhoa * p.f_nuf / rhopf / ((2.0f * rr) * (2.0f * rr));
         const float dtf = (float)dt;
         const float den = 1.0f + dtf * taup_if;
         float d[3] = {(float)(v[0] - uf[0]), (float)(v[1] - uf[1]), (float)(v[2] - uf[2])};
-        const double Rep = (double)(2.0f * rr * sqrtf(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) / (float)p.nuf);
+        const double Rep = (double)(2.0f * rr * sqrtf(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) / p.f_nuf);
         // the reference's update rearranged as an increment,
         // v_new - v = (dt taup_i (uf - v) + dt g) / (1 + dt taup_i), formed in
         // FP32 and added to v in FP64: the increment keeps FP32's relative
         // precision, which the momentum source (v_new - v)/dt needs when |v|
         // (a mean wind) is far larger than the change over one step
         for (int a = 0; a < 3; ++a)
-            v[a] = v[a] + (double)((dtf * (float)p.g[a] - taup_if * dtf * d[a]) / den);
+            v[a] = v[a] + (double)((dtf * p.f_g[a] - taup_if * dtf * d[a]) / den);
         return Rep;
     } else {
         const double Volp = p.pi2 * 2.0 / 3.0 * cube(radius);
@@ -920,11 +920,10 @@ __device__ __forceinline__ int be_body(const DevBox &B, const DevParams &p, cons
         // (Tp - Tf)/(Tf Tp) from the FP64 difference, and Volp*rhop - m_s
         // as Volp*rhow (the same quantity)
         const float Tpf = (float)Tp, Tff = (float)Tf, rf = (float)radius;
-        const float volp = (float)(p.pi2 * 2.0 / 3.0) * (rf * rf * rf);
+        const float volp = p.f_vol * (rf * rf * rf);
         const float dinv = (float)(Tp - Tf) / (Tff * Tpf);
-        const float E = (float)p.m_e1 * dinv + (float)p.m_g / (rf * Tpf) -
-                        (float)(kap * m_s) / ((float)p.rhos * volp);
-        qstar = (double)((float)p.m_q / (Tpf * (float)rhoa) * (float)einf * expf(E));
+        const float E = p.f_m_e1 * dinv + p.f_m_g / (rf * Tpf) - (float)(kap * m_s) / (p.f_rhos * volp);
+        qstar = (double)(p.f_m_q / (Tpf * (float)rhoa) * (float)einf * expf(E));
     } else {
         qstar = (p.Mw / (p.Ru * Tp * rhoa)) * einf *
                 ntlp_exp(((p.Lv * p.Mw / p.Ru) * ((1.0 / Tf) - (1.0 / Tp))) +
@@ -955,7 +954,7 @@ __device__ __forceinline__ int be_body(const DevBox &B, const DevParams &p, cons
         if (hi >= lo) {
             // the droplet's mass rhop*Volp; mixed: as m_s + Volp*rhow (the
             // same quantity, no divide)
-            const double pmass = MIXED ? m_s + (p.pi2 * 2.0 / 3.0 * cube(radius)) * p.rhow : rhop * Volp;
+            const double pmass = MIXED ? m_s + (p.vol * cube(radius)) * p.rhow : rhop * Volp;
             double mterm = pmass * mult;
             double eterm = pmass * p.Cpp * Tp * mult;
             const int nz1 = g.nnz + 1;
