@@ -501,6 +501,8 @@ void fill_devparams(const ntlp_params *p, DevParams &d) {
     d.m_vri = 1.0 / ((2.0 / 3.0) * p->pi2 * (p->radius_init * p->radius_init * p->radius_init));
     d.m_t0 = (2.0 * p->radius_init) * (2.0 * p->radius_init) / (18.0 * p->nuf);
     d.vol = p->pi2 * 2.0 / 3.0;
+    d.inv_surf_rho = 1.0 / p->surf_rho;
+    d.f_inv_surf_rho = 1.0f / (float)p->surf_rho;
     d.f_pi2 = (float)p->pi2;
     d.f_vol = (float)(p->pi2 * 2.0 / 3.0);
     d.f_rhow = (float)p->rhow;
@@ -1195,6 +1197,7 @@ int launch_step(ntlp_ctx *c, int kind, int istage, double dt, int32_t it, bool w
     const int nt = kNtValues[c->nt_variant];
     StepIn in;
     in.dt = dt;
+    in.inv_dt = 1.0 / dt;
     in.it = it;
     in.istage = istage;
     in.write_payload = (kind == 1 || istage == 3) ? 1 : 0;

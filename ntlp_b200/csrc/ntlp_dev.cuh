@@ -82,10 +82,13 @@ struct DevParams {
     double m_vri, m_t0;
     // mixed path only: run constants as its FP32 expressions use them, each
     // formed once here with the operations the device would repeat per
-    // droplet (the same values): pi2*2/3 in FP64, then in FP32 pi2,
+    // droplet (the same values): pi2*2/3 and 1/surf_rho in FP64, then in
+    // FP32 1/surf_rho, pi2,
     // pi2*2/3, rhow, nuf, rhos, g, m_q, m_g, m_e1, m_clat, 0.6*Sc13,
     // 0.6*Pra13, 1/((2/3)*pi2*rhos), rhow/CpaCpp, Cpv/Cpa
     double vol;
+    double inv_surf_rho;    // 1/surf_rho: 1/rhoa when iexner = 0
+    float f_inv_surf_rho;   // 1.0f/(float)surf_rho
     float f_pi2, f_vol, f_rhow, f_nuf, f_rhos, f_g[3], f_m_q, f_m_g, f_m_e1, f_m_clat, f_sc6, f_pr6, f_isol,
         f_rhow_cc, f_cpv_cpa;
     // histogram binning (particles.f90:1909-1921), by NTLP_H_* kind

@@ -29,6 +29,7 @@ constexpr int kNtValues[kNtVariants] = {128, 256};
 
 struct StepIn {
     double dt;
+    double inv_dt;   // 1/dt
     int it;
     int istage;
     int write_payload;

@@ -628,7 +628,8 @@ void launch_update_be_mixed(int ilin, int nt, DevBox *boxes, const Tile *tiles, 
 
 // Mixed payload from the stored state, for a coupling call whose dt differs
 // from the step's (runs after the finish kernel: st[cur] is the new state).
-__global__ void k_payload_mixed(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevParams P, double dt) {
+__global__ void k_payload_mixed(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevParams P,
+                                double inv_dt) {
     const Tile tl = tiles[blockIdx.x];
     const DevBox &B = boxes[tl.box];
     const int t = tl.start + threadIdx.x;
@@ -640,12 +641,12 @@ __global__ void k_payload_mixed(DevBox *boxes, const Tile *tiles, const __grid_c
     int ipt, jpt, kpt;
     if (cell_key(B.g, x[0], x[1], x[2], &ipt, &jpt, &kpt) >= (int)B.g.ncells) return;
     write_payload_mixed(B, P, s, ipt, jpt, kpt, x, v, vold, S.r[s], S.rold[s], S.Tp[s], S.Tpold[s], S.Tf[s],
-                        S.m_s[s], S.mult[s], dt);
+                        S.m_s[s], S.mult[s], inv_dt);
 }
 
 void launch_payload_mixed(DevBox *boxes, const Tile *tiles, int ntiles, const DevParams &P, double dt,
                           cudaStream_t st) {
-    if (ntiles > 0) k_payload_mixed<<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles, P, dt);
+    if (ntiles > 0) k_payload_mixed<<<ntiles, kUpdateThreads, 0, st>>>(boxes, tiles, P, 1.0 / dt);
 }
 
 template <int V>

@@ -668,12 +668,12 @@ __device__ __forceinline__ void write_payload(const DevBox &B, const DevParams &
 __device__ __forceinline__ void write_payload_mixed(const DevBox &B, const DevParams &p, int t, int ipt, int jpt,
                                                     int kpt, const double x[3], const double v[3],
                                                     const double vold[3], double r, double rold, double Tp,
-                                                    double Tpold, double Tf, double m_s, long long mult, double dt) {
+                                                    double Tpold, double Tf, double m_s, long long mult,
+                                                    double inv_dt) {
     const DevGrid &g = B.g;
     // the rates from FP64 differences; the factors, stored in FP32, computed
     // in FP32 (the reference's expressions, with Volp*rhop for partmass and
     // H0*Cpv/Cpa*(Tf - Tp) for the latent-heat term)
-    const double inv_dt = 1.0 / dt;
     float vrhs[3];
     for (int a = 0; a < 3; ++a) vrhs[a] = (float)((v[a] - vold[a]) * inv_dt);
     const double radrhs = (r - rold) * inv_dt;
@@ -682,7 +682,7 @@ __device__ __forceinline__ void write_payload_mixed(const DevBox &B, const DevPa
     const double rhoa =
         (p.iexner == 1) ? func_p_base64(p, p.surf_p, p.tsfcc1, x[2]) / p.Rd / Tf : p.surf_rho;
     const float rf = (float)r, pi2 = p.f_pi2, rhow = p.f_rhow;
-    const float irhoa = 1.0f / (float)rhoa;
+    const float irhoa = p.iexner == 1 ? 1.0f / (float)rhoa : p.f_inv_surf_rho;   // rhoa = surf_rho
     const float volp = p.f_vol * (rf * rf * rf);
     // partmass = rhop*Volp = m_s + Volp*rhow; the reference's heat factor
     // Tprhs_s*6*rhow/rhop/CpaCpp/taup_i*(pi2/2)*r*nuf with taup_i =
@@ -789,7 +789,7 @@ __device__ __forceinline__ int be_body(const DevBox &B, const DevParams &p, cons
             v[a] = (in.it <= 1) ? uf[a] : S.v[a][s];
         }
         be_drag<MIXED>(p, radius, m_s, rhoa, dt, v, uf);
-        const double irhoa = MIXED ? 1.0 / rhoa : 0.0;
+        const double irhoa = MIXED ? (p.iexner == 1 ? 1.0 / rhoa : p.inv_surf_rho) : 0.0;   // rhoa = surf_rho
         // mixed: taup0 from the per-run factors (one reciprocal of rhoa,
         // shared with the solve's constants)
         const double taup0 = MIXED ? (m_s * p.m_vri + p.rhow) * p.m_t0 * irhoa : taup0_64(p, m_s, rhoa);
@@ -994,7 +994,8 @@ __device__ __forceinline__ int be_body(const DevBox &B, const DevParams &p, cons
         key = cell_key(B.g, x[0], x[1], x[2], &ipt, &jpt, &kpt);
         if (in.write_payload && key < (int)B.g.ncells) {
             if (MIXED)
-                write_payload_mixed(B, p, t, ipt, jpt, kpt, x, v, vold, radius, rold, Tp, Tpold, Tf, m_s, multi, dt);
+                write_payload_mixed(B, p, t, ipt, jpt, kpt, x, v, vold, radius, rold, Tp, Tpold, Tf, m_s, multi,
+                                    in.inv_dt);
             else
                 write_payload(B, p, t, x, v, vold, radius, rold, Tp, Tpold, Tf, m_s, multi, dt);
         }
