@@ -74,13 +74,16 @@ struct DevParams {
     double radius_init, surf_rho, surf_p, tsfcc1, pi2;
     // derived on the host once: Cpa/Cpp (les.F:10759), Sc**(1./3.), Pra**(1./3.)
     double CpaCpp, Sc13, Pra13;
-    // mixed path only: per-run factors of the residual's constants
+    // per-run factors of the mixed residual's constants (m_clat, m_e1 and
+    // m_q, quotients of the reference's own expressions, in the FP64
+    // formulas as well)
     // 1/(36 Sc rhow), -CpaCpp/(12 Pra rhow), 2/nuf, 1/(rhow (2/3) pi2),
     // 3 Lv/Cpp, 2 Mw Gam/(Ru rhow), Lv Mw/Ru, Mw/Ru
     double m_rpre, m_tpre, m_rep, m_solv, m_clat, m_g, m_e1, m_q;
     // and of taup0: 1/((2/3) pi2 radius_init^3), (2 radius_init)^2/(18 nuf)
     double m_vri, m_t0;
-    // mixed path only: run constants as its FP32 expressions use them, each
+    // run constants as the mixed path's FP32 expressions use them (vol in
+    // the FP64 formulas as well), each
     // formed once here with the operations the device would repeat per
     // droplet (the same values): pi2*2/3 and 1/surf_rho in FP64, then in
     // FP32 1/surf_rho, pi2,

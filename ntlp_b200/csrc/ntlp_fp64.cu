@@ -347,7 +347,7 @@ k_update_rk3_64(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevPar
         double d0 = v[0] - I.uf[0], d1 = v[1] - I.uf[1], d2 = v[2] - I.uf[2];
         double diffnorm = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
         double Rep = 2.0 * radius * diffnorm / p.nuf;
-        double Volp = p.pi2 * 2.0 / 3.0 * cube(radius);
+        double Volp = p.vol * cube(radius);
         double rhop = (m_s + Volp * p.rhow) / Volp;
         double taup_i = 18.0 * rhoa * p.nuf / rhop / ((2.0 * radius) * (2.0 * radius));
         double corrfac = (1.0 + 0.15 * ntlp_pow(Rep, 0.687));
@@ -357,7 +357,7 @@ k_update_rk3_64(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevPar
         double Eff_C = 2.0 * p.Mw * p.Gam / (p.Ru * p.rhow * radius * Tp);
         double Eff_S = kap * m_s * p.rhow / p.rhos / (Volp * rhop - m_s);
         double estar = einf * ntlp_exp(p.Mw * p.Lv / p.Ru * (1.0 / Tf - 1.0 / Tp) + Eff_C - Eff_S);
-        double qstar = p.Mw / p.Ru * estar / Tp / rhoa;
+        double qstar = p.m_q * estar / Tp / rhoa;
         double xtmp[3], vtmp[3];
         for (int a = 0; a < 3; ++a) xtmp[a] = x[a] + dt * zs * xrhs[a];
         for (int a = 0; a < 3; ++a) vtmp[a] = v[a] + dt * zs * vrhs[a];
@@ -371,7 +371,7 @@ k_update_rk3_64(DevBox *boxes, const Tile *tiles, const __grid_constant__ DevPar
         else
             radrhs = 0.0;
         Tprhs_s = -Nup / 3.0 / p.Pra * p.CpaCpp * rhop / p.rhow * taup_i * (Tp - Tf);
-        Tprhs_L = 3.0 * p.Lv / p.Cpp / radius * radrhs;
+        Tprhs_L = p.m_clat / radius * radrhs;
         for (int a = 0; a < 3; ++a) x[a] = xtmp[a] + dt * ga * xrhs[a];
         for (int a = 0; a < 3; ++a) v[a] = vtmp[a] + dt * ga * vrhs[a];
         Tp = Tptmp + dt * ga * Tprhs_s;

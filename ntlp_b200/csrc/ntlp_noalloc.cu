@@ -147,6 +147,12 @@ extern "C" int ntlp_coupling_noalloc(const ntlp_grid *grid, const ntlp_params *p
     dp.CpaCpp = params->Cpa / params->Cpp;
     dp.Sc13 = ntlp_pow(params->Sc, 1.0 / 3.0);
     dp.Pra13 = ntlp_pow(params->Pra, 1.0 / 3.0);
+    // constant quotients the payload and state formulas use (the values
+    // the device would form per droplet)
+    dp.vol = params->pi2 * 2.0 / 3.0;
+    dp.m_clat = 3.0 * params->Lv / params->Cpp;
+    dp.m_e1 = params->Lv * params->Mw / params->Ru;
+    dp.m_q = params->Mw / params->Ru;
 
     const int nz2 = grid->nnz + 2, nz3 = grid->nnz + 3;
     double *zg = (double *)(S + kOffGrid);

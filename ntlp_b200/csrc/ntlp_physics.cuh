@@ -81,7 +81,7 @@ __device__ __forceinline__ void tpart(const DevParams &p, const Drop &d, const R
                                       double out[2]) {
     double Tnext = tempt * d.Tp;
     double qstr = (p.Mw / (p.Ru * Tnext * d.rhoa)) * d.esa *
-                  ntlp_exp(((p.Lv * p.Mw / p.Ru) * (d.inv_Tf - (1.0 / Tnext))) +
+                  ntlp_exp((p.m_e1 * (d.inv_Tf - (1.0 / Tnext))) +
                            ((2.0 * p.Mw * p.Gam) / (r.ruwr * Tnext)) - r.solterm);
     double rprime = r.rpre * (d.qinf - qstr);
     rprime = rprime * d.t0r;
@@ -639,14 +639,14 @@ __device__ __forceinline__ void write_payload(const DevBox &B, const DevParams &
     double vrhs[3];
     for (int a = 0; a < 3; ++a) vrhs[a] = (v[a] - vold[a]) / dt;
     double radrhs = (r - rold) / dt;
-    double Tprhs_L = 3.0 * p.Lv / p.Cpp / r * radrhs;
+    double Tprhs_L = p.m_clat / r * radrhs;
     double Tprhs_s = (Tp - Tpold) / dt - Tprhs_L;
     double rhoa;
     if (p.iexner == 1)
         rhoa = func_p_base64(p, p.surf_p, p.tsfcc1, x[2]) / p.Rd / Tf;
     else
         rhoa = p.surf_rho;
-    double rhop = (m_s + pi2 * 2.0 / 3.0 * cube(r) * p.rhow) / (pi2 * 2.0 / 3.0 * cube(r));
+    double rhop = (m_s + p.vol * cube(r) * p.rhow) / (p.vol * cube(r));
     double partmass = rhop * 2.0 / 3.0 * pi2 * cube(r);
     double taup_i = 18.0 * rhoa * p.nuf / rhop / ((2.0 * r) * (2.0 * r));
     double H0 = p.rhow / rhoa * pi2 * 2.0 * (r * r) * radrhs;
@@ -724,7 +724,7 @@ __device__ __forceinline__ double be_drag(const DevParams &p, double radius, dou
             v[a] = v[a] + (double)((dtf * p.f_g[a] - taup_if * dtf * d[a]) / den);
         return Rep;
     } else {
-        const double Volp = p.pi2 * 2.0 / 3.0 * cube(radius);
+        const double Volp = p.vol * cube(radius);
         const double rhop = (m_s + Volp * p.rhow) / Volp;
         double d0 = v[0] - uf[0], d1 = v[1] - uf[1], d2 = v[2] - uf[2];
         double diffnorm = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
@@ -902,7 +902,7 @@ __device__ __forceinline__ int be_body(const DevBox &B, const DevParams &p, cons
         radius = rtz[0] * radius;
         Tp = rtz[1] * Tp;
     } else {
-        Volp = p.pi2 * 2.0 / 3.0 * cube(radius);
+        Volp = p.vol * cube(radius);
         rhop = (m_s + Volp * p.rhow) / Volp;
         double taup_i = 18.0 * rhoa * p.nuf / rhop / ((2.0 * radius) * (2.0 * radius));
         double Nup = 2.0 + 0.6 * sqrt(Rep) * p.Pra13;
@@ -910,7 +910,7 @@ __device__ __forceinline__ int be_body(const DevBox &B, const DevParams &p, cons
         Tp = (Tp + tmp_coeff * dt * Tf) / (1.0 + dt * tmp_coeff);
     }
     if (!MIXED) {
-        Volp = p.pi2 * 2.0 / 3.0 * cube(radius);
+        Volp = p.vol * cube(radius);
         rhop = (m_s + Volp * p.rhow) / Volp;
     }
     const double einf = solved ? esa1 : mod_magnus64(Tf);
@@ -926,7 +926,7 @@ __device__ __forceinline__ int be_body(const DevBox &B, const DevParams &p, cons
         qstar = (double)(p.f_m_q / (Tpf * (float)rhoa) * (float)einf * expf(E));
     } else {
         qstar = (p.Mw / (p.Ru * Tp * rhoa)) * einf *
-                ntlp_exp(((p.Lv * p.Mw / p.Ru) * ((1.0 / Tf) - (1.0 / Tp))) +
+                ntlp_exp((p.m_e1 * ((1.0 / Tf) - (1.0 / Tp))) +
                          ((2.0 * p.Mw * p.Gam) / (p.Ru * p.rhow * radius * Tp)) -
                          ((kap * m_s * p.rhow / p.rhos) / (Volp * rhop - m_s)));
     }

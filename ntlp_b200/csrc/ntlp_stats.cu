@@ -70,7 +70,7 @@ k_stats_tiles(const DevBox *boxes, int box, const DevParams *pp, double *tile0, 
                 const double mult = (double)S.mult[t];
                 a[kS0Count] += 1.0;
                 if (r > S.rc[t]) a[kS0Drop] += 1.0;
-                const double Volp = p.pi2 * 2.0 / 3.0 * cube(r);
+                const double Volp = p.vol * cube(r);
                 const double rhop = (m_s + Volp * p.rhow) / Volp;
                 const double d0 = vp[0] - uf[0], d1 = vp[1] - uf[1], d2 = vp[2] - uf[2];
                 const double diffnorm = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
