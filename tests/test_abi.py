@@ -41,6 +41,17 @@ def test_library_exports_every_declared_symbol(lib):
     assert not missing, missing
 
 
+def test_python_constants_match_the_header():
+    # every integer #define of the header that the ctypes mirror also names
+    # has the same value there (array sizes such as NTLP_TUNE_VARIANTS size
+    # the buffers the binding passes)
+    text = open(os.path.join(ROOT, "include", "ntlp_gpu.h")).read()
+    defs = {k: int(v) for k, v in re.findall(r"#define\s+(NTLP_[A-Z0-9_]+)\s+(-?\d+)\b", text)}
+    shared = [k for k in defs if hasattr(abi, k)]
+    assert "NTLP_TUNE_VARIANTS" in shared and len(shared) >= 10
+    assert {k: getattr(abi, k) for k in shared} == {k: defs[k] for k in shared}
+
+
 def test_struct_sizes_match_header_layout():
     # the ABI structs are plain C: sizes follow from their fields
     assert C.sizeof(abi.NtlpGrid) == 4 * 4 + 3 * 8 + 4 * 8
